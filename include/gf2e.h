@@ -1,0 +1,215 @@
+/*
+ * gf2e.h -- C ABI of the B200 engine for smallest irreducible factors of
+ * x^r + x^s + 1 over GF(2) (libgf2e.so).
+ *
+ * Plain pointers and sizes only.  Every entry point returns an int status
+ * (GF2E_OK = 0, negative on error) and never exits the process; the C++
+ * drop-in headers (gf2e_cantor.hpp, gf2e_trinomial.hpp) turn a non-zero
+ * status into the reference's print-and-exit behaviour.  Pointers named
+ * *_dev are device pointers; `stream` is a cudaStream_t (NULL = legacy
+ * default stream).  All launches are asynchronous on `stream` unless noted.
+ *
+ * Bit layout (shared with the reference, gf2_gcd.h:1-4): little-endian
+ * uint64 words, bit i of word w is the coefficient of x^(64w+i); a residue
+ * mod x^r + x^s + 1 has nw = ceil(r/64) words and bits >= r are zero.
+ *
+ * Each declaration names the reference interface it replaces.
+ */
+#ifndef GF2E_H
+#define GF2E_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define GF2E_ABI_VERSION 1
+
+/* status codes */
+#define GF2E_OK 0
+#define GF2E_ERR_INVALID -1        /* bad argument (the reference exit(1)s) */
+#define GF2E_ERR_CUDA -2           /* CUDA runtime error, see gf2e_last_error() */
+#define GF2E_ERR_NOMEM -3          /* workspace too small / allocation failed */
+#define GF2E_ERR_UNSUPPORTED_R -4  /* gcd(r, 2^d - 1) != 1 (sieve_ref.cpp:79-83) */
+#define GF2E_ERR_TIMEOUT -5        /* a bounded device-side wait gave up */
+#define GF2E_ERR_OVERFLOW -6       /* a fixed-capacity device queue overflowed */
+#define GF2E_ERR_INTERNAL -7       /* consistency check failed on the device */
+
+int gf2e_abi_version(void);
+const char *gf2e_status_string(int status);
+/* Human-readable detail of the last error raised on the calling thread. */
+const char *gf2e_last_error(void);
+/* Synchronize `stream` and return GF2E_ERR_CUDA if any launch failed. */
+int gf2e_stream_sync(void *stream);
+
+/* Device memory helpers for callers without their own allocator (the
+ * reference's contexts cudaMalloc in init, gf2_trinomial_cuda.h:100-116).
+ * The copies are ordered on `stream` and return after it has drained. */
+int gf2e_device_alloc(void **ptr_dev, size_t bytes);
+int gf2e_device_free(void *ptr_dev);
+int gf2e_copy_to_host(void *dst_host, const void *src_dev, size_t bytes, void *stream);
+int gf2e_copy_to_device(void *dst_dev, const void *src_host, size_t bytes, void *stream);
+
+/* ======================================================================
+ * (a) Zech-log sieve.
+ * Replaces coarse_sieve.cu run_gpu (1119-1225) / sieve_degree_gpu (852-918)
+ * and sieve_ref.cpp run_sieve (125-134).  best_dev[s], s = 0..smax, holds
+ * the packed key (d << 48) | mask of the smallest-degree, then numerically
+ * least, irreducible factor p of x^r + x^s + 1 with dmin <= d <= dmax; all
+ * ones where none was found.  Keys are merged with min, so degrees may be
+ * sieved in any order and a preloaded best[] (coarse_sieve --load) is
+ * extended exactly.
+ * ====================================================================== */
+
+/* Device workspace bytes needed by gf2e_sieve_run for degrees <= dmax. */
+int gf2e_sieve_workspace_size(int dmax, size_t *bytes);
+
+/* best_dev[0..smax] = UINT64_MAX (coarse_sieve.cu k_fill 301-305). */
+int gf2e_sieve_fill(uint64_t *best_dev, uint64_t smax, void *stream);
+
+/* Sieve degrees dmin..dmax (2 <= dmin <= dmax <= 24) into best_dev.
+ * Host-side per-degree setup (primitive polynomial search) is cached.
+ * Returns GF2E_ERR_UNSUPPORTED_R when gcd(r mod (2^d-1), 2^d-1) != 1 for
+ * some d in range, before launching anything.  All degrees are enqueued on
+ * `stream`; the call then reads a small status block, so it returns after
+ * the sieve has finished on the device. */
+int gf2e_sieve_run(uint64_t r, int dmin, int dmax, uint64_t smax,
+                   uint64_t *best_dev, void *workspace_dev,
+                   size_t workspace_bytes, void *stream);
+
+/* Read back per-degree statistics of the last gf2e_sieve_run on this
+ * workspace (sized for `dmax`): coset classes and marks, arrays of 25
+ * entries indexed by d (sieve_ref.cpp:128-132 prints the same counts).
+ * Synchronizes `stream`. */
+int gf2e_sieve_stats(const void *workspace_dev, int dmax, uint64_t *classes_host,
+                     uint64_t *marks_host, void *stream);
+
+/* Smallest primitive polynomial of degree d, 2 <= d <= 32
+ * (gf2_field_setup.h:49-58).  Host only. */
+uint64_t gf2e_primitive_poly(int d);
+
+/* ======================================================================
+ * (b) Squaring with trinomial fold reduction in GF(2)[x]/(x^r + x^s + 1).
+ * Requires r odd, 1 <= s, 2s < r (gf2_trinomial_cuda.h:118-123).
+ * ====================================================================== */
+
+/* out = in^2 mod T, single pass (tsfactor.cu k_square_fused 139-186;
+ * gf2_trinomial_cuda.h TrinGPU::square_A 149-154).  in != out. */
+int gf2e_trin_square(const uint64_t *in_dev, uint64_t *out_dev, uint64_t r,
+                     uint64_t s, void *stream);
+
+/* Batched repeated squaring: each of `nstates` states (state i at
+ * states_dev + i*stride_words, stride_words >= nw, even) is squared k times
+ * mod x^r + x^(s_i) + 1, s_i = s_dev[i] (device array).  scratch_dev has the
+ * same shape as states_dev; the result is left in states_dev.
+ * (trinomial_stage2.cu run loop 232-253: F_k = x^(2^k) mod T, many s at once.) */
+int gf2e_trin_square_batch(uint64_t *states_dev, uint64_t *scratch_dev,
+                           size_t stride_words, int nstates, uint64_t r,
+                           const uint64_t *s_dev, uint32_t k, void *stream);
+
+/* Host-buffer form of the above, the whole of trinomial_stage2.cu `run`
+ * (195-277) for many s with k0 > k1: F_k = x^(2^k) mod x^r + x^(s_i) + 1 for
+ * every s_host[i], written to out_host + i*out_stride_words (nw words each).
+ * Device memory is a per-thread workspace kept between calls; returns after
+ * the results are in host memory. */
+int gf2e_trin_frobenius_host(uint64_t r, const uint64_t *s_host, int nstates,
+                             uint32_t k, uint64_t *out_host,
+                             size_t out_stride_words, void *stream);
+
+/* states <- x (gf2_trinomial_cuda.h k_set_x 80-84), nstates at stride. */
+int gf2e_trin_set_x(uint64_t *states_dev, size_t stride_words, int nstates,
+                    uint64_t r, void *stream);
+
+/* states <- 1 (TrinGPU::reset_acc 124-128; tsfactor.cu k_set_one 198-202). */
+int gf2e_trin_set_one(uint64_t *states_dev, size_t stride_words, int nstates,
+                      uint64_t r, void *stream);
+
+/* out (nw words) = prod mod T where prod has prod_bits <= 2r - 1 bits,
+ * stored in ceil(prod_bits/64) words (TrinGPU::reduce 136-146). */
+int gf2e_trin_reduce(const uint64_t *prod_dev, uint64_t prod_bits,
+                     uint64_t *out_dev, uint64_t r, uint64_t s, void *stream);
+
+/* ======================================================================
+ * (c) Cantor additive FFT over GF(2^64) and GF(2)[x] multiplication.
+ * Replaces gf2_cantor_cuda.h CudaFFT (361-521) and gf2_cantor_engine.h
+ * gf2x_fft_mul_buf / gf2x_fft_mul (207-242).  Transform points and order
+ * are the reference's: values f(W-indexed points) in natural order.
+ * ====================================================================== */
+typedef struct gf2e_fft_plan gf2e_fft_plan;
+
+/* The Cantor basis b[0..len) (CantorBasis::build, gf2_cantor_engine.h:78-103). */
+int gf2e_cantor_basis(uint64_t *basis64, int *len);
+
+/* Plan for transforms of n = 2^m points, 1 <= m <= 30 (CudaFFT::init). */
+int gf2e_fft_plan_create(int m, gf2e_fft_plan **plan);
+int gf2e_fft_plan_destroy(gf2e_fft_plan *plan);
+int gf2e_fft_plan_m(const gf2e_fft_plan *plan);
+
+/* In-place forward / inverse transform of n device words (CudaFFT::fwd/inv). */
+int gf2e_fft_fwd(const gf2e_fft_plan *plan, uint64_t *f_dev, void *stream);
+int gf2e_fft_inv(const gf2e_fft_plan *plan, uint64_t *f_dev, void *stream);
+
+/* Twiddle table W[t], t < n/2 (CudaFFT::dW / CantorFFT::W), to host memory. */
+int gf2e_fft_twiddles(const gf2e_fft_plan *plan, uint64_t *W_host);
+
+/* FFT size exponent for an abits x bbits product (gf2_cantor_engine.h:232-238)
+ * and the product's word count (mul_out_words, :201-203). */
+int gf2e_mul_fft_m(uint64_t abits, uint64_t bbits);
+size_t gf2e_mul_out_words(uint64_t abits, uint64_t bbits);
+
+/* out = a * b over GF(2)[x] (gf2x_fft_mul_buf).  All device pointers; plan
+ * size must be >= gf2e_mul_fft_m(abits, bbits); fa, fb: 2^m words each of
+ * scratch; out has gf2e_mul_out_words(abits, bbits) words, fully written. */
+int gf2e_mul(const gf2e_fft_plan *plan, const uint64_t *a_dev, uint64_t abits,
+             const uint64_t *b_dev, uint64_t bbits, uint64_t *out_dev,
+             uint64_t *fa_dev, uint64_t *fb_dev, void *stream);
+
+/* One product in a batch (config: many uneven products in one call). */
+typedef struct gf2e_mul_job {
+    const uint64_t *a_dev;
+    uint64_t abits;
+    const uint64_t *b_dev;
+    uint64_t bbits;
+    uint64_t *out_dev;      /* gf2e_mul_out_words(abits, bbits) words */
+} gf2e_mul_job;
+
+/* Scratch bytes gf2e_mul_batch needs for these jobs. */
+int gf2e_mul_batch_workspace_size(const gf2e_mul_job *jobs_host, int njobs,
+                                  size_t *bytes);
+
+/* All products of jobs_host[0..njobs) on the device; plans are created and
+ * cached per FFT size inside the library. */
+int gf2e_mul_batch(const gf2e_mul_job *jobs_host, int njobs, void *workspace_dev,
+                   size_t workspace_bytes, void *stream);
+
+/* ======================================================================
+ * TrinGPU context (gf2_trinomial_cuda.h:87-178): F (dA), ACC (dACC),
+ * product scratch and an FFT plan for r-bit x r-bit products.
+ * ====================================================================== */
+typedef struct gf2e_trin gf2e_trin;
+
+int gf2e_trin_create(uint64_t r, gf2e_trin **ctx);        /* TrinGPU::init */
+int gf2e_trin_destroy(gf2e_trin *ctx);                    /* TrinGPU::fini */
+int gf2e_trin_set_s(gf2e_trin *ctx, uint64_t s);          /* TrinGPU::set_s */
+/* Device pointers of F (dA) and ACC (dACC), nw words each; product scratch
+ * dT0 (2*nw words); FFT size exponent m. */
+int gf2e_trin_buffers(gf2e_trin *ctx, uint64_t **dA, uint64_t **dACC,
+                      uint64_t **dT0, size_t *nw, int *m);
+int gf2e_trin_reset_A(gf2e_trin *ctx, void *stream);      /* k_set_x on dA */
+int gf2e_trin_reset_acc(gf2e_trin *ctx, void *stream);    /* ACC <- 1 */
+int gf2e_trin_square_A(gf2e_trin *ctx, void *stream);     /* dA <- dA^2 mod T */
+/* dT0 (2r-1 bits) <- x * y, both r-bit device operands (TrinGPU::mul_dev). */
+int gf2e_trin_mul_dev(gf2e_trin *ctx, const uint64_t *x_dev,
+                      const uint64_t *y_dev, void *stream);
+/* dst <- dT0 mod T where dT0 holds L bits (TrinGPU::reduce). */
+int gf2e_trin_reduce_T0(gf2e_trin *ctx, uint64_t *dst_dev, uint64_t L,
+                        void *stream);
+/* ACC <- ACC * (F + x) mod T (TrinGPU::accumulate). */
+int gf2e_trin_accumulate(gf2e_trin *ctx, void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* GF2E_H */

@@ -1,0 +1,118 @@
+"""ctypes binding of libgf2e.so (the C ABI declared in include/gf2e.h).
+
+The shared library is built in-tree by `python -m mersenne_trinomial_b200.build`.
+There is no fallback: if the library is missing or fails to load, every
+entry point raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import threading
+
+LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "libgf2e.so")
+
+GF2E_OK = 0
+STATUS = {
+    0: "GF2E_OK",
+    -1: "GF2E_ERR_INVALID",
+    -2: "GF2E_ERR_CUDA",
+    -3: "GF2E_ERR_NOMEM",
+    -4: "GF2E_ERR_UNSUPPORTED_R",
+    -5: "GF2E_ERR_TIMEOUT",
+    -6: "GF2E_ERR_OVERFLOW",
+    -7: "GF2E_ERR_INTERNAL",
+}
+
+
+class Gf2eError(RuntimeError):
+    def __init__(self, status: int, detail: str):
+        super().__init__(f"{STATUS.get(status, status)}: {detail}")
+        self.status = status
+        self.detail = detail
+
+
+class MulJob(C.Structure):
+    _fields_ = [("a_dev", C.c_void_p), ("abits", C.c_uint64), ("b_dev", C.c_void_p),
+                ("bbits", C.c_uint64), ("out_dev", C.c_void_p)]
+
+
+_lib = None
+_lock = threading.Lock()
+
+_u64, _i32, _vp, _sz = C.c_uint64, C.c_int, C.c_void_p, C.c_size_t
+_P = C.POINTER
+
+# name -> (restype, argtypes); every symbol of include/gf2e.h
+SIGNATURES = {
+    "gf2e_abi_version": (_i32, []),
+    "gf2e_status_string": (C.c_char_p, [_i32]),
+    "gf2e_last_error": (C.c_char_p, []),
+    "gf2e_stream_sync": (_i32, [_vp]),
+    "gf2e_device_alloc": (_i32, [_P(_vp), _sz]),
+    "gf2e_device_free": (_i32, [_vp]),
+    "gf2e_copy_to_host": (_i32, [_vp, _vp, _sz, _vp]),
+    "gf2e_copy_to_device": (_i32, [_vp, _vp, _sz, _vp]),
+    "gf2e_sieve_workspace_size": (_i32, [_i32, _P(_sz)]),
+    "gf2e_sieve_fill": (_i32, [_vp, _u64, _vp]),
+    "gf2e_sieve_run": (_i32, [_u64, _i32, _i32, _u64, _vp, _vp, _sz, _vp]),
+    "gf2e_sieve_stats": (_i32, [_vp, _i32, _vp, _vp, _vp]),
+    "gf2e_primitive_poly": (_u64, [_i32]),
+    "gf2e_trin_square": (_i32, [_vp, _vp, _u64, _u64, _vp]),
+    "gf2e_trin_square_batch": (_i32, [_vp, _vp, _sz, _i32, _u64, _vp, C.c_uint32, _vp]),
+    "gf2e_trin_frobenius_host": (_i32, [_u64, _vp, _i32, C.c_uint32, _vp, _sz, _vp]),
+    "gf2e_trin_set_x": (_i32, [_vp, _sz, _i32, _u64, _vp]),
+    "gf2e_trin_set_one": (_i32, [_vp, _sz, _i32, _u64, _vp]),
+    "gf2e_trin_reduce": (_i32, [_vp, _u64, _vp, _u64, _u64, _vp]),
+    "gf2e_cantor_basis": (_i32, [_vp, _P(_i32)]),
+    "gf2e_fft_plan_create": (_i32, [_i32, _P(_vp)]),
+    "gf2e_fft_plan_destroy": (_i32, [_vp]),
+    "gf2e_fft_plan_m": (_i32, [_vp]),
+    "gf2e_fft_fwd": (_i32, [_vp, _vp, _vp]),
+    "gf2e_fft_inv": (_i32, [_vp, _vp, _vp]),
+    "gf2e_fft_twiddles": (_i32, [_vp, _vp]),
+    "gf2e_mul_fft_m": (_i32, [_u64, _u64]),
+    "gf2e_mul_out_words": (_sz, [_u64, _u64]),
+    "gf2e_mul": (_i32, [_vp, _vp, _u64, _vp, _u64, _vp, _vp, _vp, _vp]),
+    "gf2e_mul_batch_workspace_size": (_i32, [_P(MulJob), _i32, _P(_sz)]),
+    "gf2e_mul_batch": (_i32, [_P(MulJob), _i32, _vp, _sz, _vp]),
+    "gf2e_trin_create": (_i32, [_u64, _P(_vp)]),
+    "gf2e_trin_destroy": (_i32, [_vp]),
+    "gf2e_trin_set_s": (_i32, [_vp, _u64]),
+    "gf2e_trin_buffers": (_i32, [_vp, _P(_vp), _P(_vp), _P(_vp), _P(_sz), _P(_i32)]),
+    "gf2e_trin_reset_A": (_i32, [_vp, _vp]),
+    "gf2e_trin_reset_acc": (_i32, [_vp, _vp]),
+    "gf2e_trin_square_A": (_i32, [_vp, _vp]),
+    "gf2e_trin_mul_dev": (_i32, [_vp, _vp, _vp, _vp]),
+    "gf2e_trin_reduce_T0": (_i32, [_vp, _vp, _u64, _vp]),
+    "gf2e_trin_accumulate": (_i32, [_vp, _vp]),
+}
+
+
+def lib():
+    """Load libgf2e.so once; raise if it is absent (no CPU fallback exists)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    with _lock:
+        if _lib is None:
+            if not os.path.exists(LIB_PATH):
+                raise RuntimeError(
+                    f"{LIB_PATH} is missing: build it with `python -m mersenne_trinomial_b200.build`")
+            L = C.CDLL(LIB_PATH)
+            for name, (res, args) in SIGNATURES.items():
+                fn = getattr(L, name)
+                fn.restype = res
+                fn.argtypes = args
+            _lib = L
+    return _lib
+
+
+def check(status: int) -> None:
+    if status != GF2E_OK:
+        detail = lib().gf2e_last_error()
+        raise Gf2eError(status, detail.decode() if detail else "")
+
+
+def call(name: str, *args) -> None:
+    check(getattr(lib(), name)(*args))

@@ -1,0 +1,602 @@
+// cantor.cu -- Cantor additive FFT over GF(2^64) and GF(2)[x] multiply.
+//
+// Transform definition (points, order, twiddles) is the reference's
+// (gf2_cantor_engine.h:125-188): a Taylor cascade of range-XORs for depths
+// L = 0..m-2, then butterflies for levels m-1..0 with twiddle
+// W[t] = XOR of basis[j+1] over the set bits j of t.
+//
+// B200 mapping.  Every Taylor level and butterfly level acts on "rows" of a
+// strided 2-D view of the array, so a run of consecutive levels fits in one
+// shared-memory tile of NS rows (row stride CH elements) x C contiguous
+// columns.  One kernel launch (a "pass") loads each tile once from HBM,
+// applies up to ~10 levels in shared memory and stores it once.  Once the
+// depth L0 is reached at which a whole depth-L0 subproblem (n >> L0 rows of
+// the view) fits in a tile, one pass finishes every remaining Taylor depth
+// and the matching butterfly levels (m-1..L0) for a group of columns.  At
+// m = 24 with 4096-element tiles this is ~36 passes per transform instead of
+// the reference's ~70 fused / ~550 legacy passes.  Twiddles are rebuilt
+// from four 256-entry byte tables (W is GF(2)-linear in t), so no n/2-entry
+// table is streamed from HBM.
+#include "gf2e_internal.cuh"
+
+#include <map>
+#include <mutex>
+#include <vector>
+#include <algorithm>
+
+namespace {
+
+constexpr int TILE_LOG = 12;
+constexpr int TILE = 1 << TILE_LOG;        // elements per shared-memory tile
+constexpr int CMIN = 4;                    // minimum contiguous columns (32 B)
+constexpr int MAXOPS = 96;
+constexpr int FFT_THREADS = 256;
+constexpr int NTWTAB = 4;                  // byte tables: t < 2^32
+
+enum OpType : u32 { TAY_F = 0, TAY_I = 1, BF_F = 2, BF_I = 3 };
+
+// op word: type | log2(row quarter or row distance) << 2 | L << 8
+__host__ __device__ inline u32 mkop(u32 type, u32 lg, u32 L) { return type | (lg << 2) | (L << 8); }
+
+struct Pass {
+    u64 CH;          // row stride (elements)
+    u32 ns_log;      // log2 rows per window
+    u32 c_log;       // log2 columns per tile
+    u32 wpt_log;     // log2 windows per tile (only when C == CH)
+    u32 nops;
+    u32 ops[MAXOPS];
+};
+
+// W(t) from byte tables: tab[k*256 + b] = XOR of basis[8k+j+1], bits j of b
+GF2E_DEV u64 twiddle(const u64 *__restrict__ tab, u64 t) {
+    u64 w = 0;
+#pragma unroll
+    for (int k = 0; k < NTWTAB; k++) w ^= __ldg(tab + k * 256 + ((t >> (8 * k)) & 255));
+    return w;
+}
+
+// One pass over all tiles.  src32/nchunks: when non-null the tile is loaded
+// from 32-bit chunks of an operand (packing fused into the first pass),
+// zero beyond nchunks.
+__global__ void __launch_bounds__(FFT_THREADS)
+k_fft_pass(u64 *__restrict__ f, const u64 *__restrict__ tab, const Pass P, u64 ntiles,
+           const u32 *__restrict__ src32, u64 nchunks) {
+    extern __shared__ u64 sm[];
+    const u32 C = 1u << P.c_log;
+    const u32 NS = 1u << P.ns_log;
+    const u32 rows_total = NS << P.wpt_log;          // rows in the tile (all windows)
+    const u32 tile_elems = rows_total * C;
+    const u64 cgroups = P.CH >> P.c_log;             // column groups per window
+
+    for (u64 tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+        u64 base;
+        if (P.wpt_log) {                             // several whole windows, C == CH
+            base = tile * ((u64)tile_elems);
+        } else {
+            u64 win = tile / cgroups, cg = tile - win * cgroups;
+            base = win * ((u64)NS * P.CH) + cg * C;
+        }
+        // load
+        for (u32 e = threadIdx.x; e < tile_elems; e += FFT_THREADS) {
+            u32 row = e >> P.c_log, col = e & (C - 1);
+            u64 g = base + (u64)row * P.CH + col;
+            u64 v;
+            if (src32) v = (g < nchunks) ? (u64)__ldg(src32 + g) : 0ull;
+            else v = f[g];
+            sm[e] = v;
+        }
+        __syncthreads();
+        for (u32 k = 0; k < P.nops; k++) {
+            const u32 op = P.ops[k];
+            const u32 type = op & 3, lg = (op >> 2) & 63, L = op >> 8;
+            if (type <= TAY_I) {
+                const u32 qr = 1u << lg;
+                const u32 ntrip = tile_elems >> 2;
+                for (u32 tau = threadIdx.x; tau < ntrip; tau += FFT_THREADS) {
+                    u32 col = tau & (C - 1), tt = tau >> P.c_log;
+                    u32 blk = tt >> lg, i = tt & (qr - 1);
+                    u32 r1 = (blk << (lg + 2)) + qr + i;
+                    u32 i1 = (r1 << P.c_log) + col, i2 = i1 + (qr << P.c_log),
+                        i3 = i2 + (qr << P.c_log);
+                    u64 a = sm[i1], b = sm[i2], c = sm[i3];
+                    if (type == TAY_F) { b ^= c; a ^= b; }
+                    else { a ^= b; b ^= c; }
+                    sm[i1] = a;
+                    sm[i2] = b;
+                }
+            } else {
+                const u32 D = 1u << lg;
+                const u32 npair = tile_elems >> 1;
+                for (u32 tau = threadIdx.x; tau < npair; tau += FFT_THREADS) {
+                    u32 col = tau & (C - 1), pp = tau >> P.c_log;
+                    u32 ra = ((pp >> lg) << (lg + 1)) + (pp & (D - 1));
+                    u32 ia = (ra << P.c_log) + col, ib = ia + (D << P.c_log);
+                    // physical index of (row ra, column 0); the window of a
+                    // multi-window tile is folded into the row count
+                    u64 phys = base + (u64)ra * P.CH;
+                    u64 tw = twiddle(tab, phys >> (L + 1));
+                    u64 e1 = sm[ia], e2 = sm[ib];
+                    if (type == BF_F) {
+                        u64 e = e1 ^ gf64_mul(tw, e2);
+                        sm[ia] = e;
+                        sm[ib] = e ^ e2;
+                    } else {
+                        u64 hh = e1 ^ e2;
+                        sm[ia] = e1 ^ gf64_mul(tw, hh);
+                        sm[ib] = hh;
+                    }
+                }
+            }
+            __syncthreads();
+        }
+        for (u32 e = threadIdx.x; e < tile_elems; e += FFT_THREADS) {
+            u32 row = e >> P.c_log, col = e & (C - 1);
+            f[base + (u64)row * P.CH + col] = sm[e];
+        }
+        __syncthreads();
+    }
+}
+
+__global__ void k_pack(const u32 *__restrict__ a32, u64 nchunks, u64 *__restrict__ F, u64 n) {
+    for (u64 k = (u64)blockIdx.x * blockDim.x + threadIdx.x; k < n;
+         k += (u64)gridDim.x * blockDim.x)
+        F[k] = (k < nchunks) ? (u64)a32[k] : 0ull;
+}
+
+__global__ void k_pointwise(u64 *__restrict__ fa, const u64 *__restrict__ fb, u64 n) {
+    for (u64 k = (u64)blockIdx.x * blockDim.x + threadIdx.x; k < n;
+         k += (u64)gridDim.x * blockDim.x)
+        fa[k] = gf64_mul(fa[k], fb[k]);
+}
+
+// gather-form overlap-add of 64-bit coefficients at 32-bit stride
+__global__ void k_overlap_add(const u64 *__restrict__ F, u64 nchunks, u64 *__restrict__ out,
+                              u64 ow) {
+    for (u64 w = (u64)blockIdx.x * blockDim.x + threadIdx.x; w < ow;
+         w += (u64)gridDim.x * blockDim.x) {
+        u64 k = 2 * w, v = 0;
+        if (k < nchunks) v ^= F[k];
+        if (k + 1 < nchunks) v ^= F[k + 1] << 32;
+        if (w && k - 1 < nchunks) v ^= F[k - 1] >> 32;
+        out[w] = v;
+    }
+}
+
+// ------------------------------------------------------------- host side
+u64 host_gf64_mul(u64 a, u64 b) {
+    u64 lo = 0, hi = 0;
+    for (int i = 0; i < 64; i++)
+        if ((b >> i) & 1) {
+            lo ^= a << i;
+            if (i) hi ^= a >> (64 - i);
+        }
+    u64 t = lo ^ hi ^ (hi << 1) ^ (hi << 3) ^ (hi << 4);
+    u64 h2 = (hi >> 63) ^ (hi >> 61) ^ (hi >> 60);
+    return t ^ h2 ^ (h2 << 1) ^ (h2 << 3) ^ (h2 << 4);
+}
+
+// Cantor basis: b0 = 1, b_i^2 + b_i = b_{i-1}; of the two solutions
+// {y, y+1} the one with zero constant coefficient is taken (the choice the
+// reference's elimination makes, gf2_cantor_engine.h:78-103).
+int host_cantor_basis(u64 *b) {
+    u64 pv[64] = {0}, pt[64] = {0};
+    for (int i = 1; i < 64; i++) {
+        u64 e = 1ull << i, v = host_gf64_mul(e, e) ^ e, t = e;
+        for (int bit = 63; bit >= 0 && v; bit--) {
+            if (!((v >> bit) & 1)) continue;
+            if (pv[bit]) { v ^= pv[bit]; t ^= pt[bit]; }
+            else { pv[bit] = v; pt[bit] = t; v = 0; }
+        }
+    }
+    b[0] = 1;
+    int len = 1;
+    while (len < 64) {
+        u64 c = b[len - 1], v = c, y = 0;
+        bool ok = true;
+        for (int bit = 63; bit >= 0 && v; bit--) {
+            if (!((v >> bit) & 1)) continue;
+            if (!pv[bit]) { ok = false; break; }
+            v ^= pv[bit];
+            y ^= pt[bit];
+        }
+        if (!ok || v) break;
+        y &= ~1ull;
+        if ((host_gf64_mul(y, y) ^ y) != c) return -1;
+        b[len++] = y;
+    }
+    return len;
+}
+
+const u64 *basis_host() {
+    static u64 b[64];
+    static int len = 0;
+    static std::once_flag once;
+    std::call_once(once, [] { len = host_cantor_basis(b); });
+    return len == 64 ? b : nullptr;
+}
+
+// smallest column count fitting the tile, or 0 if the group does not fit
+u32 choose_c(u64 CH, u64 NS) {
+    if (NS > (u64)TILE) return 0;
+    u64 c = std::min<u64>(CH, (u64)TILE / NS);
+    if (c < CMIN && c != CH) return 0;
+    return (u32)c;
+}
+
+int ilog2u(u64 v) { return 63 - __builtin_clzll(v); }
+
+Pass make_pass(u64 CH, u64 NS, u32 C, u64 n) {
+    Pass p;
+    memset(&p, 0, sizeof p);
+    p.CH = CH;
+    p.ns_log = (u32)ilog2u(NS);
+    p.c_log = (u32)ilog2u(C);
+    // whole windows: pack several into one tile (never more than exist)
+    if ((u64)C == CH) {
+        u64 win_elems = NS * CH;
+        u64 wpt = std::min<u64>((u64)TILE / win_elems, n / win_elems);
+        if (wpt < 1) wpt = 1;
+        p.wpt_log = (u32)ilog2u(wpt);
+    }
+    return p;
+}
+
+struct PlanImpl {
+    int m = 0;
+    u64 n = 0;
+    u64 *d_tab = nullptr;                // NTWTAB x 256 twiddle byte tables
+    std::vector<Pass> fwd, inv;
+    std::vector<u64> ntiles_fwd, ntiles_inv;
+};
+
+u64 pass_tiles(const Pass &p, u64 n) {
+    u64 elems = ((u64)1 << (p.ns_log + p.c_log + p.wpt_log));
+    return n / elems;
+}
+
+void build_passes(PlanImpl &P) {
+    const int m = P.m;
+    const u64 n = P.n;
+    // deep depth L0: smallest L0 at which n >> L0 rows x C columns fit
+    int L0 = 0;
+    u32 Cd = 0;
+    for (L0 = 0; L0 <= m; L0++) {
+        u64 rows = n >> L0;
+        if (rows > (u64)TILE) continue;
+        Cd = choose_c((u64)1 << L0, rows);
+        if (Cd) break;
+    }
+    if (L0 > m - 1) L0 = m - 1;            // n <= 2: degenerate
+    if (m == 1) L0 = 0;
+    if (!Cd) Cd = 1;
+    std::vector<Pass> fwd, inv;
+    // Taylor depths 0..L0-1, grouped levels
+    for (int L = 0; L < L0 && L <= m - 2; L++) {
+        int b_hi = m - L;
+        while (b_hi >= 2) {
+            int best_lo = b_hi;
+            for (int b_lo = 2; b_lo <= b_hi; b_lo++) {
+                u64 CH = (u64)1 << (b_lo - 2 + L);
+                u64 NS = (u64)1 << (b_hi - b_lo + 2);
+                if (b_hi - b_lo + 1 <= MAXOPS && choose_c(CH, NS)) { best_lo = b_lo; break; }
+            }
+            u64 CH = (u64)1 << (best_lo - 2 + L);
+            u64 NS = (u64)1 << (b_hi - best_lo + 2);
+            Pass pf = make_pass(CH, NS, choose_c(CH, NS), n);
+            Pass pi = pf;
+            for (int b = b_hi; b >= best_lo; b--) pf.ops[pf.nops++] = mkop(TAY_F, b - best_lo, 0);
+            for (int b = best_lo; b <= b_hi; b++) pi.ops[pi.nops++] = mkop(TAY_I, b - best_lo, 0);
+            fwd.push_back(pf);
+            inv.push_back(pi);
+            b_hi = best_lo - 1;
+        }
+    }
+    // deep pass: Taylor depths L0..m-2 and butterflies m-1..L0
+    {
+        const int mp = m - L0;
+        u64 CH = (u64)1 << L0, NS = n >> L0;
+        Pass pf = make_pass(CH, NS, Cd, n);
+        Pass pi = pf;
+        for (int Lp = 0; Lp <= mp - 2; Lp++)
+            for (int e = mp - 2; e >= Lp; e--) pf.ops[pf.nops++] = mkop(TAY_F, e, 0);
+        for (int L = m - 1; L >= L0; L--) pf.ops[pf.nops++] = mkop(BF_F, L - L0, L);
+        for (int L = L0; L <= m - 1; L++) pi.ops[pi.nops++] = mkop(BF_I, L - L0, L);
+        for (int Lp = mp - 2; Lp >= 0; Lp--)
+            for (int e = Lp; e <= mp - 2; e++) pi.ops[pi.nops++] = mkop(TAY_I, e, 0);
+        fwd.push_back(pf);
+        inv.push_back(pi);
+    }
+    // butterflies L0-1..0 in groups, built bottom-up
+    std::vector<std::pair<int, int>> groups;   // (L_lo, L_hi)
+    {
+        int L_lo = 0;
+        while (L_lo <= L0 - 1) {
+            int best_hi = L_lo;
+            for (int L_hi = L0 - 1; L_hi >= L_lo; L_hi--) {
+                u64 CH = (u64)1 << L_lo, NS = (u64)1 << (L_hi - L_lo + 1);
+                if (choose_c(CH, NS)) { best_hi = L_hi; break; }
+            }
+            groups.push_back({L_lo, best_hi});
+            L_lo = best_hi + 1;
+        }
+    }
+    for (size_t gi = groups.size(); gi-- > 0;) {          // forward: top group first
+        int L_lo = groups[gi].first, L_hi = groups[gi].second;
+        u64 CH = (u64)1 << L_lo, NS = (u64)1 << (L_hi - L_lo + 1);
+        Pass pf = make_pass(CH, NS, choose_c(CH, NS), n);
+        for (int L = L_hi; L >= L_lo; L--) pf.ops[pf.nops++] = mkop(BF_F, L - L_lo, L);
+        fwd.push_back(pf);
+    }
+    std::vector<Pass> inv_b;
+    for (size_t gi = 0; gi < groups.size(); gi++) {       // inverse: bottom group first
+        int L_lo = groups[gi].first, L_hi = groups[gi].second;
+        u64 CH = (u64)1 << L_lo, NS = (u64)1 << (L_hi - L_lo + 1);
+        Pass pi = make_pass(CH, NS, choose_c(CH, NS), n);
+        for (int L = L_lo; L <= L_hi; L++) pi.ops[pi.nops++] = mkop(BF_I, L - L_lo, L);
+        inv_b.push_back(pi);
+    }
+    // inverse order: butterflies (bottom-up), deep pass, Taylor depths L0-1..0
+    std::vector<Pass> inv_all = inv_b;
+    inv_all.push_back(inv.back());
+    for (size_t i = inv.size() - 1; i-- > 0;) inv_all.push_back(inv[i]);
+    P.fwd = fwd;
+    P.inv = inv_all;
+    for (auto &p : P.fwd) P.ntiles_fwd.push_back(pass_tiles(p, n));
+    for (auto &p : P.inv) P.ntiles_inv.push_back(pass_tiles(p, n));
+}
+
+int run_passes(const PlanImpl &P, bool forward, u64 *f, const u32 *src32, u64 nchunks,
+               cudaStream_t st) {
+    const auto &ps = forward ? P.fwd : P.inv;
+    const auto &nt = forward ? P.ntiles_fwd : P.ntiles_inv;
+    for (size_t i = 0; i < ps.size(); i++) {
+        u64 elems = (u64)1 << (ps[i].ns_log + ps[i].c_log + ps[i].wpt_log);
+        size_t smem = elems * sizeof(u64);
+        int grid = (int)std::min<u64>(nt[i], (u64)gf2e::sm_count() * 8);
+        k_fft_pass<<<grid, FFT_THREADS, smem, st>>>(f, P.d_tab, ps[i], nt[i],
+                                                    (i == 0) ? src32 : nullptr, nchunks);
+        GF2E_CHECK_LAUNCH("k_fft_pass");
+    }
+    return GF2E_OK;
+}
+
+}  // namespace
+
+struct gf2e_fft_plan {
+    PlanImpl impl;
+};
+
+namespace gf2e {
+
+int fft_plan_create(int m, gf2e_fft_plan **out) {
+    if (m < 1 || m > 30) return invalid("FFT size exponent m=%d outside 1..30", m);
+    const u64 *b = basis_host();
+    if (!b) return invalid("Cantor basis construction failed");
+    static bool attr_done = false;
+    if (!attr_done) {
+        cudaFuncSetAttribute(k_fft_pass, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             TILE * (int)sizeof(u64));
+        attr_done = true;
+    }
+    gf2e_fft_plan *p = new gf2e_fft_plan;
+    p->impl.m = m;
+    p->impl.n = (u64)1 << m;
+    std::vector<u64> tab(NTWTAB * 256, 0);
+    for (int k = 0; k < NTWTAB; k++)
+        for (int v = 0; v < 256; v++) {
+            u64 w = 0;
+            for (int j = 0; j < 8; j++)
+                if ((v >> j) & 1) w ^= b[8 * k + j + 1 < 64 ? 8 * k + j + 1 : 63];
+            tab[k * 256 + v] = w;
+        }
+    cudaError_t e = cudaMalloc(&p->impl.d_tab, tab.size() * sizeof(u64));
+    if (e == cudaSuccess)
+        e = cudaMemcpy(p->impl.d_tab, tab.data(), tab.size() * sizeof(u64), cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) {
+        cudaFree(p->impl.d_tab);
+        delete p;
+        return cuda_status(e, "fft plan twiddle tables");
+    }
+    build_passes(p->impl);
+    *out = p;
+    return GF2E_OK;
+}
+
+int fft_fwd_packed(const gf2e_fft_plan *plan, u64 *f, const u32 *src32, u64 nchunks,
+                   cudaStream_t st) {
+    return run_passes(plan->impl, true, f, src32, nchunks, st);
+}
+
+int fft_run(const gf2e_fft_plan *plan, bool forward, u64 *f, cudaStream_t st) {
+    return run_passes(plan->impl, forward, f, nullptr, 0, st);
+}
+
+int pointwise(u64 *fa, const u64 *fb, u64 n, cudaStream_t st) {
+    k_pointwise<<<grid_for(n, 256), 256, 0, st>>>(fa, fb, n);
+    GF2E_CHECK_LAUNCH("k_pointwise");
+    return GF2E_OK;
+}
+
+int overlap_add(const u64 *F, u64 nchunks, u64 *out, u64 ow, cudaStream_t st) {
+    k_overlap_add<<<grid_for(ow, 256), 256, 0, st>>>(F, nchunks, out, ow);
+    GF2E_CHECK_LAUNCH("k_overlap_add");
+    return GF2E_OK;
+}
+
+int pack(const u64 *a, u64 nchunks, u64 *F, u64 n, cudaStream_t st) {
+    k_pack<<<grid_for(n, 256), 256, 0, st>>>(reinterpret_cast<const u32 *>(a), nchunks, F, n);
+    GF2E_CHECK_LAUNCH("k_pack");
+    return GF2E_OK;
+}
+
+int mul_fft_m(u64 abits, u64 bbits) {
+    u64 ca = (abits + 31) >> 5, cb = (bbits + 31) >> 5;
+    int m = 1;
+    while (((u64)1 << m) < ca + cb - 1) m++;
+    return m;
+}
+
+// full product with a plan of size >= the needed one (gf2x_fft_mul_buf)
+int mul(const gf2e_fft_plan *plan, const u64 *a, u64 abits, const u64 *b, u64 bbits,
+        u64 *out, u64 *fa, u64 *fb, cudaStream_t st) {
+    const u64 n = plan->impl.n;
+    const u64 ca = (abits + 31) >> 5, cb = (bbits + 31) >> 5;
+    if (abits == 0 || bbits == 0) return invalid("gf2e_mul: empty operand");
+    if (ca + cb - 1 > n) return invalid("FFT too small: plan m=%d for %llu x %llu bits",
+                                         plan->impl.m, (unsigned long long)abits,
+                                         (unsigned long long)bbits);
+    GF2E_TRY(fft_fwd_packed(plan, fa, reinterpret_cast<const u32 *>(a), ca, st));
+    if (b == a && bbits == abits) {
+        GF2E_TRY(pointwise(fa, fa, n, st));
+    } else {
+        GF2E_TRY(fft_fwd_packed(plan, fb, reinterpret_cast<const u32 *>(b), cb, st));
+        GF2E_TRY(pointwise(fa, fb, n, st));
+    }
+    GF2E_TRY(fft_run(plan, false, fa, st));
+    u64 ow = ((abits + bbits + 63) >> 6) + 1;
+    return overlap_add(fa, ca + cb - 1, out, ow, st);
+}
+
+// plan cache shared by the batch API and the trinomial context
+gf2e_fft_plan *cached_plan(int m) {
+    static std::mutex mu;
+    static std::map<std::pair<int, int>, gf2e_fft_plan *> cache;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    std::lock_guard<std::mutex> lk(mu);
+    auto it = cache.find({dev, m});
+    if (it != cache.end()) return it->second;
+    gf2e_fft_plan *p = nullptr;
+    if (fft_plan_create(m, &p) != GF2E_OK) return nullptr;
+    cache[{dev, m}] = p;
+    return p;
+}
+
+}  // namespace gf2e
+
+extern "C" {
+
+int gf2e_cantor_basis(uint64_t *basis64, int *len) {
+    const u64 *b = basis_host();
+    if (!b) return gf2e::invalid("Cantor basis construction failed");
+    if (basis64) memcpy(basis64, b, 64 * sizeof(u64));
+    if (len) *len = 64;
+    return GF2E_OK;
+}
+
+int gf2e_fft_plan_create(int m, gf2e_fft_plan **plan) {
+    if (!plan) return gf2e::invalid("null plan pointer");
+    return gf2e::fft_plan_create(m, plan);
+}
+
+int gf2e_fft_plan_destroy(gf2e_fft_plan *plan) {
+    if (!plan) return GF2E_OK;
+    cudaFree(plan->impl.d_tab);
+    delete plan;
+    return GF2E_OK;
+}
+
+int gf2e_fft_plan_m(const gf2e_fft_plan *plan) { return plan ? plan->impl.m : -1; }
+
+int gf2e_fft_fwd(const gf2e_fft_plan *plan, uint64_t *f_dev, void *stream) {
+    if (!plan || !f_dev) return gf2e::invalid("gf2e_fft_fwd: null argument");
+    return gf2e::fft_run(plan, true, f_dev, (cudaStream_t)stream);
+}
+
+int gf2e_fft_inv(const gf2e_fft_plan *plan, uint64_t *f_dev, void *stream) {
+    if (!plan || !f_dev) return gf2e::invalid("gf2e_fft_inv: null argument");
+    return gf2e::fft_run(plan, false, f_dev, (cudaStream_t)stream);
+}
+
+int gf2e_fft_twiddles(const gf2e_fft_plan *plan, uint64_t *W_host) {
+    if (!plan || !W_host) return gf2e::invalid("gf2e_fft_twiddles: null argument");
+    const u64 *b = basis_host();
+    u64 half = plan->impl.n >> 1;
+    if (half == 0) return GF2E_OK;
+    W_host[0] = 0;
+    for (u64 t = 1; t < half; t++) {
+        int hb = 63 - __builtin_clzll(t);
+        W_host[t] = W_host[t ^ (1ull << hb)] ^ b[hb + 1];
+    }
+    return GF2E_OK;
+}
+
+int gf2e_mul_fft_m(uint64_t abits, uint64_t bbits) { return gf2e::mul_fft_m(abits, bbits); }
+
+size_t gf2e_mul_out_words(uint64_t abits, uint64_t bbits) {
+    return (size_t)(((abits + bbits + 63) >> 6) + 1);
+}
+
+int gf2e_mul(const gf2e_fft_plan *plan, const uint64_t *a_dev, uint64_t abits,
+             const uint64_t *b_dev, uint64_t bbits, uint64_t *out_dev, uint64_t *fa_dev,
+             uint64_t *fb_dev, void *stream) {
+    if (!plan || !a_dev || !b_dev || !out_dev || !fa_dev || !fb_dev)
+        return gf2e::invalid("gf2e_mul: null argument");
+    return gf2e::mul(plan, a_dev, abits, b_dev, bbits, out_dev, fa_dev, fb_dev,
+                     (cudaStream_t)stream);
+}
+
+int gf2e_mul_batch_workspace_size(const gf2e_mul_job *jobs, int njobs, size_t *bytes) {
+    if (!jobs || njobs < 0 || !bytes) return gf2e::invalid("bad batch arguments");
+    size_t tot = 0;
+    for (int i = 0; i < njobs; i++) {
+        if (jobs[i].abits == 0 || jobs[i].bbits == 0) return gf2e::invalid("empty operand in job %d", i);
+        tot += 2 * ((size_t)1 << gf2e::mul_fft_m(jobs[i].abits, jobs[i].bbits)) * sizeof(u64);
+    }
+    *bytes = tot;
+    return GF2E_OK;
+}
+
+int gf2e_mul_batch(const gf2e_mul_job *jobs, int njobs, void *workspace, size_t ws_bytes,
+                   void *stream) {
+    size_t need = 0;
+    GF2E_TRY(gf2e_mul_batch_workspace_size(jobs, njobs, &need));
+    if (ws_bytes < need || (!workspace && need))
+        return gf2e::invalid("gf2e_mul_batch: workspace %zu < %zu bytes", ws_bytes, need);
+    cudaStream_t st = (cudaStream_t)stream;
+    // fork onto a few internal streams so small products overlap large ones
+    constexpr int NSTREAMS = 8;
+    static thread_local cudaStream_t side[NSTREAMS] = {};
+    static thread_local cudaEvent_t ev_side[NSTREAMS] = {};
+    static thread_local cudaEvent_t ev_fork = nullptr;
+    if (!ev_fork) {
+        for (int i = 0; i < NSTREAMS; i++) {
+            cudaStreamCreateWithFlags(&side[i], cudaStreamNonBlocking);
+            cudaEventCreateWithFlags(&ev_side[i], cudaEventDisableTiming);
+        }
+        cudaEventCreateWithFlags(&ev_fork, cudaEventDisableTiming);
+    }
+    cudaError_t e = cudaEventRecord(ev_fork, st);
+    if (e != cudaSuccess) return gf2e::cuda_status(e, "batch fork");
+    for (int i = 0; i < NSTREAMS; i++) cudaStreamWaitEvent(side[i], ev_fork, 0);
+    // largest first, round-robin over streams
+    std::vector<int> order(njobs);
+    for (int i = 0; i < njobs; i++) order[i] = i;
+    std::sort(order.begin(), order.end(), [&](int x, int y) {
+        return jobs[x].abits + jobs[x].bbits > jobs[y].abits + jobs[y].bbits;
+    });
+    std::vector<size_t> offs(njobs);
+    size_t off = 0;
+    for (int i = 0; i < njobs; i++) {
+        offs[i] = off;
+        off += 2 * ((size_t)1 << gf2e::mul_fft_m(jobs[i].abits, jobs[i].bbits));
+    }
+    u64 *ws = (u64 *)workspace;
+    for (int k = 0; k < njobs; k++) {
+        int i = order[k];
+        int m = gf2e::mul_fft_m(jobs[i].abits, jobs[i].bbits);
+        gf2e_fft_plan *p = gf2e::cached_plan(m);
+        if (!p) return gf2e::invalid("plan creation failed for m=%d", m);
+        u64 *fa = ws + offs[i], *fb = fa + ((size_t)1 << m);
+        GF2E_TRY(gf2e::mul(p, jobs[i].a_dev, jobs[i].abits, jobs[i].b_dev, jobs[i].bbits,
+                           jobs[i].out_dev, fa, fb, side[k % NSTREAMS]));
+    }
+    for (int i = 0; i < NSTREAMS; i++) {
+        cudaEventRecord(ev_side[i], side[i]);
+        cudaStreamWaitEvent(st, ev_side[i], 0);
+    }
+    GF2E_CHECK_LAUNCH("gf2e_mul_batch");
+    return GF2E_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,424 @@
+// sieve.cu -- Zech-log sieve for the smallest irreducible factor of degree
+// d <= 24 of x^r + x^s + 1, for every s in [1, smax] at once.
+//
+// Number theory (the reference's, sieve_ref.cpp:8-26): in GF(2^d) built on
+// the smallest primitive q_d (x generates the group of order M = 2^d - 1), an
+// irreducible p of degree d with root beta = x^j divides x^r + x^s + 1 iff
+// j*s == Z(j*r mod M) (mod M), Z the Zech logarithm Z(u) = log(x^u + 1): an
+// arithmetic progression in s of modulus n = M / gcd(j, M).  Only the
+// smallest j of each cyclotomic coset and no proper-subfield j is used;
+// key (d << 48) | mask(p) is merged into best[s] with min.
+//
+// B200 mapping:
+//   k_tables    antilog A[i] = x^i (a multiply-by-x chain per 32 entries) and
+//               the log scatter L[A[i]] = i in the same pass (tables are
+//               L2-resident up to d = 23: 2 x 32 MB).
+//   k_classes   one thread per j: coset/subfield filters, Zech lookup,
+//               progression; the minimal polynomial only for classes that
+//               mark some s <= smax, by GF(2) elimination on the powers
+//               beta^0..beta^d (O(d^2) word ops instead of O(d^2) field
+//               multiplies; the minimal polynomial is unique so the mask is
+//               identical).  Progressions are routed by length:
+//                 n < STRIP          -> strip list (applied in shared memory)
+//                 <= INLINE marks    -> marked at once with atomicMin
+//                 otherwise          -> heavy list (grid-stride atomicMin)
+//   k_heavy     all heavy progressions of all degrees, one launch.
+//   k_strip     each CTA owns a STRIP-wide slice of best[], applies every
+//               short-period progression with shared-memory atomics and
+//               writes the slice back once (last writer, so plain min).
+// All degrees are enqueued on one stream with no host round trip; the only
+// synchronisation is the final overflow/status read.
+#include "gf2e_internal.cuh"
+
+#include <mutex>
+#include <vector>
+
+namespace {
+
+constexpr int DMAX = 24;
+constexpr u64 STRIP = 4096;               // best[] entries per strip CTA (32 KB smem)
+constexpr u64 INLINE = 32;                // marks done inline by the class thread
+constexpr u64 SCAP = 1ull << 17;          // strip-list capacity
+constexpr u64 HCAP = 1ull << 21;          // heavy-list capacity
+
+struct Prog { u64 s0, n, key; };          // first s, period, packed key
+
+struct Counters {
+    unsigned long long nstrip, nheavy, overflow, bad;
+    unsigned long long classes[DMAX + 1];
+    unsigned long long marks[DMAX + 1];
+};
+
+struct Layout {
+    size_t off_A, off_L, off_strip, off_heavy, off_cnt, total;
+};
+
+Layout layout_for(int dmax) {
+    Layout l;
+    size_t tab = ((size_t)1 << dmax) * sizeof(u32);
+    tab = (tab + 255) & ~(size_t)255;
+    l.off_A = 0;
+    l.off_L = tab;
+    l.off_strip = 2 * tab;
+    l.off_heavy = l.off_strip + SCAP * sizeof(Prog);
+    l.off_cnt = l.off_heavy + HCAP * sizeof(Prog);
+    l.total = l.off_cnt + ((sizeof(Counters) + 255) & ~(size_t)255);
+    return l;
+}
+
+// ---- small field GF(2^d), d <= 24, modulus q (bit d set)
+GF2E_DEV u32 sf_mul(u32 a, u32 b, u32 q, int d) {
+    u64 t = clmul32(a, b);
+    for (int bit = 2 * d - 2; bit >= d; bit--)
+        if ((t >> bit) & 1) t ^= (u64)q << (bit - d);
+    return (u32)t;
+}
+GF2E_DEV u32 sf_mulx(u32 a, u32 q, int d) {
+    u32 t = a << 1;
+    return ((t >> d) & 1) ? (t ^ q) : t;
+}
+GF2E_DEV u32 sf_powx(u64 e, u32 q, int d) {     // x^e
+    u32 r = 1, b = 2;
+    while (e) {
+        if (e & 1) r = sf_mul(r, b, q, d);
+        b = sf_mul(b, b, q, d);
+        e >>= 1;
+    }
+    return r;
+}
+// x mod (2^d - 1)
+GF2E_DEV u64 mod_mersenne(u64 x, int d, u64 M) {
+    while (x > M) x = (x & M) + (x >> d);
+    return x == M ? 0 : x;
+}
+GF2E_DEV u64 gcd_u64(u64 a, u64 b) {
+    while (b) { u64 t = a % b; a = b; b = t; }
+    return a;
+}
+GF2E_DEV u64 inv_mod(u64 a, u64 m) {
+    long long t = 0, nt = 1, r = (long long)m, nr = (long long)(a % m);
+    while (nr) {
+        long long qq = r / nr, tmp;
+        tmp = t - qq * nt; t = nt; nt = tmp;
+        tmp = r - qq * nr; r = nr; nr = tmp;
+    }
+    if (t < 0) t += (long long)m;
+    return (u64)t;
+}
+
+__global__ void k_tables(u32 *__restrict__ A, u32 *__restrict__ L, int d, u32 q, u64 M) {
+    u64 nchunk = (M + 31) >> 5;
+    for (u64 t = (u64)blockIdx.x * blockDim.x + threadIdx.x; t < nchunk;
+         t += (u64)gridDim.x * blockDim.x) {
+        u64 i0 = t << 5;
+        u32 v = sf_powx(i0, q, d);
+        for (int e = 0; e < 32; e++) {
+            u64 i = i0 + e;
+            if (i >= M) break;
+            A[i] = v;
+            L[v] = (u32)i;
+            v = sf_mulx(v, q, d);
+        }
+    }
+}
+
+struct DegreeArgs {
+    int d;
+    u32 q;
+    u64 M, rmod, smax;
+    int nsub;
+    u64 subq[6];
+};
+
+__global__ void __launch_bounds__(256)
+k_classes(const u32 *__restrict__ A, const u32 *__restrict__ L, const DegreeArgs a,
+          unsigned long long *__restrict__ best, Prog *__restrict__ strip, Prog *__restrict__ heavy,
+          Counters *__restrict__ cnt) {
+    const int d = a.d;
+    const u64 M = a.M;
+    unsigned long long my_classes = 0, my_marks = 0;
+    for (u64 j = (u64)blockIdx.x * blockDim.x + threadIdx.x + 1; j < M;
+         j += (u64)gridDim.x * blockDim.x) {
+        bool skip = false;
+        for (int k = 0; k < a.nsub; k++)
+            if (j % a.subq[k] == 0) { skip = true; break; }
+        if (skip) continue;
+        u64 jj = j;
+        bool minimal = true;
+        for (int i = 1; i < d; i++) {
+            jj = ((jj << 1) | (jj >> (d - 1))) & M;
+            if (jj < j) { minimal = false; break; }
+        }
+        if (!minimal) continue;
+        my_classes++;
+        u64 u = mod_mersenne(j * a.rmod, d, M);
+        if (u == 0) continue;
+        u64 v = L[A[u] ^ 1u];
+        u64 gg = gcd_u64(j, M);
+        if (v % gg) continue;
+        u64 n = M / gg;
+        u64 s0 = (inv_mod(j / gg, n) * (v / gg)) % n;
+        u64 first = s0 ? s0 : n;
+        if (first > a.smax) continue;
+        u64 count = (a.smax - first) / n + 1;
+        // minimal polynomial of beta = x^j: first linear dependency among
+        // beta^0..beta^d over GF(2)
+        u32 prow[DMAX + 1], ptag[DMAX + 1];
+        int pbit[DMAX + 1];
+        int np = 0;
+        u32 mask = 0;
+        u64 idx = 0;
+        for (int k = 0; k <= d; k++) {
+            u32 row = A[idx], tag = 1u << k;
+            for (int p = 0; p < np; p++)
+                if ((row >> pbit[p]) & 1) { row ^= prow[p]; tag ^= ptag[p]; }
+            if (row == 0) { mask = tag; break; }
+            pbit[np] = 31 - __clz(row);
+            prow[np] = row;
+            ptag[np] = tag;
+            np++;
+            idx += j;
+            if (idx >= M) idx -= M;
+        }
+        if (!((mask >> d) & 1) || !(mask & 1)) {        // cannot happen
+            atomicAdd(&cnt->bad, 1ull);
+            continue;
+        }
+        const unsigned long long key = ((u64)d << 48) | mask;
+        my_marks += count;
+        if (n < STRIP) {
+            unsigned long long slot = atomicAdd(&cnt->nstrip, 1ull);
+            if (slot < SCAP) strip[slot] = Prog{first, n, key};
+            else atomicAdd(&cnt->overflow, 1ull);
+        } else if (count <= INLINE) {
+            for (u64 s = first; s <= a.smax; s += n) atomicMin(&best[s], key);
+        } else {
+            unsigned long long slot = atomicAdd(&cnt->nheavy, 1ull);
+            if (slot < HCAP) heavy[slot] = Prog{first, n, key};
+            else atomicAdd(&cnt->overflow, 1ull);
+        }
+    }
+    // warp-aggregated statistics
+    for (int o = 16; o; o >>= 1) {
+        my_classes += __shfl_down_sync(0xffffffffu, my_classes, o);
+        my_marks += __shfl_down_sync(0xffffffffu, my_marks, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        if (my_classes) atomicAdd(&cnt->classes[d], my_classes);
+        if (my_marks) atomicAdd(&cnt->marks[d], my_marks);
+    }
+}
+
+// heavy progressions: block-strided over records, threads over marks
+__global__ void k_heavy(const Prog *__restrict__ heavy, const Counters *__restrict__ cnt,
+                        u64 smax, unsigned long long *__restrict__ best) {
+    u64 nh = cnt->nheavy;
+    if (nh > HCAP) nh = HCAP;
+    for (u64 rec = blockIdx.x; rec < nh; rec += gridDim.x) {
+        Prog p = heavy[rec];
+        for (u64 s = p.s0 + (u64)threadIdx.x * p.n; s <= smax; s += (u64)blockDim.x * p.n)
+            atomicMin(&best[s], (unsigned long long)p.key);
+    }
+}
+
+// short-period progressions, one STRIP-wide slice of best[] per CTA
+__global__ void __launch_bounds__(512)
+k_strip(const Prog *__restrict__ strip, const Counters *__restrict__ cnt, u64 smax,
+        unsigned long long *__restrict__ best) {
+    __shared__ unsigned long long sb[STRIP];
+    u64 ns = cnt->nstrip;
+    if (ns > SCAP) ns = SCAP;
+    const u64 nstrips = (smax + 1 + STRIP - 1) / STRIP;
+    for (u64 sid = blockIdx.x; sid < nstrips; sid += gridDim.x) {
+        const u64 lo = sid * STRIP;
+        const u64 hi = (lo + STRIP - 1 < smax) ? lo + STRIP - 1 : smax;   // inclusive
+        for (u64 i = threadIdx.x; i < STRIP; i += blockDim.x) sb[i] = ~0ull;
+        __syncthreads();
+        // warps take progressions, lanes take marks
+        const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
+        for (u64 pi = warp; pi < ns; pi += nwarps) {
+            Prog p = strip[pi];
+            if (p.s0 > hi) continue;
+            u64 s = p.s0;
+            if (s < lo) s += ((lo - s + p.n - 1) / p.n) * p.n;
+            for (s += (u64)lane * p.n; s <= hi; s += 32 * p.n) atomicMin(&sb[s - lo], p.key);
+        }
+        __syncthreads();
+        for (u64 i = threadIdx.x; i <= hi - lo; i += blockDim.x) {
+            unsigned long long v = sb[i];
+            if (v != ~0ull) {
+                unsigned long long cur = best[lo + i];
+                if (v < cur) best[lo + i] = v;
+            }
+        }
+        __syncthreads();
+    }
+}
+
+__global__ void k_fill(unsigned long long *p, u64 n, unsigned long long v) {
+    for (u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += (u64)gridDim.x * blockDim.x)
+        p[i] = v;
+}
+
+// ---- host-side field setup (gf2_field_setup.h:14-58 restated)
+u32 h_mul(u32 a, u32 b, u64 q, int d) {
+    u64 t = 0, x = a;
+    while (b) { if (b & 1) t ^= x; x <<= 1; b >>= 1; }
+    for (int bit = 2 * d - 2; bit >= d; bit--)
+        if ((t >> bit) & 1) t ^= q << (bit - d);
+    return (u32)t;
+}
+u32 h_pow(u32 base, u64 e, u64 q, int d) {
+    u32 r = 1;
+    while (e) { if (e & 1) r = h_mul(r, base, q, d); base = h_mul(base, base, q, d); e >>= 1; }
+    return r;
+}
+int h_prime_factors(u64 m, u64 *out) {
+    int n = 0;
+    for (u64 p = 2; p * p <= m; p += (p == 2 ? 1 : 2))
+        if (m % p == 0) { out[n++] = p; while (m % p == 0) m /= p; }
+    if (m > 1) out[n++] = m;
+    return n;
+}
+bool h_irreducible(u64 q, int d) {
+    u32 chain[40];
+    u32 t = 2;
+    chain[0] = t;
+    for (int i = 1; i <= d; i++) { t = h_mul(t, t, q, d); chain[i] = t; }
+    if (chain[d] != 2) return false;
+    u64 ps[16];
+    int np = h_prime_factors((u64)d, ps);
+    for (int i = 0; i < np; i++)
+        if (chain[d / ps[i]] == 2) return false;
+    return true;
+}
+u64 h_primitive(int d) {
+    u64 M = ((u64)1 << d) - 1, ps[64];
+    int np = h_prime_factors(M, ps);
+    for (u64 q = ((u64)1 << d) | 1; q < ((u64)2 << d); q += 2) {
+        if (!h_irreducible(q, d)) continue;
+        bool prim = true;
+        for (int i = 0; i < np && prim; i++)
+            if (h_pow(2, M / ps[i], q, d) == 1) prim = false;
+        if (prim) return q;
+    }
+    return 0;
+}
+u64 cached_primitive(int d) {
+    static std::mutex mu;
+    static u64 cache[33] = {0};
+    std::lock_guard<std::mutex> lk(mu);
+    if (!cache[d]) cache[d] = h_primitive(d);
+    return cache[d];
+}
+u64 h_gcd(u64 a, u64 b) { while (b) { u64 t = a % b; a = b; b = t; } return a; }
+
+}  // namespace
+
+extern "C" {
+
+uint64_t gf2e_primitive_poly(int d) {
+    if (d < 2 || d > 32) return 0;
+    return cached_primitive(d);
+}
+
+int gf2e_sieve_workspace_size(int dmax, size_t *bytes) {
+    if (dmax < 2 || dmax > DMAX || !bytes) return gf2e::invalid("dmax must be in 2..%d", DMAX);
+    *bytes = layout_for(dmax).total;
+    return GF2E_OK;
+}
+
+int gf2e_sieve_fill(uint64_t *best_dev, uint64_t smax, void *stream) {
+    if (!best_dev) return gf2e::invalid("null best");
+    k_fill<<<gf2e::grid_for(smax + 1, 256), 256, 0, (cudaStream_t)stream>>>(
+        (unsigned long long *)best_dev, smax + 1, ~0ull);
+    GF2E_CHECK_LAUNCH("k_fill");
+    return GF2E_OK;
+}
+
+int gf2e_sieve_run(uint64_t r, int dmin, int dmax, uint64_t smax, uint64_t *best_dev,
+                   void *workspace, size_t ws_bytes, void *stream) {
+    if (dmin < 2 || dmax > DMAX || dmin > dmax)
+        return gf2e::invalid("degrees must satisfy 2 <= dmin <= dmax <= %d", DMAX);
+    if (!best_dev || !workspace || smax < 1 || r < 3)
+        return gf2e::invalid("gf2e_sieve_run: bad arguments");
+    Layout lay = layout_for(dmax);
+    if (ws_bytes < lay.total)
+        return gf2e::invalid("sieve workspace %zu < %zu bytes", ws_bytes, lay.total);
+    // host-side checks and setup for every degree before any launch
+    std::vector<DegreeArgs> args;
+    for (int d = dmin; d <= dmax; d++) {
+        DegreeArgs a;
+        memset(&a, 0, sizeof a);
+        a.d = d;
+        a.M = ((u64)1 << d) - 1;
+        a.q = (u32)cached_primitive(d);
+        a.rmod = r % a.M;
+        a.smax = smax;
+        if (h_gcd(a.rmod ? a.rmod : a.M, a.M) != 1) {
+            gf2e::set_error("d=%d: gcd(r, 2^d-1) != 1; unsupported r", d);
+            return GF2E_ERR_UNSUPPORTED_R;
+        }
+        u64 ps[16];
+        int np = h_prime_factors((u64)d, ps);
+        a.nsub = np;
+        for (int i = 0; i < np; i++) a.subq[i] = a.M / (((u64)1 << (d / ps[i])) - 1);
+        args.push_back(a);
+    }
+    cudaStream_t st = (cudaStream_t)stream;
+    char *ws = (char *)workspace;
+    u32 *A = (u32 *)(ws + lay.off_A);
+    u32 *L = (u32 *)(ws + lay.off_L);
+    Prog *strip = (Prog *)(ws + lay.off_strip);
+    Prog *heavy = (Prog *)(ws + lay.off_heavy);
+    Counters *cnt = (Counters *)(ws + lay.off_cnt);
+    cudaError_t e = cudaMemsetAsync(cnt, 0, sizeof(Counters), st);
+    if (e != cudaSuccess) return gf2e::cuda_status(e, "sieve counters");
+    unsigned long long *best = (unsigned long long *)best_dev;
+    for (const DegreeArgs &a : args) {
+        u64 nchunk = (a.M + 31) >> 5;
+        k_tables<<<gf2e::grid_for(nchunk, 256, 16), 256, 0, st>>>(A, L, a.d, a.q, a.M);
+        GF2E_CHECK_LAUNCH("k_tables");
+        k_classes<<<gf2e::grid_for(a.M, 256, 16), 256, 0, st>>>(A, L, a, best, strip, heavy, cnt);
+        GF2E_CHECK_LAUNCH("k_classes");
+    }
+    k_heavy<<<gf2e::sm_count() * 16, 256, 0, st>>>(heavy, cnt, smax, best);
+    GF2E_CHECK_LAUNCH("k_heavy");
+    u64 nstrips = (smax + STRIP) / STRIP;
+    k_strip<<<gf2e::grid_for(nstrips * 512, 512, 2), 512, 0, st>>>(strip, cnt, smax, best);
+    GF2E_CHECK_LAUNCH("k_strip");
+    // status: overflow / internal failures (one small read, synchronizes)
+    unsigned long long flags[4];
+    e = cudaMemcpyAsync(flags, cnt, sizeof flags, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) return gf2e::cuda_status(e, "sieve status");
+    if (flags[2]) {
+        gf2e::set_error("sieve progression list overflow (%llu)", flags[2]);
+        return GF2E_ERR_OVERFLOW;
+    }
+    if (flags[3]) {
+        gf2e::set_error("minimal polynomial consistency failure (%llu classes)", flags[3]);
+        return GF2E_ERR_INTERNAL;
+    }
+    return GF2E_OK;
+}
+
+int gf2e_sieve_stats(const void *workspace, int dmax, uint64_t *classes_host,
+                     uint64_t *marks_host, void *stream) {
+    if (!workspace || dmax < 2 || dmax > DMAX) return gf2e::invalid("gf2e_sieve_stats: bad arguments");
+    Layout lay = layout_for(dmax);
+    Counters c;
+    cudaStream_t st = (cudaStream_t)stream;
+    cudaError_t e = cudaMemcpyAsync(&c, (const char *)workspace + lay.off_cnt, sizeof c,
+                                    cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) return gf2e::cuda_status(e, "sieve stats");
+    for (int d = 0; d <= DMAX; d++) {
+        if (classes_host) classes_host[d] = c.classes[d];
+        if (marks_host) marks_host[d] = c.marks[d];
+    }
+    return GF2E_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,289 @@
+// trinomial.cu -- arithmetic in GF(2)[x]/(x^r + x^s + 1): single-pass
+// squaring (batched over many s), fold reduction of a product, and state
+// initialisation.
+//
+// Squaring, derived for odd r and 1 <= s, 2s < r.  Split the input at
+// h = (r+1)/2: in = A_lo + x^h A_hi.  Then
+//     in^2 = A_lo^2 + x^(r+1) A_hi^2,   x^(r+1) = x^(s+1) + x  (mod T).
+// A_lo^2 has degree <= r-1 and needs no reduction.  With S = A_hi^2 (the
+// bit-spread of A_hi, degree <= r-3):
+//     x*S                      degree <= r-2
+//     x^(s+1)*S = Y_lo + x^r Y_hi,  Y_hi = S >> (r-s-1),  deg Y_hi <= s-2
+//     x^r Y_hi = Y_hi + x^s Y_hi     (degree <= 2s-2 < r, no further fold)
+// so every output word is the XOR of five 64-bit windows:
+//     spread(A_lo)[w] ^ S<<1 ^ (S<<(s+1) mod x^r) ^ S>>(r-s-1)
+//                     ^ (S>>(r-s-1))<<s.
+// A 64-bit window of S starting at bit p is the spread of 32 bits of A_hi
+// starting at ceil(p/2) (shifted left one place when p is odd), i.e. ONE
+// funnel-shifted 32-bit read of the input and one spread per window.  The
+// last two windows are zero outside the first ~2s/64 words and are skipped
+// there.  This is the same identity the reference's fused squaring
+// evaluates as five clipped windows of the virtual spread
+// (tsfactor.cu:128-186); the output is bit-identical.
+#include "gf2e_internal.cuh"
+
+namespace {
+
+// in bits [P, P+32) of a state held as n32 32-bit words (zero beyond)
+GF2E_DEV u32 in_bits32(const u32 *__restrict__ in32, size_t n32, u64 P) {
+    size_t i = (size_t)(P >> 5);
+    unsigned sh = (unsigned)(P & 31);
+    u32 lo = (i < n32) ? __ldg(in32 + i) : 0u;
+    u32 hi = (i + 1 < n32) ? __ldg(in32 + i + 1) : 0u;
+    return __funnelshift_r(lo, hi, sh);
+}
+
+// S bits [p, p+64), S = spread(A_hi), A_hi = in >> h; p may be negative
+GF2E_DEV u64 s_window(const u32 *__restrict__ in32, size_t n32, u64 h, int64_t p) {
+    int64_t j = (p + 1) >> 1;                     // first A_hi index used
+    u32 a;
+    if (j >= 0)
+        a = in_bits32(in32, n32, h + (u64)j);
+    else if (j > -32)
+        a = in_bits32(in32, n32, h) << (unsigned)(-j);
+    else
+        a = 0;
+    u64 v = spread32(a);
+    return (p & 1) ? (v << 1) : v;
+}
+
+// one output word of in^2 mod T
+GF2E_DEV u64 square_word(const u32 *__restrict__ in32, size_t n32, u64 r, u64 h,
+                         u64 s, size_t w) {
+    const u64 b = (u64)w << 6;
+    u64 v = 0;
+    if (32 * (u64)w < h) {                        // spread(A_lo)
+        u32 a = __ldg(in32 + w);
+        u64 valid = h - 32 * (u64)w;
+        if (valid < 32) a &= (1u << valid) - 1u;
+        v = spread32(a);
+    }
+    v ^= s_window(in32, n32, h, (int64_t)b - 1);                   // S<<1
+    u64 t3 = s_window(in32, n32, h, (int64_t)b - (int64_t)s - 1);  // S<<(s+1)
+    if (b + 64 > r) t3 &= low_mask(r - b);
+    v ^= t3;
+    if (b + 1 < s)                                                   // S>>(r-s-1)
+        v ^= s_window(in32, n32, h, (int64_t)(b + r - s - 1));
+    if (b + 64 > s && b + 1 < 2 * s) {                               // (..)<<s
+        u64 t5 = s_window(in32, n32, h, (int64_t)(b + r - 2 * s - 1));
+        if (b < s) t5 &= ~low_mask(s - b);
+        v ^= t5;
+    }
+    return v;
+}
+
+// batched squaring: blockIdx.y = state; each thread writes two words
+__global__ void __launch_bounds__(256)
+k_square_batch(const u64 *__restrict__ in, u64 *__restrict__ out, size_t stride,
+               u64 r, const u64 *__restrict__ s_arr, u64 s_uniform) {
+    const int st = blockIdx.y;
+    const u64 s = s_arr ? s_arr[st] : s_uniform;
+    const size_t nw = (size_t)((r + 63) >> 6);
+    const size_t n32 = 2 * nw;
+    const u64 h = (r + 1) >> 1;
+    const u32 *in32 = reinterpret_cast<const u32 *>(in + (size_t)st * stride);
+    u64 *o = out + (size_t)st * stride;
+    for (size_t w = 2 * ((size_t)blockIdx.x * blockDim.x + threadIdx.x); w < nw;
+         w += 2 * (size_t)gridDim.x * blockDim.x) {
+        u64 v0 = square_word(in32, n32, r, h, s, w);
+        if (w + 1 < nw) {
+            u64 v1 = square_word(in32, n32, r, h, s, w + 1);
+            *reinterpret_cast<ulonglong2 *>(o + w) = make_ulonglong2(v0, v1);
+        } else {
+            o[w] = v0;
+        }
+    }
+}
+
+// P_hi bits [k, k+64) where P_hi = P >> r, P of L bits in pw words; bits of
+// P below r (k < 0) and at or above L are excluded.  Callers pass k >= -s,
+// so the absolute position r + k is never negative.
+GF2E_DEV u64 phi_window(const u64 *__restrict__ P, size_t pw, u64 r, u64 L, int64_t k) {
+    int64_t q = (int64_t)r + k;                   // absolute bit position
+    u64 lo_clip = 0;
+    if (k < 0) {
+        lo_clip = (u64)(-k);
+        if (lo_clip >= 64) return 0;
+    }
+    u64 pos = (u64)q;
+    if (pos >= L) return 0;
+    size_t i = (size_t)(pos >> 6);
+    unsigned sh = (unsigned)(pos & 63);
+    u64 a = (i < pw) ? P[i] : 0;
+    u64 b2 = (i + 1 < pw) ? P[i + 1] : 0;
+    u64 v = funnel64(a, b2, sh);
+    if (L - pos < 64) v &= low_mask(L - pos);
+    if (lo_clip) v &= ~low_mask(lo_clip);
+    return v;
+}
+
+// out = P mod T for a product P of L <= 2r-1 bits (five windows of P_hi)
+__global__ void k_reduce(const u64 *__restrict__ P, size_t pw, u64 L, u64 *__restrict__ out,
+                         u64 r, u64 s) {
+    const size_t nw = (size_t)((r + 63) >> 6);
+    for (size_t w = (size_t)blockIdx.x * blockDim.x + threadIdx.x; w < nw;
+         w += (size_t)gridDim.x * blockDim.x) {
+        const u64 b = (u64)w << 6;
+        u64 v = (w < pw) ? P[w] : 0;                  // P_lo
+        if (b + 64 > r) v &= low_mask(r > b ? r - b : 0);
+        if (b >= L) v = 0;
+        else if (L - b < 64) v &= low_mask(L - b);
+        v ^= phi_window(P, pw, r, L, (int64_t)b);                    // P_hi
+        u64 y = phi_window(P, pw, r, L, (int64_t)b - (int64_t)s);    // P_hi<<s
+        if (b + 64 > r) y &= low_mask(r - b);
+        v ^= y;
+        v ^= phi_window(P, pw, r, L, (int64_t)(b + r - s));          // Q
+        u64 z = phi_window(P, pw, r, L, (int64_t)(b + r) - 2 * (int64_t)s);  // Q<<s
+        if (b < s) z &= (s - b >= 64) ? 0 : ~low_mask(s - b);
+        v ^= z;
+        out[w] = v;
+    }
+}
+
+__global__ void k_set_const(u64 *states, size_t stride, int nstates, size_t nw, u64 w0) {
+    size_t total = (size_t)nstates * stride;
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < total;
+         i += (size_t)gridDim.x * blockDim.x) {
+        size_t w = i % stride;
+        states[i] = (w == 0) ? w0 : 0;
+        (void)nw;
+    }
+}
+
+int check_rs(u64 r, u64 s) {
+    if (r < 5 || !(r & 1))
+        return gf2e::invalid("r must be odd and >= 5 (got %llu)", (unsigned long long)r);
+    if (!(s >= 1 && 2 * s < r))
+        return gf2e::invalid("need 1 <= s <= (r-1)/2 (r=%llu s=%llu)",
+                             (unsigned long long)r, (unsigned long long)s);
+    return GF2E_OK;
+}
+
+int launch_square(const u64 *in, u64 *out, size_t stride, int nstates, u64 r,
+                  const u64 *s_dev, u64 s, cudaStream_t st) {
+    const size_t nw = (size_t)((r + 63) >> 6);
+    const int threads = 256;
+    size_t bx = (nw + 2 * threads - 1) / (2 * threads);
+    if (bx > 65535) bx = 65535;
+    dim3 grid((unsigned)bx, (unsigned)nstates);
+    k_square_batch<<<grid, threads, 0, st>>>(in, out, stride, r, s_dev, s);
+    GF2E_CHECK_LAUNCH("k_square_batch");
+    return GF2E_OK;
+}
+
+}  // namespace
+
+namespace gf2e {
+int trin_reduce(const u64 *P, size_t pw, u64 L, u64 *out, u64 r, u64 s, cudaStream_t st) {
+    const size_t nw = (size_t)((r + 63) >> 6);
+    int threads = 256;
+    k_reduce<<<grid_for(nw, threads), threads, 0, st>>>(P, pw, L, out, r, s);
+    GF2E_CHECK_LAUNCH("k_reduce");
+    return GF2E_OK;
+}
+int trin_square(const u64 *in, u64 *out, u64 r, u64 s, cudaStream_t st) {
+    return launch_square(in, out, (size_t)((r + 63) >> 6), 1, r, nullptr, s, st);
+}
+int trin_set_const(u64 *states, size_t stride, int nstates, u64 r, u64 w0, cudaStream_t st) {
+    const size_t nw = (size_t)((r + 63) >> 6);
+    size_t total = (size_t)nstates * stride;
+    int threads = 256;
+    k_set_const<<<grid_for(total, threads), threads, 0, st>>>(states, stride, nstates, nw, w0);
+    GF2E_CHECK_LAUNCH("k_set_const");
+    return GF2E_OK;
+}
+}  // namespace gf2e
+
+extern "C" {
+
+int gf2e_trin_square(const uint64_t *in_dev, uint64_t *out_dev, uint64_t r, uint64_t s,
+                     void *stream) {
+    GF2E_TRY(check_rs(r, s));
+    if (!in_dev || !out_dev || in_dev == out_dev)
+        return gf2e::invalid("gf2e_trin_square: need distinct non-null buffers");
+    return gf2e::trin_square(in_dev, out_dev, r, s, (cudaStream_t)stream);
+}
+
+int gf2e_trin_square_batch(uint64_t *states_dev, uint64_t *scratch_dev, size_t stride_words,
+                           int nstates, uint64_t r, const uint64_t *s_dev, uint32_t k,
+                           void *stream) {
+    GF2E_TRY(check_rs(r, 1));
+    const size_t nw = (size_t)((r + 63) >> 6);
+    if (!states_dev || !scratch_dev || !s_dev || nstates < 1 || nstates > 65535)
+        return gf2e::invalid("gf2e_trin_square_batch: bad buffers or nstates=%d", nstates);
+    if (stride_words < nw || (stride_words & 1))
+        return gf2e::invalid("stride_words must be even and >= ceil(r/64)");
+    cudaStream_t st = (cudaStream_t)stream;
+    u64 *a = states_dev, *b = scratch_dev;
+    for (uint32_t i = 0; i < k; i++) {
+        GF2E_TRY(launch_square(a, b, stride_words, nstates, r, s_dev, 0, st));
+        u64 *t = a; a = b; b = t;
+    }
+    if (a != states_dev) {
+        cudaError_t e = cudaMemcpyAsync(states_dev, a, (size_t)nstates * stride_words * 8,
+                                        cudaMemcpyDeviceToDevice, st);
+        if (e != cudaSuccess) return gf2e::cuda_status(e, "square_batch copy-back");
+    }
+    return GF2E_OK;
+}
+
+int gf2e_trin_set_x(uint64_t *states_dev, size_t stride_words, int nstates, uint64_t r,
+                    void *stream) {
+    if (!states_dev || nstates < 1 || stride_words < (size_t)((r + 63) >> 6) || r < 2)
+        return gf2e::invalid("gf2e_trin_set_x: bad arguments");
+    return gf2e::trin_set_const(states_dev, stride_words, nstates, r, 2, (cudaStream_t)stream);
+}
+
+int gf2e_trin_set_one(uint64_t *states_dev, size_t stride_words, int nstates, uint64_t r,
+                      void *stream) {
+    if (!states_dev || nstates < 1 || stride_words < (size_t)((r + 63) >> 6) || r < 1)
+        return gf2e::invalid("gf2e_trin_set_one: bad arguments");
+    return gf2e::trin_set_const(states_dev, stride_words, nstates, r, 1, (cudaStream_t)stream);
+}
+
+int gf2e_trin_frobenius_host(uint64_t r, const uint64_t *s_host, int nstates, uint32_t k,
+                             uint64_t *out_host, size_t out_stride_words, void *stream) {
+    GF2E_TRY(check_rs(r, 1));
+    const size_t nw = (size_t)((r + 63) >> 6);
+    if (!s_host || !out_host || nstates < 1 || nstates > 65535 || out_stride_words < nw)
+        return gf2e::invalid("gf2e_trin_frobenius_host: bad arguments");
+    for (int i = 0; i < nstates; i++) GF2E_TRY(check_rs(r, s_host[i]));
+    cudaStream_t st = (cudaStream_t)stream;
+    const size_t stride = nw + (nw & 1);
+    const size_t need = 2 * stride * (size_t)nstates * 8 + (size_t)nstates * 8;
+    // per-thread device workspace, grown on demand and kept between calls
+    static thread_local u64 *ws = nullptr;
+    static thread_local size_t ws_bytes = 0;
+    static thread_local int ws_dev = -1;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (ws_bytes < need || ws_dev != dev) {
+        if (ws && ws_dev == dev) cudaFree(ws);
+        ws = nullptr;
+        ws_bytes = 0;
+        cudaError_t e = cudaMalloc(&ws, need);
+        if (e != cudaSuccess) return gf2e::cuda_status(e, "frobenius workspace");
+        ws_bytes = need;
+        ws_dev = dev;
+    }
+    u64 *states = ws, *scratch = ws + stride * nstates, *sdev = scratch + stride * nstates;
+    cudaError_t e = cudaMemcpyAsync(sdev, s_host, (size_t)nstates * 8, cudaMemcpyHostToDevice, st);
+    if (e != cudaSuccess) return gf2e::cuda_status(e, "frobenius s upload");
+    GF2E_TRY(gf2e::trin_set_const(states, stride, nstates, r, 2, st));
+    GF2E_TRY(gf2e_trin_square_batch(states, scratch, stride, nstates, r, sdev, k, stream));
+    e = cudaMemcpy2DAsync(out_host, out_stride_words * 8, states, stride * 8, nw * 8,
+                          (size_t)nstates, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    return gf2e::cuda_status(e, "frobenius readback");
+}
+
+int gf2e_trin_reduce(const uint64_t *prod_dev, uint64_t prod_bits, uint64_t *out_dev,
+                     uint64_t r, uint64_t s, void *stream) {
+    GF2E_TRY(check_rs(r, s));
+    if (!prod_dev || !out_dev || prod_bits > 2 * r - 1)
+        return gf2e::invalid("gf2e_trin_reduce: need prod_bits <= 2r-1");
+    size_t pw = (size_t)((prod_bits + 63) >> 6);
+    return gf2e::trin_reduce(prod_dev, pw, prod_bits, out_dev, r, s, (cudaStream_t)stream);
+}
+
+}  // extern "C"
