@@ -1,0 +1,72 @@
+"""Small, self-contained launches of each hot kernel, sized for a profiler
+capture (inputs larger than L2, a few GB at most, a handful of launches).
+
+    python -m mersenne_trinomial_b200.profile_cases square [--r R] [--n N] [--k K]
+    python -m mersenne_trinomial_b200.profile_cases fft [--m M]
+    python -m mersenne_trinomial_b200.profile_cases sieve [--r R] [--depth D]
+    python -m mersenne_trinomial_b200.profile_cases mul [--m M]
+"""
+from __future__ import annotations
+
+import argparse
+import sys
+import time
+
+import numpy as np
+
+import mersenne_trinomial_b200 as M
+from mersenne_trinomial_b200 import workloads as W
+
+
+def case_square(a):
+    r, n, k = a.r, a.n, a.k
+    nw = (r + 63) // 64
+    stride = nw + (nw & 1)
+    st = M.DeviceBuffer(8 * stride * n)
+    sc = M.DeviceBuffer(st.nbytes)
+    rng = np.random.default_rng(3)
+    s = rng.integers(3, r // 2, size=n).astype(np.uint64)
+    M.trin_set_x(st, stride, n, r)
+    M.trin_square_batch(st, sc, stride, n, r, M.DeviceBuffer.from_array(s), k)
+    M.stream_sync()
+
+
+def case_fft(a):
+    m = a.m
+    F = M.CudaFFT()
+    F.init(m)
+    d = M.DeviceBuffer.from_array(W.splitmix64(5, 1 << m))
+    F.fwd(d)
+    F.inv(d)
+    M.stream_sync()
+
+
+def case_mul(a):
+    bits = 1 << (a.m + 4)
+    x = W.random_bits(bits, 1)
+    y = W.random_bits(bits, 2)
+    M.gf2x_fft_mul(x, bits, y, bits)
+
+
+def case_sieve(a):
+    smax = a.r // 2
+    M.run_sieve(a.r, a.depth, smax)
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser()
+    ap.add_argument("case", choices=["square", "fft", "mul", "sieve"])
+    ap.add_argument("--r", type=int, default=136279841)
+    ap.add_argument("--n", type=int, default=8)
+    ap.add_argument("--k", type=int, default=3)
+    ap.add_argument("--m", type=int, default=22)
+    ap.add_argument("--depth", type=int, default=24)
+    a = ap.parse_args(argv)
+    t0 = time.perf_counter()
+    {"square": case_square, "fft": case_fft, "mul": case_mul, "sieve": case_sieve}[a.case](a)
+    print(f"{a.case}: done in {time.perf_counter() - t0:.3f} s")
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())
