@@ -76,14 +76,26 @@ k_fft_pass(u64 *__restrict__ f, const u64 *__restrict__ tab, const Pass P, u64 n
             u64 win = tile / cgroups, cg = tile - win * cgroups;
             base = win * ((u64)NS * P.CH) + cg * C;
         }
-        // load
-        for (u32 e = threadIdx.x; e < tile_elems; e += FFT_THREADS) {
-            u32 row = e >> P.c_log, col = e & (C - 1);
-            u64 g = base + (u64)row * P.CH + col;
-            u64 v;
-            if (src32) v = (g < nchunks) ? (u64)__ldg(src32 + g) : 0ull;
-            else v = f[g];
-            sm[e] = v;
+        // load: every thread issues all of its loads before the first use
+        {
+            constexpr int EPT = TILE / FFT_THREADS;
+            u64 v[EPT];
+#pragma unroll
+            for (int j = 0; j < EPT; j++) {
+                u32 e = threadIdx.x + j * FFT_THREADS;
+                v[j] = 0;
+                if (e < tile_elems) {
+                    u32 row = e >> P.c_log, col = e & (C - 1);
+                    u64 g = base + (u64)row * P.CH + col;
+                    if (src32) v[j] = (g < nchunks) ? (u64)__ldg(src32 + g) : 0ull;
+                    else v[j] = f[g];
+                }
+            }
+#pragma unroll
+            for (int j = 0; j < EPT; j++) {
+                u32 e = threadIdx.x + j * FFT_THREADS;
+                if (e < tile_elems) sm[e] = v[j];
+            }
         }
         __syncthreads();
         for (u32 k = 0; k < P.nops; k++) {

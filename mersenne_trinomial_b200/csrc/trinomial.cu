@@ -72,25 +72,91 @@ GF2E_DEV u64 square_word(const u32 *__restrict__ in32, size_t n32, u64 r, u64 h,
     return v;
 }
 
-// batched squaring: blockIdx.y = state; each thread writes two words
-__global__ void __launch_bounds__(256)
+// Four consecutive output words, one window: XOR the 32-bit input windows
+// starting at in32[b + q] bit `sh` (q = 0..3) into acc.  Five coalesced
+// 32-bit loads serve four words.
+template <bool GUARD>
+GF2E_DEV void window4(const u32 *__restrict__ in32, u32 n32, u32 b, u32 sh, u32 (&acc)[4]) {
+    u32 x[5];
+#pragma unroll
+    for (int q = 0; q < 5; q++) x[q] = (!GUARD || b + q < n32) ? __ldg(in32 + b + q) : 0u;
+#pragma unroll
+    for (int q = 0; q < 4; q++) acc[q] ^= __funnelshift_r(x[q], x[q + 1], sh);
+}
+
+// batched squaring: blockIdx.y = state; each thread writes four words.
+//
+// Every window is a spread of 32 input bits placed on the even bit
+// positions (window offset even) or on the odd ones (offset odd), and the
+// spread is linear over XOR.  So a clean group XORs the 32-bit inputs of
+// all even windows into E and of all odd windows into O and writes
+//     out = spread(E) ^ (spread(O) << 1):
+// two spreads per output word however many windows are active.  Parities:
+// spread(A_lo) and the last window are even, S<<1 is odd, the two middle
+// windows are odd/even or even/odd with the parity of s.
+// Groups of four words away from every window boundary take this path
+// (32-bit index arithmetic, hoisted offsets, no clipping); the few groups
+// that touch a boundary use the clipped per-word form above.
+template <bool SODD>
+GF2E_DEV void square_group_fast(const u32 *__restrict__ in32, u32 n32, u32 w0, bool t1_on,
+                                bool t3_on, bool t4_on, bool t5_on, u32 K2, u32 K3, u32 K4, u32 K5,
+                                u64 *__restrict__ o) {
+    u32 E[4] = {0, 0, 0, 0}, O[4] = {0, 0, 0, 0};
+    if (t1_on) {
+        uint4 a = __ldg(reinterpret_cast<const uint4 *>(in32 + w0));
+        E[0] = a.x; E[1] = a.y; E[2] = a.z; E[3] = a.w;
+    }
+    window4<false>(in32, n32, w0 + (K2 >> 5), K2 & 31, O);
+    if (t3_on) window4<false>(in32, n32, w0 + (K3 >> 5), K3 & 31, SODD ? E : O);
+    if (t4_on) window4<true>(in32, n32, w0 + (K4 >> 5), K4 & 31, SODD ? O : E);
+    if (t5_on) window4<true>(in32, n32, w0 + (K5 >> 5), K5 & 31, E);
+    u64 v[4];
+#pragma unroll
+    for (int q = 0; q < 4; q++) v[q] = spread32(E[q]) ^ (spread32(O[q]) << 1);
+    reinterpret_cast<ulonglong2 *>(o + w0)[0] = make_ulonglong2(v[0], v[1]);
+    reinterpret_cast<ulonglong2 *>(o + w0)[1] = make_ulonglong2(v[2], v[3]);
+}
+
+__global__ void __launch_bounds__(256, 4)
 k_square_batch(const u64 *__restrict__ in, u64 *__restrict__ out, size_t stride,
                u64 r, const u64 *__restrict__ s_arr, u64 s_uniform) {
     const int st = blockIdx.y;
     const u64 s = s_arr ? s_arr[st] : s_uniform;
-    const size_t nw = (size_t)((r + 63) >> 6);
-    const size_t n32 = 2 * nw;
+    const u32 nw = (u32)((r + 63) >> 6);
+    const u32 n32 = 2 * nw;
     const u64 h = (r + 1) >> 1;
     const u32 *in32 = reinterpret_cast<const u32 *>(in + (size_t)st * stride);
     u64 *o = out + (size_t)st * stride;
-    for (size_t w = 2 * ((size_t)blockIdx.x * blockDim.x + threadIdx.x); w < nw;
-         w += 2 * (size_t)gridDim.x * blockDim.x) {
-        u64 v0 = square_word(in32, n32, r, h, s, w);
-        if (w + 1 < nw) {
-            u64 v1 = square_word(in32, n32, r, h, s, w + 1);
-            *reinterpret_cast<ulonglong2 *>(o + w) = make_ulonglong2(v0, v1);
+    // window geometry: input bit position of word w's window is 32w + K
+    const u32 K2 = (u32)h;                                 // S << 1
+    const u32 K3 = (u32)(h - ((s + 1) >> 1));              // S << (s+1)
+    const u32 K4 = (u32)(h + ((r - s) >> 1));              // S >> (r-s-1)
+    const u32 K5 = (u32)(h + ((r - 2 * s) >> 1));          // (S >> (r-s-1)) << s
+    const bool sodd = (s & 1) != 0;
+    const u32 ngroups = (nw + 3) >> 2;
+    for (u32 g = blockIdx.x * blockDim.x + threadIdx.x; g < ngroups;
+         g += gridDim.x * blockDim.x) {
+        const u32 w0 = 4 * g;
+        const u64 b0 = (u64)w0 << 6, b3 = b0 + 192;
+        const bool t1_on = 32 * (u64)(w0 + 4) <= h, t1_off = 32 * (u64)w0 >= h;
+        const bool t4_on = b3 + 1 < s, t4_off = b0 + 1 >= s;
+        const bool t5_on = b0 >= s && b3 + 1 < 2 * s;
+        const bool t5_off = b3 + 64 <= s || b0 + 1 >= 2 * s;
+        // S<<(s+1): whole windows above bit 0 of S, or entirely below it (zero)
+        const bool t3_on = 32 * (u64)w0 >= ((s + 1) >> 1);
+        const bool t3_off = b3 + 64 <= s + 1;
+        const bool clean = (w0 + 5 <= nw) && (t1_on || t1_off) && (t3_on || t3_off) &&
+                           (t4_on || t4_off) && (t5_on || t5_off) && r < (1ull << 31);
+        if (clean) {
+            if (sodd)
+                square_group_fast<true>(in32, n32, w0, t1_on, t3_on, t4_on, t5_on, K2, K3, K4,
+                                        K5, o);
+            else
+                square_group_fast<false>(in32, n32, w0, t1_on, t3_on, t4_on, t5_on, K2, K3, K4,
+                                         K5, o);
         } else {
-            o[w] = v0;
+            for (u32 w = w0; w < w0 + 4 && w < nw; w++)
+                o[w] = square_word(in32, n32, r, h, s, w);
         }
     }
 }
