@@ -166,6 +166,24 @@ int gf2e_mul(const gf2e_fft_plan *plan, const uint64_t *a_dev, uint64_t abits,
              const uint64_t *b_dev, uint64_t bbits, uint64_t *out_dev,
              uint64_t *fa_dev, uint64_t *fb_dev, void *stream);
 
+/* The same product with no memory allocated by the call: no counterpart in
+ * the reference.  For callers that cannot allocate device memory while they
+ * run (an HBM budget fixed at start-up, or a loop that must not let an
+ * allocator call synchronise the device).  The transform scratch and
+ * twiddle tables are fixed arrays inside the library, sized for transforms
+ * of at most 2^GF2E_MUL_NOALLOC_MAX_M points, i.e.
+ * ceil(abits/32) + ceil(bbits/32) - 1 <= 2^18; larger products return
+ * GF2E_ERR_INVALID.  Every GPU that loads the library holds the 4 MiB of
+ * scratch until the process exits.  The first call on a device sets up that
+ * device (symbol addresses, twiddle upload, pass schedules) and should come
+ * before any stream capture.  All calls share the scratch, which keeps the
+ * last call's contents (nothing is read from it before being written): calls
+ * that overlap on the GPU, e.g. on two streams, race.  a_dev, b_dev and
+ * out_dev (gf2e_mul_out_words words) are the caller's device buffers. */
+#define GF2E_MUL_NOALLOC_MAX_M 18
+int gf2e_mul_noalloc(const uint64_t *a_dev, uint64_t abits, const uint64_t *b_dev,
+                     uint64_t bbits, uint64_t *out_dev, void *stream);
+
 /* One product in a batch (config: many uneven products in one call). */
 typedef struct gf2e_mul_job {
     const uint64_t *a_dev;

@@ -74,6 +74,7 @@ SIGNATURES = {
     "gf2e_mul_fft_m": (_i32, [_u64, _u64]),
     "gf2e_mul_out_words": (_sz, [_u64, _u64]),
     "gf2e_mul": (_i32, [_vp, _vp, _u64, _vp, _u64, _vp, _vp, _vp, _vp]),
+    "gf2e_mul_noalloc": (_i32, [_vp, _u64, _vp, _u64, _vp, _vp]),
     "gf2e_mul_batch_workspace_size": (_i32, [_P(MulJob), _i32, _P(_sz)]),
     "gf2e_mul_batch": (_i32, [_P(MulJob), _i32, _vp, _sz, _vp]),
     "gf2e_trin_create": (_i32, [_u64, _P(_vp)]),

@@ -256,7 +256,8 @@ Pass make_pass(u64 CH, u64 NS, u32 C, u64 n) {
 struct PlanImpl {
     int m = 0;
     u64 n = 0;
-    u64 *d_tab = nullptr;                // NTWTAB x 256 twiddle byte tables
+    u64 *d_tab = nullptr;                // owned NTWTAB x 256 twiddle byte tables
+    const u64 *tab = nullptr;            // tables the passes read (d_tab or caller's)
     std::vector<Pass> fwd, inv;
     std::vector<u64> ntiles_fwd, ntiles_inv;
 };
@@ -365,7 +366,7 @@ int run_passes(const PlanImpl &P, bool forward, u64 *f, const u32 *src32, u64 nc
         u64 elems = (u64)1 << (ps[i].ns_log + ps[i].c_log + ps[i].wpt_log);
         size_t smem = elems * sizeof(u64);
         int grid = (int)std::min<u64>(nt[i], (u64)gf2e::sm_count() * 8);
-        k_fft_pass<<<grid, FFT_THREADS, smem, st>>>(f, P.d_tab, ps[i], nt[i],
+        k_fft_pass<<<grid, FFT_THREADS, smem, st>>>(f, P.tab, ps[i], nt[i],
                                                     (i == 0) ? src32 : nullptr, nchunks);
         GF2E_CHECK_LAUNCH("k_fft_pass");
     }
@@ -380,20 +381,9 @@ struct gf2e_fft_plan {
 
 namespace gf2e {
 
-int fft_plan_create(int m, gf2e_fft_plan **out) {
-    if (m < 1 || m > 30) return invalid("FFT size exponent m=%d outside 1..30", m);
+// the four 256-entry byte tables of W[t] (W is GF(2)-linear in t)
+void twiddle_byte_tables(u64 *tab) {
     const u64 *b = basis_host();
-    if (!b) return invalid("Cantor basis construction failed");
-    static bool attr_done = false;
-    if (!attr_done) {
-        cudaFuncSetAttribute(k_fft_pass, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             TILE * (int)sizeof(u64));
-        attr_done = true;
-    }
-    gf2e_fft_plan *p = new gf2e_fft_plan;
-    p->impl.m = m;
-    p->impl.n = (u64)1 << m;
-    std::vector<u64> tab(NTWTAB * 256, 0);
     for (int k = 0; k < NTWTAB; k++)
         for (int v = 0; v < 256; v++) {
             u64 w = 0;
@@ -401,16 +391,53 @@ int fft_plan_create(int m, gf2e_fft_plan **out) {
                 if ((v >> j) & 1) w ^= b[8 * k + j + 1 < 64 ? 8 * k + j + 1 : 63];
             tab[k * 256 + v] = w;
         }
-    cudaError_t e = cudaMalloc(&p->impl.d_tab, tab.size() * sizeof(u64));
-    if (e == cudaSuccess)
-        e = cudaMemcpy(p->impl.d_tab, tab.data(), tab.size() * sizeof(u64), cudaMemcpyHostToDevice);
-    if (e != cudaSuccess) {
-        cudaFree(p->impl.d_tab);
-        delete p;
-        return cuda_status(e, "fft plan twiddle tables");
+}
+
+int twiddle_table_words() { return NTWTAB * 256; }
+
+static int allow_tile_smem() {
+    static bool done[64] = {false};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev >= 0 && dev < 64 && !done[dev]) {
+        cudaError_t e = cudaFuncSetAttribute(k_fft_pass, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             TILE * (int)sizeof(u64));
+        if (e != cudaSuccess) return cuda_status(e, "k_fft_pass smem attribute");
+        done[dev] = true;
     }
+    return GF2E_OK;
+}
+
+// plan whose passes read the caller's twiddle tables; no device allocation
+int fft_plan_create_tables(int m, const u64 *tab_dev, gf2e_fft_plan **out) {
+    if (m < 1 || m > 30) return invalid("FFT size exponent m=%d outside 1..30", m);
+    if (!basis_host()) return invalid("Cantor basis construction failed");
+    GF2E_TRY(allow_tile_smem());
+    gf2e_fft_plan *p = new gf2e_fft_plan;
+    p->impl.m = m;
+    p->impl.n = (u64)1 << m;
+    p->impl.tab = tab_dev;
     build_passes(p->impl);
     *out = p;
+    return GF2E_OK;
+}
+
+int fft_plan_create(int m, gf2e_fft_plan **out) {
+    if (m < 1 || m > 30) return invalid("FFT size exponent m=%d outside 1..30", m);
+    if (!basis_host()) return invalid("Cantor basis construction failed");
+    std::vector<u64> tab(NTWTAB * 256, 0);
+    twiddle_byte_tables(tab.data());
+    u64 *d_tab = nullptr;
+    cudaError_t e = cudaMalloc(&d_tab, tab.size() * sizeof(u64));
+    if (e == cudaSuccess)
+        e = cudaMemcpy(d_tab, tab.data(), tab.size() * sizeof(u64), cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) {
+        cudaFree(d_tab);
+        return cuda_status(e, "fft plan twiddle tables");
+    }
+    int st = fft_plan_create_tables(m, d_tab, out);
+    if (st != GF2E_OK) { cudaFree(d_tab); return st; }
+    (*out)->impl.d_tab = d_tab;
     return GF2E_OK;
 }
 
