@@ -203,6 +203,28 @@ int gf2e_mul_batch(const gf2e_mul_job *jobs_host, int njobs, void *workspace_dev
                    size_t workspace_bytes, void *stream);
 
 /* ======================================================================
+ * (d) gcd over GF(2)[x], batched, one GPU thread block per pair.
+ * Replaces the CPU gcd of the interval accumulator (trinomial_scan.cu:64-141
+ * GcdPool; gf2_gcd.h:48-75 poly_gcd_naive, same return convention: deg(gcd),
+ * 0 for gcd = 1 and for gcd(0, 0)).
+ * ====================================================================== */
+typedef struct gf2e_gcd_job {
+    const uint64_t *a_dev;   /* operands, ceil(bits/64) words, not modified */
+    uint64_t abits;
+    const uint64_t *b_dev;
+    uint64_t bbits;
+    uint64_t *g_dev;         /* receives the gcd if it fits g_cap_words (or NULL) */
+    size_t g_cap_words;
+} gf2e_gcd_job;
+
+int gf2e_gcd_workspace_size(const gf2e_gcd_job *jobs_host, int njobs, size_t *bytes);
+/* deg_host[i] = deg gcd(a_i, b_i).  Returns after the results are on the host;
+ * GF2E_ERR_TIMEOUT if a job exceeded its round bound (cannot happen for
+ * valid inputs; reported instead of looping). */
+int gf2e_gcd_batch(const gf2e_gcd_job *jobs_host, int njobs, int64_t *deg_host,
+                   void *workspace_dev, size_t workspace_bytes, void *stream);
+
+/* ======================================================================
  * TrinGPU context (gf2_trinomial_cuda.h:87-178): F (dA), ACC (dACC),
  * product scratch and an FFT plan for r-bit x r-bit products.
  * ====================================================================== */

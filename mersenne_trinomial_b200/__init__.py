@@ -5,13 +5,13 @@ from ._lib import Gf2eError, lib  # noqa: F401
 from .engine import (  # noqa: F401
     CantorBasis, CudaFFT, DeviceBuffer, TrinGPU, bits_to_words, cert_lines, fmt_line,
     gf2x_fft_mul, gf2x_fft_mul_dev, mul_batch_dev, mul_out_words, primitive_poly, run_sieve,
-    sieve_device, spread32, stream_sync, frobenius_host, trin_reduce, trin_set_one, trin_set_x, trin_square,
+    sieve_device, spread32, stream_sync, frobenius_host, gcd_batch, trin_reduce, trin_set_one, trin_set_x, trin_square,
     trin_square_batch,
 )
 
 __all__ = [
     "Gf2eError", "lib", "CantorBasis", "CudaFFT", "DeviceBuffer", "TrinGPU", "bits_to_words",
     "cert_lines", "fmt_line", "gf2x_fft_mul", "gf2x_fft_mul_dev", "mul_batch_dev",
-    "mul_out_words", "primitive_poly", "run_sieve", "sieve_device", "spread32", "stream_sync", "frobenius_host", "trin_reduce",
+    "mul_out_words", "primitive_poly", "run_sieve", "sieve_device", "spread32", "stream_sync", "frobenius_host", "gcd_batch", "trin_reduce",
     "trin_set_one", "trin_set_x", "trin_square", "trin_square_batch",
 ]

@@ -32,6 +32,11 @@ class Gf2eError(RuntimeError):
         self.detail = detail
 
 
+class GcdJob(C.Structure):
+    _fields_ = [("a_dev", C.c_void_p), ("abits", C.c_uint64), ("b_dev", C.c_void_p),
+                ("bbits", C.c_uint64), ("g_dev", C.c_void_p), ("g_cap_words", C.c_size_t)]
+
+
 class MulJob(C.Structure):
     _fields_ = [("a_dev", C.c_void_p), ("abits", C.c_uint64), ("b_dev", C.c_void_p),
                 ("bbits", C.c_uint64), ("out_dev", C.c_void_p)]
@@ -77,6 +82,8 @@ SIGNATURES = {
     "gf2e_mul_noalloc": (_i32, [_vp, _u64, _vp, _u64, _vp, _vp]),
     "gf2e_mul_batch_workspace_size": (_i32, [_P(MulJob), _i32, _P(_sz)]),
     "gf2e_mul_batch": (_i32, [_P(MulJob), _i32, _vp, _sz, _vp]),
+    "gf2e_gcd_workspace_size": (_i32, [_P(GcdJob), _i32, _P(_sz)]),
+    "gf2e_gcd_batch": (_i32, [_P(GcdJob), _i32, _vp, _vp, _sz, _vp]),
     "gf2e_trin_create": (_i32, [_u64, _P(_vp)]),
     "gf2e_trin_destroy": (_i32, [_vp]),
     "gf2e_trin_set_s": (_i32, [_vp, _u64]),

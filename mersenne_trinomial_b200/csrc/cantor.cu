@@ -55,13 +55,24 @@ GF2E_DEV u64 twiddle(const u64 *__restrict__ tab, u64 t) {
     return w;
 }
 
+// Batch description for one pass: blockIdx.y selects the transform
+// (f + y*fstride) and its operand (src32 + y*sstride32).  xor0 is XORed into
+// chunk 0 of every packed operand (the running product multiplies by F + x).
+struct Batch {
+    u64 fstride;
+    u64 sstride32;
+    u64 xor0;
+};
+
 // One pass over all tiles.  src32/nchunks: when non-null the tile is loaded
 // from 32-bit chunks of an operand (packing fused into the first pass),
 // zero beyond nchunks.
 __global__ void __launch_bounds__(FFT_THREADS)
 k_fft_pass(u64 *__restrict__ f, const u64 *__restrict__ tab, const Pass P, u64 ntiles,
-           const u32 *__restrict__ src32, u64 nchunks) {
+           const u32 *__restrict__ src32, u64 nchunks, const Batch bt) {
     extern __shared__ u64 sm[];
+    f += (u64)blockIdx.y * bt.fstride;
+    if (src32) src32 += (u64)blockIdx.y * bt.sstride32;
     const u32 C = 1u << P.c_log;
     const u32 NS = 1u << P.ns_log;
     const u32 rows_total = NS << P.wpt_log;          // rows in the tile (all windows)
@@ -87,8 +98,12 @@ k_fft_pass(u64 *__restrict__ f, const u64 *__restrict__ tab, const Pass P, u64 n
                 if (e < tile_elems) {
                     u32 row = e >> P.c_log, col = e & (C - 1);
                     u64 g = base + (u64)row * P.CH + col;
-                    if (src32) v[j] = (g < nchunks) ? (u64)__ldg(src32 + g) : 0ull;
-                    else v[j] = f[g];
+                    if (src32) {
+                        v[j] = (g < nchunks) ? (u64)__ldg(src32 + g) : 0ull;
+                        if (g == 0) v[j] ^= bt.xor0;
+                    } else {
+                        v[j] = f[g];
+                    }
                 }
             }
 #pragma unroll
@@ -161,9 +176,12 @@ __global__ void k_pointwise(u64 *__restrict__ fa, const u64 *__restrict__ fb, u6
         fa[k] = gf64_mul(fa[k], fb[k]);
 }
 
-// gather-form overlap-add of 64-bit coefficients at 32-bit stride
+// gather-form overlap-add of 64-bit coefficients at 32-bit stride;
+// blockIdx.y selects F + y*fstride -> out + y*ostride
 __global__ void k_overlap_add(const u64 *__restrict__ F, u64 nchunks, u64 *__restrict__ out,
-                              u64 ow) {
+                              u64 ow, u64 fstride = 0, u64 ostride = 0) {
+    F += (u64)blockIdx.y * fstride;
+    out += (u64)blockIdx.y * ostride;
     for (u64 w = (u64)blockIdx.x * blockDim.x + threadIdx.x; w < ow;
          w += (u64)gridDim.x * blockDim.x) {
         u64 k = 2 * w, v = 0;
@@ -359,15 +377,16 @@ void build_passes(PlanImpl &P) {
 }
 
 int run_passes(const PlanImpl &P, bool forward, u64 *f, const u32 *src32, u64 nchunks,
-               cudaStream_t st) {
+               cudaStream_t st, int batch = 1, Batch bt = Batch{0, 0, 0}) {
     const auto &ps = forward ? P.fwd : P.inv;
     const auto &nt = forward ? P.ntiles_fwd : P.ntiles_inv;
     for (size_t i = 0; i < ps.size(); i++) {
         u64 elems = (u64)1 << (ps[i].ns_log + ps[i].c_log + ps[i].wpt_log);
         size_t smem = elems * sizeof(u64);
-        int grid = (int)std::min<u64>(nt[i], (u64)gf2e::sm_count() * 8);
+        u64 per = std::max<u64>(1, (u64)gf2e::sm_count() * 8 / (u64)batch);
+        dim3 grid((unsigned)std::min<u64>(nt[i], per), (unsigned)batch);
         k_fft_pass<<<grid, FFT_THREADS, smem, st>>>(f, P.tab, ps[i], nt[i],
-                                                    (i == 0) ? src32 : nullptr, nchunks);
+                                                    (i == 0) ? src32 : nullptr, nchunks, bt);
         GF2E_CHECK_LAUNCH("k_fft_pass");
     }
     return GF2E_OK;
@@ -450,6 +469,21 @@ int fft_run(const gf2e_fft_plan *plan, bool forward, u64 *f, cudaStream_t st) {
     return run_passes(plan->impl, forward, f, nullptr, 0, st);
 }
 
+// `batch` transforms in one launch per pass: transform y at f + y*fstride,
+// packed from src32 + y*sstride32 (chunk 0 XORed with xor0)
+int fft_fwd_packed_batch(const gf2e_fft_plan *plan, u64 *f, u64 fstride, const u32 *src32,
+                         u64 sstride32, u64 nchunks, u64 xor0, int batch, cudaStream_t st) {
+    return run_passes(plan->impl, true, f, src32, nchunks, st, batch,
+                      Batch{fstride, sstride32, xor0});
+}
+
+int fft_run_batch(const gf2e_fft_plan *plan, bool forward, u64 *f, u64 fstride, int batch,
+                  cudaStream_t st) {
+    return run_passes(plan->impl, forward, f, nullptr, 0, st, batch, Batch{fstride, 0, 0});
+}
+
+u64 fft_plan_n(const gf2e_fft_plan *plan) { return plan->impl.n; }
+
 int pointwise(u64 *fa, const u64 *fb, u64 n, cudaStream_t st) {
     k_pointwise<<<grid_for(n, 256), 256, 0, st>>>(fa, fb, n);
     GF2E_CHECK_LAUNCH("k_pointwise");
@@ -459,6 +493,14 @@ int pointwise(u64 *fa, const u64 *fb, u64 n, cudaStream_t st) {
 int overlap_add(const u64 *F, u64 nchunks, u64 *out, u64 ow, cudaStream_t st) {
     k_overlap_add<<<grid_for(ow, 256), 256, 0, st>>>(F, nchunks, out, ow);
     GF2E_CHECK_LAUNCH("k_overlap_add");
+    return GF2E_OK;
+}
+
+int overlap_add_batch(const u64 *F, u64 fstride, u64 nchunks, u64 *out, u64 ostride, u64 ow,
+                      int batch, cudaStream_t st) {
+    int per = std::max(1, grid_for(ow, 256) / batch);
+    k_overlap_add<<<dim3(per, batch), 256, 0, st>>>(F, nchunks, out, ow, fstride, ostride);
+    GF2E_CHECK_LAUNCH("k_overlap_add batch");
     return GF2E_OK;
 }
 

@@ -22,6 +22,8 @@
 // (tsfactor.cu:128-186); the output is bit-identical.
 #include "gf2e_internal.cuh"
 
+#include <algorithm>
+
 namespace {
 
 // in bits [P, P+32) of a state held as n32 32-bit words (zero beyond)
@@ -183,9 +185,14 @@ GF2E_DEV u64 phi_window(const u64 *__restrict__ P, size_t pw, u64 r, u64 L, int6
     return v;
 }
 
-// out = P mod T for a product P of L <= 2r-1 bits (five windows of P_hi)
+// out = P mod T for a product P of L <= 2r-1 bits (five windows of P_hi).
+// Batched: blockIdx.y selects P + y*pstride, out + y*ostride and s_arr[y].
 __global__ void k_reduce(const u64 *__restrict__ P, size_t pw, u64 L, u64 *__restrict__ out,
-                         u64 r, u64 s) {
+                         u64 r, u64 s, size_t pstride = 0, size_t ostride = 0,
+                         const u64 *__restrict__ s_arr = nullptr) {
+    P += (size_t)blockIdx.y * pstride;
+    out += (size_t)blockIdx.y * ostride;
+    if (s_arr) s = s_arr[blockIdx.y];
     const size_t nw = (size_t)((r + 63) >> 6);
     for (size_t w = (size_t)blockIdx.x * blockDim.x + threadIdx.x; w < nw;
          w += (size_t)gridDim.x * blockDim.x) {
@@ -246,6 +253,18 @@ int trin_reduce(const u64 *P, size_t pw, u64 L, u64 *out, u64 r, u64 s, cudaStre
     k_reduce<<<grid_for(nw, threads), threads, 0, st>>>(P, pw, L, out, r, s);
     GF2E_CHECK_LAUNCH("k_reduce");
     return GF2E_OK;
+}
+int trin_reduce_batch(const u64 *P, size_t pstride, size_t pw, u64 L, u64 *out, size_t ostride,
+                      u64 r, const u64 *s_dev, int batch, cudaStream_t st) {
+    const size_t nw = (size_t)((r + 63) >> 6);
+    int per = std::max(1, grid_for(nw, 256) / batch);
+    k_reduce<<<dim3(per, batch), 256, 0, st>>>(P, pw, L, out, r, 0, pstride, ostride, s_dev);
+    GF2E_CHECK_LAUNCH("k_reduce batch");
+    return GF2E_OK;
+}
+int trin_square_states(const u64 *in, u64 *out, size_t stride, int nstates, u64 r,
+                       const u64 *s_dev, cudaStream_t st) {
+    return launch_square(in, out, stride, nstates, r, s_dev, 0, st);
 }
 int trin_square(const u64 *in, u64 *out, u64 r, u64 s, cudaStream_t st) {
     return launch_square(in, out, (size_t)((r + 63) >> 6), 1, r, nullptr, s, st);

@@ -289,6 +289,33 @@ def mul_batch_workspace_bytes(sizes: Sequence[tuple]) -> int:
     return need.value
 
 
+# ======================================================================= gcd
+def gcd_batch(pairs, g_cap_words: int = 0, stream=None):
+    """deg gcd(a, b) for every (a_dev, abits, b_dev, bbits) pair, on the GPU
+    (gf2_gcd.h:48-75 contract: 0 means gcd = 1).  With g_cap_words > 0 the
+    gcds that fit are returned as host arrays (None where they do not fit)."""
+    from ._lib import GcdJob
+    n = len(pairs)
+    jobs = (GcdJob * n)()
+    outs = []
+    for i, (a, ab, b, bb) in enumerate(pairs):
+        g = DeviceBuffer(8 * g_cap_words) if g_cap_words else None
+        outs.append(g)
+        jobs[i] = GcdJob(_ptr(a), ab, _ptr(b), bb, g.ptr if g else None, g_cap_words)
+    need = C.c_size_t()
+    call("gf2e_gcd_workspace_size", jobs, n, C.byref(need))
+    ws = DeviceBuffer(need.value)
+    degs = np.zeros(n, dtype=np.int64)
+    call("gf2e_gcd_batch", jobs, n, degs.ctypes.data, ws.ptr, ws.nbytes, _sp(stream))
+    gs = []
+    for d, g in zip(degs.tolist(), outs):
+        if g is None or d // 64 + 1 > g_cap_words:
+            gs.append(None)
+        else:
+            gs.append(g.to_numpy(g_cap_words, stream=stream))
+    return degs, gs
+
+
 # ========================================================== trinomial arithmetic
 def spread32(v: int) -> int:
     """Interleave zeros (gf2_trinomial_cuda.h:22-30); host helper."""
