@@ -416,7 +416,54 @@ def run_extras(torch, M, W):
     out["mul_config3"] = {"products_per_s": 64 / (ms / 1e3), "ms": ms,
                           "algorithmic_GBps": bytes3 / (ms / 1e3) / 1e9,
                           "operand_bits": tot_bits}
+    del bufs, jobs, wsb
+    out["deep_scan_r136279841"] = deep_scan_sample(torch, M)
+    out["serving"] = serving_sample()
     return out
+
+
+def deep_scan_sample(torch, M, nsurv=4, degrees=32):
+    """Config 4's per-degree leg at full size: F <- F^2 and ACC <- ACC*(F+x)
+    mod T for `nsurv` d<=24 survivors of r = 136279841, batched, degrees
+    25..24+degrees.  The interval gcd at this size needs a subquadratic gcd
+    (not built), so the sample stops before the first interval end."""
+    import ctypes as C
+    from mersenne_trinomial_b200._lib import call
+    smax = 200000
+    best = M.run_sieve(R, 24, smax)
+    surv = [s for s in range(3, smax + 1) if int(best[s]) == 0xFFFFFFFFFFFFFFFF][:nsurv]
+    h = C.c_void_p()
+    call("gf2e_scanner_create", R, nsurv, C.byref(h))
+    s_arr = np.asarray(surv, dtype=np.uint64)
+    call("gf2e_scanner_submit", h.value, s_arr.ctypes.data, nsurv, 24, 24 + 1000000, 1 << 30,
+         1 << 30, 0)
+    call("gf2e_scanner_step", h.value, 1, None)              # ramp + first degree (warm-up)
+    torch.cuda.synchronize()
+    a = torch.cuda.Event(enable_timing=True)
+    b = torch.cuda.Event(enable_timing=True)
+    a.record()
+    call("gf2e_scanner_step", h.value, degrees, None)
+    b.record()
+    torch.cuda.synchronize()
+    ms = a.elapsed_time(b)
+    M.lib().gf2e_scanner_destroy(h.value)
+    return {"survivors": surv, "degrees": degrees, "ms": ms,
+            "sd_pairs_per_s": nsurv * degrees / (ms / 1e3),
+            "ms_per_degree_per_s": ms / degrees / nsurv,
+            "note": "square + running product per degree; gcd leg not run at this size"}
+
+
+def serving_sample(n_jobs=16, rate=8.0, seed=1):
+    from mersenne_trinomial_b200 import serve
+    jobs = serve.job_stream(seed, n_jobs, rate, deep_max=600, s_lo=16, s_hi=128)
+    lat, wall, lines = serve.run_stream(jobs, slots=64)
+    plain_wall, plain_lines = serve.run_one_at_a_time(jobs, slots=64)
+    v = sorted(lat.values())
+    pairs = serve.pairs_of(jobs)
+    return {"jobs": n_jobs, "rate_per_s": rate, "p50_s": float(np.percentile(v, 50)),
+            "p99_s": float(np.percentile(v, 99)), "sd_pairs_per_s": pairs / wall,
+            "plain_one_at_a_time_sd_pairs_per_s": pairs / plain_wall,
+            "results_identical_alone_vs_mixed": all(lines[k] == plain_lines[k] for k in lines)}
 
 
 if __name__ == "__main__":

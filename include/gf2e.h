@@ -225,6 +225,82 @@ int gf2e_gcd_batch(const gf2e_gcd_job *jobs_host, int njobs, int64_t *deg_host,
                    void *workspace_dev, size_t workspace_bytes, void *stream);
 
 /* ======================================================================
+ * (e) Deep scan of sieve survivors (trinomial_scan.cu:240-381 scan_one_s,
+ * 542-697 main), batched over the s values on one GPU.
+ * ====================================================================== */
+typedef struct gf2e_scan_result {
+    uint64_t s;
+    int status;           /* 1: least factor found (d, mask); 2: none of degree
+                             <= maxd ("s u"); 3: a factor with degree in
+                             [rlo, rhi] that could not be isolated ("s rA-B") */
+    uint64_t d;           /* least factor degree (status 1) */
+    uint64_t mask_words;  /* words of the factor written to the mask buffer */
+    uint64_t rlo, rhi;    /* interval of the hit */
+} gf2e_scan_result;
+
+/* Least-degree irreducible factor of x^r + x^s + 1 with degree in (k0, maxd]
+ * for every s_host[i] (sieve survivors: no factor of degree <= k0), and the
+ * numerically least factor of that degree, written to
+ * masks_host + i*mask_cap_words.  Intervals of L0, 2*L0, ... <= Lmax degrees
+ * between gcd checks (trinomial_scan --l0/--interval).  `batch` s values are
+ * resident on the device at once; retired s are replaced from the list.
+ * Returns after all results are on the host. */
+int gf2e_scan(uint64_t r, const uint64_t *s_host, int ns, uint64_t k0, uint64_t maxd,
+              uint64_t L0, uint64_t Lmax, int batch, gf2e_scan_result *results_host,
+              uint64_t *masks_host, size_t mask_cap_words, void *stream);
+
+/* The steppable engine behind gf2e_scan, for callers that interleave work
+ * (the serving loop): one scanner per r keeps `slots` s values resident on
+ * the device; submitted s wait in a queue and enter freed slots; each step
+ * advances every resident s by one degree (batched launches) and runs the
+ * interval-end gcds; finished s are returned by poll with their tags
+ * (tag0 + i for the i-th submitted s).  No counterpart in the reference,
+ * which scans one s at a time (trinomial_scan.cu:648-689). */
+typedef struct gf2e_scanner gf2e_scanner;
+int gf2e_scanner_footprint(uint64_t r, int slots, size_t *device_bytes);
+int gf2e_scanner_create(uint64_t r, int slots, gf2e_scanner **scanner);
+int gf2e_scanner_destroy(gf2e_scanner *scanner);
+int gf2e_scanner_submit(gf2e_scanner *scanner, const uint64_t *s_host, int ns, uint64_t k0,
+                        uint64_t maxd, uint64_t L0, uint64_t Lmax, uint64_t tag0);
+int gf2e_scanner_step(gf2e_scanner *scanner, int degrees, void *stream);
+int gf2e_scanner_status(const gf2e_scanner *scanner, int *queued, int *resident,
+                        int *finished, uint64_t *sd_pairs);
+int gf2e_scanner_poll(gf2e_scanner *scanner, gf2e_scan_result *results_host,
+                      uint64_t *tags_host, uint64_t *masks_host, size_t mask_cap_words,
+                      int cap, int *nout);
+
+/* ======================================================================
+ * (f) Serving: continuous batching of (r, s-set, d-range) search jobs.  No
+ * counterpart in the reference.  A job is admitted when its device memory
+ * (a scanner for its r, shared by all jobs with that r) fits the budget;
+ * admission sieves degrees 2..min(dmax, 24) and queues the survivors on the
+ * scanner; step() advances every resident scanner; poll() returns finished
+ * jobs and their latency since submit; job_lines() gives one result line per
+ * s ("s d p<hex>", "s u" for no factor of degree <= dmax, "s rA-B").
+ * ====================================================================== */
+typedef struct gf2e_server gf2e_server;
+int gf2e_server_create(size_t budget_bytes, int slots_per_r, gf2e_server **server);
+int gf2e_server_destroy(gf2e_server *server);
+int gf2e_server_submit(gf2e_server *server, uint64_t job_id, uint64_t r, const uint64_t *s_host,
+                       int ns, uint64_t dmax, uint64_t L0, uint64_t Lmax);
+int gf2e_server_step(gf2e_server *server, int degrees, void *stream);
+int gf2e_server_status(const gf2e_server *server, int *waiting, int *active, int *finished,
+                       size_t *used_bytes);
+int gf2e_server_poll(gf2e_server *server, uint64_t *job_ids_host, double *latency_s_host,
+                     int cap, int *nout);
+int gf2e_server_job_lines(gf2e_server *server, uint64_t job_id, char *buf, size_t cap,
+                          size_t *needed);
+int gf2e_server_release(gf2e_server *server, uint64_t job_id);
+
+/* Host-side resolution of a hit (trinomial_scan.cu:208-235,
+ * gf2_gcd_ntl.cpp:68-92): for g whose irreducible factors all have degree in
+ * [kmin, kmax], the least such degree and the numerically least factor of it
+ * (equal-degree splitting when several share the degree). */
+int gf2e_resolve_factor(const uint64_t *g_host, size_t gw, uint64_t kmin, uint64_t kmax,
+                        uint64_t *d_out, uint64_t *mask_host, size_t mask_cap_words,
+                        size_t *mask_words);
+
+/* ======================================================================
  * TrinGPU context (gf2_trinomial_cuda.h:87-178): F (dA), ACC (dACC),
  * product scratch and an FFT plan for r-bit x r-bit products.
  * ====================================================================== */

@@ -37,6 +37,11 @@ class GcdJob(C.Structure):
                 ("bbits", C.c_uint64), ("g_dev", C.c_void_p), ("g_cap_words", C.c_size_t)]
 
 
+class ScanResult(C.Structure):
+    _fields_ = [("s", C.c_uint64), ("status", C.c_int), ("d", C.c_uint64),
+                ("mask_words", C.c_uint64), ("rlo", C.c_uint64), ("rhi", C.c_uint64)]
+
+
 class MulJob(C.Structure):
     _fields_ = [("a_dev", C.c_void_p), ("abits", C.c_uint64), ("b_dev", C.c_void_p),
                 ("bbits", C.c_uint64), ("out_dev", C.c_void_p)]
@@ -84,6 +89,24 @@ SIGNATURES = {
     "gf2e_mul_batch": (_i32, [_P(MulJob), _i32, _vp, _sz, _vp]),
     "gf2e_gcd_workspace_size": (_i32, [_P(GcdJob), _i32, _P(_sz)]),
     "gf2e_gcd_batch": (_i32, [_P(GcdJob), _i32, _vp, _vp, _sz, _vp]),
+    "gf2e_scan": (_i32, [_u64, _vp, _i32, _u64, _u64, _u64, _u64, _i32, _P(ScanResult), _vp,
+                         _sz, _vp]),
+    "gf2e_resolve_factor": (_i32, [_vp, _sz, _u64, _u64, _P(_u64), _vp, _sz, _P(_sz)]),
+    "gf2e_server_create": (_i32, [_sz, _i32, _P(_vp)]),
+    "gf2e_server_destroy": (_i32, [_vp]),
+    "gf2e_server_submit": (_i32, [_vp, _u64, _u64, _vp, _i32, _u64, _u64, _u64]),
+    "gf2e_server_step": (_i32, [_vp, _i32, _vp]),
+    "gf2e_server_status": (_i32, [_vp, _P(_i32), _P(_i32), _P(_i32), _P(_sz)]),
+    "gf2e_server_poll": (_i32, [_vp, _vp, _vp, _i32, _P(_i32)]),
+    "gf2e_server_job_lines": (_i32, [_vp, _u64, C.c_char_p, _sz, _P(_sz)]),
+    "gf2e_server_release": (_i32, [_vp, _u64]),
+    "gf2e_scanner_footprint": (_i32, [_u64, _i32, _P(_sz)]),
+    "gf2e_scanner_create": (_i32, [_u64, _i32, _P(_vp)]),
+    "gf2e_scanner_destroy": (_i32, [_vp]),
+    "gf2e_scanner_submit": (_i32, [_vp, _vp, _i32, _u64, _u64, _u64, _u64, _u64]),
+    "gf2e_scanner_step": (_i32, [_vp, _i32, _vp]),
+    "gf2e_scanner_status": (_i32, [_vp, _P(_i32), _P(_i32), _P(_i32), _P(_u64)]),
+    "gf2e_scanner_poll": (_i32, [_vp, _P(ScanResult), _vp, _vp, _sz, _i32, _P(_i32)]),
     "gf2e_trin_create": (_i32, [_u64, _P(_vp)]),
     "gf2e_trin_destroy": (_i32, [_vp]),
     "gf2e_trin_set_s": (_i32, [_vp, _u64]),

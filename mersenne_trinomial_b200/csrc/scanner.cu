@@ -1,0 +1,379 @@
+// scanner.cu -- the resident, steppable deep-scan engine behind gf2e_scan
+// and the serving loop.
+//
+// One scanner serves one r.  It owns device state for `slots` s values
+// (F, scratch, ACC, the two transform buffers, the product, the trinomial),
+// a queue of submitted s values (each with its own k0, maxd and interval
+// policy, tagged by the caller), and a list of finished results.  A step
+// advances every resident s by one degree with batched launches (squaring,
+// two packed transforms, pointwise product, inverse, overlap-add, fold),
+// runs one batched gcd for the s whose interval ends, resolves hits on the
+// host, retires finished s and refills their slots from the queue (or
+// compacts the slots when the queue is empty).  Per-s state stays on the
+// device between steps, so different jobs' s values share every launch.
+#include "gf2e_internal.cuh"
+
+#include <algorithm>
+#include <deque>
+#include <vector>
+
+namespace gf2e {
+int trin_square_states(const u64 *in, u64 *out, size_t stride, int nstates, u64 r,
+                       const u64 *s_dev, cudaStream_t st);
+int trin_set_const(u64 *states, size_t stride, int nstates, u64 r, u64 w0, cudaStream_t st);
+int trin_reduce_batch(const u64 *P, size_t pstride, size_t pw, u64 L, u64 *out, size_t ostride,
+                      u64 r, const u64 *s_dev, int batch, cudaStream_t st);
+int fft_fwd_packed_batch(const gf2e_fft_plan *plan, u64 *f, u64 fstride, const u32 *src32,
+                         u64 sstride32, u64 nchunks, u64 xor0, int batch, cudaStream_t st);
+int fft_run_batch(const gf2e_fft_plan *plan, bool forward, u64 *f, u64 fstride, int batch,
+                  cudaStream_t st);
+int overlap_add_batch(const u64 *F, u64 fstride, u64 nchunks, u64 *out, u64 ostride, u64 ow,
+                      int batch, cudaStream_t st);
+int pointwise(u64 *fa, const u64 *fb, u64 n, cudaStream_t st);
+int mul_fft_m(u64 abits, u64 bbits);
+gf2e_fft_plan *cached_plan(int m);
+u64 fft_plan_n(const gf2e_fft_plan *plan);
+bool resolve_factor(const std::vector<u64> &g, u64 kmin, u64 kmax, u64 &d_out,
+                    std::vector<u64> &mask);
+}  // namespace gf2e
+
+struct gf2e_scanner {
+    struct Job { u64 s, k0, maxd, L0, Lmax, tag; };
+    struct Slot { Job job; u64 k, iv, L; };
+    struct Done { gf2e_scan_result res; u64 tag; std::vector<u64> mask; };
+
+    u64 r = 0;
+    int B = 0;
+    size_t nw = 0, stride = 0, tw = 0, ow = 0, pstride = 0, gcap = 0;
+    u64 n = 0, nchunks = 0;
+    gf2e_fft_plan *plan = nullptr;
+    u64 *dmem = nullptr, *F = nullptr, *Fs = nullptr, *ACC = nullptr, *FA = nullptr,
+        *FB = nullptr, *P = nullptr, *T = nullptr, *sdev = nullptr, *G = nullptr;
+    void *gws = nullptr;
+    size_t gws_bytes = 0, dmem_bytes = 0;
+    std::deque<Job> queue;
+    std::vector<Slot> slot;
+    int nact = 0;
+    std::deque<Done> done;
+    std::vector<u64> shost, thost, ghost;
+    std::vector<int64_t> degs;
+    std::vector<gf2e_gcd_job> jobs;
+    u64 degree_steps = 0, sd_pairs = 0;
+};
+
+namespace {
+
+struct Geometry {
+    size_t nw, stride, tw, ow, pstride, gcap;
+    u64 n, nchunks;
+    int m;
+};
+
+Geometry geometry(u64 r) {
+    Geometry g;
+    g.nw = (size_t)((r + 63) >> 6);
+    g.stride = g.nw + (g.nw & 1);
+    g.tw = (size_t)((r + 1 + 63) >> 6);
+    g.m = gf2e::mul_fft_m(r, r);
+    g.n = (u64)1 << g.m;
+    g.nchunks = (r + 31) >> 5;
+    g.ow = (size_t)(((2 * r + 63) >> 6) + 1);
+    g.pstride = g.ow + (g.ow & 1);
+    g.gcap = std::min<size_t>(g.tw, 4096);
+    return g;
+}
+
+size_t device_words(const Geometry &g, int B) {
+    return 3 * g.stride * B + 2 * g.n * B + g.pstride * B + g.tw * B + B + g.gcap * B;
+}
+
+int load_slot(gf2e_scanner &S, int j, const gf2e_scanner::Job &job, cudaStream_t st) {
+    std::fill(S.thost.begin(), S.thost.end(), 0);
+    S.thost[0] |= 1;
+    S.thost[job.s >> 6] |= 1ull << (job.s & 63);
+    S.thost[S.r >> 6] |= 1ull << (S.r & 63);
+    S.shost[j] = job.s;
+    cudaError_t e = cudaMemcpyAsync(S.T + S.tw * j, S.thost.data(), S.tw * 8,
+                                    cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(S.sdev + j, &S.shost[j], 8, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);      // host staging reused
+    if (e != cudaSuccess) return gf2e::cuda_status(e, "scanner slot load");
+    GF2E_TRY(gf2e::trin_set_const(S.F + S.stride * j, S.stride, 1, S.r, 2, st));
+    GF2E_TRY(gf2e::trin_set_const(S.ACC + S.stride * j, S.stride, 1, S.r, 1, st));
+    for (u64 k = 0; k < job.k0; k++) {
+        GF2E_TRY(gf2e::trin_square_states(S.F + S.stride * j, S.Fs + S.stride * j, S.stride, 1,
+                                          S.r, S.sdev + j, st));
+        e = cudaMemcpyAsync(S.F + S.stride * j, S.Fs + S.stride * j, S.nw * 8,
+                            cudaMemcpyDeviceToDevice, st);
+        if (e != cudaSuccess) return gf2e::cuda_status(e, "scanner ramp");
+    }
+    S.slot[j] = gf2e_scanner::Slot{job, job.k0, job.k0, job.L0};
+    return GF2E_OK;
+}
+
+int move_slot(gf2e_scanner &S, int to, int from, cudaStream_t st) {
+    cudaError_t e = cudaMemcpyAsync(S.F + S.stride * to, S.F + S.stride * from, S.stride * 8,
+                                    cudaMemcpyDeviceToDevice, st);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(S.ACC + S.stride * to, S.ACC + S.stride * from, S.stride * 8,
+                            cudaMemcpyDeviceToDevice, st);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(S.T + S.tw * to, S.T + S.tw * from, S.tw * 8,
+                            cudaMemcpyDeviceToDevice, st);
+    S.shost[to] = S.shost[from];
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(S.sdev + to, &S.shost[to], 8, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    S.slot[to] = S.slot[from];
+    return gf2e::cuda_status(e, "scanner compaction");
+}
+
+int fill_slots(gf2e_scanner &S, cudaStream_t st) {
+    while (S.nact < S.B && !S.queue.empty()) {
+        gf2e_scanner::Job job = S.queue.front();
+        S.queue.pop_front();
+        GF2E_TRY(load_slot(S, S.nact, job, st));
+        S.nact++;
+    }
+    return GF2E_OK;
+}
+
+// one degree for all resident s, then the interval-end gcds
+int degree_step(gf2e_scanner &S, cudaStream_t st) {
+    const int na = S.nact;
+    GF2E_TRY(gf2e::trin_square_states(S.F, S.Fs, S.stride, na, S.r, S.sdev, st));
+    std::swap(S.F, S.Fs);
+    GF2E_TRY(gf2e::fft_fwd_packed_batch(S.plan, S.FA, S.n, reinterpret_cast<const u32 *>(S.ACC),
+                                        2 * S.stride, S.nchunks, 0, na, st));
+    GF2E_TRY(gf2e::fft_fwd_packed_batch(S.plan, S.FB, S.n, reinterpret_cast<const u32 *>(S.F),
+                                        2 * S.stride, S.nchunks, 2, na, st));
+    GF2E_TRY(gf2e::pointwise(S.FA, S.FB, S.n * na, st));
+    GF2E_TRY(gf2e::fft_run_batch(S.plan, false, S.FA, S.n, na, st));
+    GF2E_TRY(gf2e::overlap_add_batch(S.FA, S.n, 2 * S.nchunks - 1, S.P, S.pstride, S.ow, na, st));
+    GF2E_TRY(gf2e::trin_reduce_batch(S.P, S.pstride, S.ow, 2 * S.r - 1, S.ACC, S.stride, S.r,
+                                     S.sdev, na, st));
+    S.degree_steps++;
+    S.sd_pairs += (u64)na;
+    std::vector<int> due;
+    for (int j = 0; j < na; j++) {
+        gf2e_scanner::Slot &sl = S.slot[j];
+        sl.k++;
+        if (sl.k - sl.iv >= sl.L || sl.k == sl.job.maxd) due.push_back(j);
+    }
+    if (due.empty()) return GF2E_OK;
+    for (size_t q = 0; q < due.size(); q++) {
+        int j = due[q];
+        S.jobs[q] = gf2e_gcd_job{S.ACC + S.stride * j, S.r, S.T + S.tw * j, S.r + 1,
+                                 S.G + S.gcap * q, S.gcap};
+    }
+    GF2E_TRY(gf2e_gcd_batch(S.jobs.data(), (int)due.size(), S.degs.data(), S.gws, S.gws_bytes,
+                            st));
+    std::vector<int> retire;
+    for (size_t q = 0; q < due.size(); q++) {
+        int j = due[q];
+        gf2e_scanner::Slot &sl = S.slot[j];
+        if (S.degs[q] > 0 || sl.k == sl.job.maxd) {
+            gf2e_scanner::Done D;
+            D.tag = sl.job.tag;
+            D.res = gf2e_scan_result{sl.job.s, 2, 0, 0, sl.iv + 1, sl.k};
+            if (S.degs[q] > 0) {
+                D.res.status = 3;
+                if ((size_t)(S.degs[q] / 64 + 1) <= S.gcap) {
+                    cudaError_t e = cudaMemcpyAsync(S.ghost.data(), S.G + S.gcap * q, S.gcap * 8,
+                                                    cudaMemcpyDeviceToHost, st);
+                    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+                    if (e != cudaSuccess) return gf2e::cuda_status(e, "gcd readback");
+                    std::vector<u64> g(S.ghost.begin(), S.ghost.end());
+                    u64 d = 0;
+                    if (gf2e::resolve_factor(g, sl.iv + 1, sl.k, d, D.mask)) {
+                        D.res.status = 1;
+                        D.res.d = d;
+                        D.res.mask_words = D.mask.size();
+                    }
+                }
+            }
+            S.done.push_back(std::move(D));
+            retire.push_back(j);
+        } else {
+            sl.iv = sl.k;
+            sl.L = std::min(2 * sl.L, sl.job.Lmax);
+            GF2E_TRY(gf2e::trin_set_const(S.ACC + S.stride * j, S.stride, 1, S.r, 1, st));
+        }
+    }
+    // refill from the queue, else compact (highest slots first)
+    std::sort(retire.begin(), retire.end(), std::greater<int>());
+    for (int j : retire) {
+        if (!S.queue.empty()) {
+            gf2e_scanner::Job job = S.queue.front();
+            S.queue.pop_front();
+            GF2E_TRY(load_slot(S, j, job, st));
+        } else {
+            if (j != S.nact - 1) GF2E_TRY(move_slot(S, j, S.nact - 1, st));
+            S.nact--;
+        }
+    }
+    return GF2E_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int gf2e_scanner_footprint(uint64_t r, int slots, size_t *bytes) {
+    if (!bytes || slots < 1 || r < 5) return gf2e::invalid("bad footprint query");
+    Geometry g = geometry(r);
+    size_t words = device_words(g, slots);
+    // gcd workspace: job table + 4 buffers per job
+    size_t gw = ((size_t)slots * 96 + 255) + (size_t)slots * 4 * (g.tw + 1) * 8;
+    *bytes = words * 8 + gw;
+    return GF2E_OK;
+}
+
+int gf2e_scanner_create(uint64_t r, int slots, gf2e_scanner **out) {
+    if (!out || slots < 1 || slots > 4096) return gf2e::invalid("scanner: 1 <= slots <= 4096");
+    if (r < 5 || !(r & 1) || r >= (1ull << 31)) return gf2e::invalid("scanner: bad r");
+    Geometry g = geometry(r);
+    gf2e_scanner *S = new gf2e_scanner;
+    S->r = r;
+    S->B = slots;
+    S->nw = g.nw; S->stride = g.stride; S->tw = g.tw; S->ow = g.ow; S->pstride = g.pstride;
+    S->gcap = g.gcap; S->n = g.n; S->nchunks = g.nchunks;
+    S->plan = gf2e::cached_plan(g.m);
+    if (!S->plan) { delete S; return gf2e::invalid("FFT plan m=%d", g.m); }
+    S->dmem_bytes = device_words(g, slots) * 8;
+    cudaError_t e = cudaMalloc(&S->dmem, S->dmem_bytes);
+    if (e != cudaSuccess) { delete S; return gf2e::cuda_status(e, "scanner buffers"); }
+    const int B = slots;
+    S->F = S->dmem;
+    S->Fs = S->F + g.stride * B;
+    S->ACC = S->Fs + g.stride * B;
+    S->FA = S->ACC + g.stride * B;
+    S->FB = S->FA + g.n * B;
+    S->P = S->FB + g.n * B;
+    S->T = S->P + g.pstride * B;
+    S->sdev = S->T + g.tw * B;
+    S->G = S->sdev + B;
+    std::vector<gf2e_gcd_job> tmp(B, gf2e_gcd_job{S->ACC, r, S->T, r + 1, S->G, g.gcap});
+    int st = gf2e_gcd_workspace_size(tmp.data(), B, &S->gws_bytes);
+    if (st == GF2E_OK) {
+        e = cudaMalloc(&S->gws, S->gws_bytes);
+        if (e != cudaSuccess) st = gf2e::cuda_status(e, "scanner gcd workspace");
+    }
+    if (st != GF2E_OK) {
+        cudaFree(S->dmem);
+        delete S;
+        return st;
+    }
+    S->slot.resize(B);
+    S->shost.assign(B, 0);
+    S->thost.assign(g.tw, 0);
+    S->ghost.assign(g.gcap, 0);
+    S->degs.assign(B, 0);
+    S->jobs.resize(B);
+    *out = S;
+    return GF2E_OK;
+}
+
+int gf2e_scanner_destroy(gf2e_scanner *S) {
+    if (!S) return GF2E_OK;
+    cudaFree(S->gws);
+    cudaFree(S->dmem);
+    delete S;
+    return GF2E_OK;
+}
+
+int gf2e_scanner_submit(gf2e_scanner *S, const uint64_t *s_host, int ns, uint64_t k0,
+                        uint64_t maxd, uint64_t L0, uint64_t Lmax, uint64_t tag0) {
+    if (!S || !s_host || ns < 0) return gf2e::invalid("scanner submit: bad arguments");
+    if (!(k0 >= 1 && maxd > k0)) return gf2e::invalid("scanner submit: need 1 <= k0 < maxd");
+    for (int i = 0; i < ns; i++)
+        if (!(s_host[i] >= 1 && 2 * s_host[i] < S->r))
+            return gf2e::invalid("scanner submit: s=%llu outside 1..(r-1)/2",
+                                 (unsigned long long)s_host[i]);
+    if (Lmax < 1) Lmax = 1;
+    if (L0 < 1) L0 = 1;
+    if (L0 > Lmax) L0 = Lmax;
+    for (int i = 0; i < ns; i++)
+        S->queue.push_back(gf2e_scanner::Job{s_host[i], k0, maxd, L0, Lmax, tag0 + (u64)i});
+    return GF2E_OK;
+}
+
+int gf2e_scanner_step(gf2e_scanner *S, int degrees, void *stream) {
+    if (!S || degrees < 0) return gf2e::invalid("scanner step: bad arguments");
+    cudaStream_t st = (cudaStream_t)stream;
+    GF2E_TRY(fill_slots(*S, st));
+    for (int i = 0; i < degrees && S->nact > 0; i++) GF2E_TRY(degree_step(*S, st));
+    return GF2E_OK;
+}
+
+int gf2e_scanner_status(const gf2e_scanner *S, int *queued, int *resident, int *finished,
+                        uint64_t *sd_pairs) {
+    if (!S) return gf2e::invalid("null scanner");
+    if (queued) *queued = (int)S->queue.size();
+    if (resident) *resident = S->nact;
+    if (finished) *finished = (int)S->done.size();
+    if (sd_pairs) *sd_pairs = S->sd_pairs;
+    return GF2E_OK;
+}
+
+int gf2e_scanner_poll(gf2e_scanner *S, gf2e_scan_result *res, uint64_t *tags,
+                      uint64_t *masks_host, size_t mask_cap_words, int cap, int *nout) {
+    if (!S || !res || !tags || !nout || cap < 0) return gf2e::invalid("scanner poll: bad arguments");
+    int k = 0;
+    while (k < cap && !S->done.empty()) {
+        gf2e_scanner::Done &D = S->done.front();
+        res[k] = D.res;
+        tags[k] = D.tag;
+        if (D.res.status == 1) {
+            if (masks_host && D.mask.size() <= mask_cap_words) {
+                for (size_t w = 0; w < mask_cap_words; w++)
+                    masks_host[(size_t)k * mask_cap_words + w] = w < D.mask.size() ? D.mask[w] : 0;
+            } else {
+                res[k].status = 3;                     // caller's mask buffer too small
+            }
+        }
+        S->done.pop_front();
+        k++;
+    }
+    *nout = k;
+    return GF2E_OK;
+}
+
+int gf2e_scan(uint64_t r, const uint64_t *s_host, int ns, uint64_t k0, uint64_t maxd,
+              uint64_t L0, uint64_t Lmax, int batch, gf2e_scan_result *res,
+              uint64_t *masks_host, size_t mask_cap_words, void *stream) {
+    if (!s_host || !res || ns < 1 || batch < 1)
+        return gf2e::invalid("gf2e_scan: ns >= 1 and batch >= 1 required");
+    gf2e_scanner *S = nullptr;
+    GF2E_TRY(gf2e_scanner_create(r, std::min(batch, ns), &S));
+    int st = gf2e_scanner_submit(S, s_host, ns, k0, maxd, L0, Lmax, 0);
+    std::vector<gf2e_scan_result> tmp(ns);
+    std::vector<u64> tags(ns), masks((size_t)ns * mask_cap_words);
+    int got = 0;
+    while (st == GF2E_OK && got < ns) {
+        int q = 0, a = 0;
+        st = gf2e_scanner_step(S, 256, stream);
+        if (st != GF2E_OK) break;
+        gf2e_scanner_status(S, &q, &a, nullptr, nullptr);
+        int n = 0;
+        st = gf2e_scanner_poll(S, tmp.data() + got, tags.data() + got,
+                               masks_host ? masks.data() + (size_t)got * mask_cap_words : nullptr,
+                               mask_cap_words, ns - got, &n);
+        got += n;
+        if (q == 0 && a == 0 && got < ns) { st = gf2e::invalid("scan lost %d results", ns - got); }
+    }
+    if (st == GF2E_OK) {
+        for (int i = 0; i < ns; i++) {
+            u64 idx = tags[i];
+            res[idx] = tmp[i];
+            if (masks_host)
+                for (size_t w = 0; w < mask_cap_words; w++)
+                    masks_host[idx * mask_cap_words + w] = masks[(size_t)i * mask_cap_words + w];
+        }
+    }
+    gf2e_scanner_destroy(S);
+    return st;
+}
+
+}  // extern "C"

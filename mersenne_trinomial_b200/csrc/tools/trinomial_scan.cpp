@@ -1,0 +1,214 @@
+// trinomial_scan -- drop-in for the reference tool of the same name
+// (trinomial_scan.cu main, 542-697) on libgf2e.so: the deep scan of sieve
+// survivors, batched over the s values on the GPU with GPU gcds.
+//
+//   trinomial_scan <r> <survivors.txt> <k0> <maxd> <out_prefix>
+//                  [--interval Lmax] [--l0 L0] [--batch B] [--verbose 0..3]
+//                  [--gcd-threads N] [--state FILE]      (accepted, unused)
+//   trinomial_scan --selftest
+//
+// Output <out_prefix>.results.txt, appended, resumable (s already listed are
+// skipped): "s d p<hex>" (least degree, numerically least factor), "s u"
+// (no factor of degree <= maxd) or "s rA-B" (a factor with degree in [A,B]
+// that could not be isolated).  k0 must be the depth the sieve reached.
+#include <cinttypes>
+#include <chrono>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <set>
+#include <string>
+#include <vector>
+
+#include "gf2e.h"
+
+typedef uint64_t u64;
+
+static double now_s() {
+    using namespace std::chrono;
+    return duration<double>(steady_clock::now().time_since_epoch()).count();
+}
+
+static std::string hexmask(const u64 *w, size_t n) {
+    static const char *dig = "0123456789abcdef";
+    long long d = -1;
+    for (size_t i = n; i-- > 0;)
+        if (w[i]) { d = (long long)(i * 64 + 63 - __builtin_clzll(w[i])); break; }
+    if (d < 0) return "0";
+    std::string s;
+    for (long long k = d / 4; k >= 0; k--) s += dig[(w[k >> 4] >> ((k & 15) * 4)) & 0xF];
+    return s;
+}
+
+// x^e mod p for a factor p of degree d (multi-word, shift-and-add)
+static bool divides(u64 r, u64 s, const u64 *p, size_t pw, u64 d) {
+    size_t nw = (size_t)(d / 64) + 1;
+    std::vector<u64> P(p, p + pw);
+    P.resize(nw + 1, 0);
+    auto mulx_mod = [&](std::vector<u64> &a) {
+        u64 carry = 0;
+        for (size_t i = 0; i < nw; i++) { u64 nc = a[i] >> 63; a[i] = (a[i] << 1) | carry; carry = nc; }
+        if ((a[d >> 6] >> (d & 63)) & 1)
+            for (size_t i = 0; i < nw; i++) a[i] ^= P[i];
+    };
+    auto sqr_mod = [&](std::vector<u64> &a) {
+        std::vector<u64> t(2 * nw + 1, 0);
+        for (size_t i = 0; i < nw; i++)
+            for (int b = 0; b < 64; b++)
+                if ((a[i] >> b) & 1) {
+                    u64 e = 2 * (i * 64 + b);
+                    t[e >> 6] ^= 1ull << (e & 63);
+                }
+        for (long long e = (long long)(2 * nw * 64) - 1; e >= (long long)d; e--) {
+            if (!((t[e >> 6] >> (e & 63)) & 1)) continue;
+            u64 sh = (u64)e - d;
+            for (size_t i = 0; i <= d / 64; i++) {
+                u64 v = P[i];
+                if (!v) continue;
+                size_t j = i + (sh >> 6);
+                unsigned bs = sh & 63;
+                if (j < t.size()) t[j] ^= v << bs;
+                if (bs && j + 1 < t.size()) t[j + 1] ^= v >> (64 - bs);
+            }
+        }
+        for (size_t i = 0; i < nw; i++) a[i] = t[i];
+    };
+    auto powx = [&](u64 e) {
+        std::vector<u64> a(nw, 0);
+        a[0] = 1;
+        for (int bit = 63; bit >= 0; bit--) {
+            sqr_mod(a);
+            if ((e >> bit) & 1) mulx_mod(a);
+        }
+        return a;
+    };
+    std::vector<u64> xr = powx(r), xs = powx(s);
+    xr[0] ^= 1;
+    for (size_t i = 0; i < nw; i++)
+        if (xr[i] != xs[i]) return false;
+    return true;
+}
+
+static int run(u64 r, const std::vector<u64> &surv, u64 k0, u64 maxd, u64 L0, u64 Lmax,
+               int batch, FILE *fres, int verbose, u64 *nfound, u64 *nu, u64 *nbad) {
+    const size_t cap = 4096;
+    std::vector<gf2e_scan_result> res(surv.size());
+    std::vector<u64> masks(surv.size() * cap);
+    int st = gf2e_scan(r, surv.data(), (int)surv.size(), k0, maxd, L0, Lmax, batch, res.data(),
+                       masks.data(), cap, nullptr);
+    if (st != GF2E_OK) {
+        fprintf(stderr, "scan failed: %s (%s)\n", gf2e_status_string(st), gf2e_last_error());
+        return 1;
+    }
+    for (size_t i = 0; i < surv.size(); i++) {
+        const gf2e_scan_result &R = res[i];
+        if (R.status == 1) {
+            std::string hx = hexmask(&masks[i * cap], R.mask_words);
+            if (fres) fprintf(fres, "%" PRIu64 " %" PRIu64 " p%s\n", R.s, R.d, hx.c_str());
+            if (!divides(r, R.s, &masks[i * cap], R.mask_words, R.d)) ++*nbad;
+            ++*nfound;
+            if (verbose >= 1) fprintf(stderr, "  s=%" PRIu64 ": d=%" PRIu64 "\n", R.s, R.d);
+        } else if (R.status == 2) {
+            if (fres) fprintf(fres, "%" PRIu64 " u\n", R.s);
+            ++*nu;
+        } else {
+            if (fres) fprintf(fres, "%" PRIu64 " r%" PRIu64 "-%" PRIu64 "\n", R.s, R.rlo, R.rhi);
+            ++*nfound;
+        }
+    }
+    return 0;
+}
+
+static int selftest() {
+    // survivors of r = 4423 with no factor of degree <= 5 among s = 2..350
+    const u64 r = 4423, k0 = 5, maxd = 200, smax = 350;
+    size_t ws = 0;
+    gf2e_sieve_workspace_size((int)k0, &ws);
+    void *dws, *dbest;
+    if (gf2e_device_alloc(&dws, ws) || gf2e_device_alloc(&dbest, 8 * (smax + 1))) return 1;
+    gf2e_sieve_fill((u64 *)dbest, smax, nullptr);
+    if (gf2e_sieve_run(r, 2, (int)k0, smax, (u64 *)dbest, dws, ws, nullptr) != GF2E_OK) return 1;
+    std::vector<u64> best(smax + 1);
+    gf2e_copy_to_host(best.data(), dbest, 8 * (smax + 1), nullptr);
+    std::vector<u64> surv;
+    for (u64 s = 2; s <= smax; s++)
+        if (best[s] == ~0ULL) surv.push_back(s);
+    int bad = 0;
+    const u64 pol[2][2] = {{32, 4096}, {8, 8}};
+    for (auto &p : pol) {
+        u64 nf = 0, nu = 0, nb = 0;
+        if (run(r, surv, k0, maxd, p[0], p[1], 64, nullptr, 0, &nf, &nu, &nb)) return 1;
+        bool ok = surv.size() == 104 && nf == 102 && nu == 2 && nb == 0;
+        printf("scan r=4423 k0=5 maxd=200 intervals %" PRIu64 "/%" PRIu64 ": %zu survivors, "
+               "%" PRIu64 " found, %" PRIu64 " u, %" PRIu64 " not dividing  %s\n",
+               p[0], p[1], surv.size(), nf, nu, nb, ok ? "PASS" : "FAIL");
+        bad += !ok;
+    }
+    printf(bad ? "\nSCAN SELFTEST: %d FAILURES\n" : "\nSCAN SELFTEST: ALL PASS\n", bad);
+    return bad ? 1 : 0;
+}
+
+int main(int argc, char **argv) {
+    if (argc >= 2 && !strcmp(argv[1], "--selftest")) return selftest();
+    if (argc < 6) {
+        fprintf(stderr, "usage: %s <r> <survivors.txt> <k0> <maxd> <out_prefix>\n"
+                        "          [--interval Lmax] [--l0 L0] [--batch B] [--verbose 0..3]\n"
+                        "       %s --selftest\n"
+                        "k0 must be the depth the coarse sieve actually reached.\n",
+                argv[0], argv[0]);
+        return 1;
+    }
+    u64 r = strtoull(argv[1], 0, 10), k0 = strtoull(argv[3], 0, 10), maxd = strtoull(argv[4], 0, 10);
+    std::string prefix = argv[5];
+    u64 L0 = 64, Lmax = 4096;
+    int batch = 64, verbose = 1;
+    for (int i = 6; i < argc; i++) {
+        if (!strcmp(argv[i], "--interval") && i + 1 < argc) Lmax = strtoull(argv[++i], 0, 10);
+        else if (!strcmp(argv[i], "--l0") && i + 1 < argc) L0 = strtoull(argv[++i], 0, 10);
+        else if (!strcmp(argv[i], "--batch") && i + 1 < argc) batch = atoi(argv[++i]);
+        else if (!strcmp(argv[i], "--verbose") && i + 1 < argc) verbose = atoi(argv[++i]);
+        else if ((!strcmp(argv[i], "--gcd-threads") || !strcmp(argv[i], "--state")) && i + 1 < argc) {
+            fprintf(stderr, "note: %s ignored (gcds run on the GPU; results file is the resume record)\n",
+                    argv[i]);
+            i++;
+        } else {
+            fprintf(stderr, "unknown option %s\n", argv[i]);
+            return 1;
+        }
+    }
+    if (Lmax < 1) Lmax = 1;
+    if (L0 > Lmax) L0 = Lmax;
+    if (!(k0 >= 1 && maxd > k0)) { fprintf(stderr, "need 1 <= k0 < maxd\n"); return 1; }
+    std::vector<u64> surv;
+    FILE *f = fopen(argv[2], "r");
+    if (!f) { perror(argv[2]); return 1; }
+    u64 s;
+    while (fscanf(f, "%" SCNu64, &s) == 1) {
+        if (s >= 1 && 2 * s < r) surv.push_back(s);
+        else fprintf(stderr, "skipping s=%" PRIu64 " (need 1 <= s <= (r-1)/2)\n", s);
+    }
+    fclose(f);
+    std::string rpath = prefix + ".results.txt";
+    std::set<u64> done;
+    if ((f = fopen(rpath.c_str(), "r"))) {
+        char line[256];
+        while (fgets(line, sizeof line, f))
+            if (sscanf(line, "%" SCNu64, &s) == 1) done.insert(s);
+        fclose(f);
+    }
+    std::vector<u64> todo;
+    for (u64 v : surv)
+        if (!done.count(v)) todo.push_back(v);
+    fprintf(stderr, "trinomial_scan r=%" PRIu64 " k0=%" PRIu64 " maxd=%" PRIu64 ": %zu survivors "
+                    "(%zu already done), gcd backend: GPU, batch %d\n",
+            r, k0, maxd, surv.size(), done.size(), batch);
+    FILE *fres = fopen(rpath.c_str(), "a");
+    if (!fres) { perror(rpath.c_str()); return 1; }
+    double t0 = now_s();
+    u64 nf = 0, nu = 0, nb = 0;
+    int rc = todo.empty() ? 0 : run(r, todo, k0, maxd, L0, Lmax, batch, fres, verbose, &nf, &nu, &nb);
+    fclose(fres);
+    fprintf(stderr, "done: %" PRIu64 " found, %" PRIu64 " u, %.1fs total%s\n", nf, nu,
+            now_s() - t0, nb ? " (WARNING: some factors failed verification)" : "");
+    return rc ? rc : (nb ? 1 : 0);
+}

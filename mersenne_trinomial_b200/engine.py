@@ -316,6 +316,48 @@ def gcd_batch(pairs, g_cap_words: int = 0, stream=None):
     return degs, gs
 
 
+def _hex(words) -> str:
+    x = 0
+    for i, w in enumerate(np.asarray(words, dtype=np.uint64).tolist()):
+        x |= int(w) << (64 * i)
+    return format(x, "x")
+
+
+def scan(r: int, survivors, k0: int, maxd: int, L0: int = 64, Lmax: int = 4096,
+         batch: int = 64, mask_cap_words: int = 1024, stream=None) -> list:
+    """Deep scan (trinomial_scan.cu): one result line per s in the reference's
+    format, 's d p<hex>', 's u' or 's rA-B'."""
+    from ._lib import ScanResult
+    s = np.ascontiguousarray(np.asarray(survivors, dtype=np.uint64))
+    n = s.size
+    res = (ScanResult * n)()
+    masks = np.zeros((n, mask_cap_words), dtype=np.uint64)
+    call("gf2e_scan", r, s.ctypes.data, n, k0, maxd, L0, Lmax, batch, res, masks.ctypes.data,
+         mask_cap_words, _sp(stream))
+    out = []
+    for i in range(n):
+        R = res[i]
+        if R.status == 1:
+            out.append(f"{R.s} {R.d} p{_hex(masks[i, :R.mask_words])}")
+        elif R.status == 2:
+            out.append(f"{R.s} u")
+        else:
+            out.append(f"{R.s} r{R.rlo}-{R.rhi}")
+    return out
+
+
+def resolve_factor(g_words, kmin: int, kmax: int, cap: int = 1024):
+    """(d, mask words) of the least-degree, then least, factor of g with
+    degree in [kmin, kmax] (host computation on a small gcd)."""
+    g = np.ascontiguousarray(np.asarray(g_words, dtype=np.uint64))
+    d = C.c_uint64()
+    mw = C.c_size_t()
+    mask = np.zeros(cap, dtype=np.uint64)
+    call("gf2e_resolve_factor", g.ctypes.data, g.size, kmin, kmax, C.byref(d), mask.ctypes.data,
+         cap, C.byref(mw))
+    return int(d.value), mask[: mw.value].copy()
+
+
 # ========================================================== trinomial arithmetic
 def spread32(v: int) -> int:
     """Interleave zeros (gf2_trinomial_cuda.h:22-30); host helper."""

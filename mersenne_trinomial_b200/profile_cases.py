@@ -48,6 +48,35 @@ def case_mul(a):
     M.gf2x_fft_mul(x, bits, y, bits)
 
 
+def case_gcd(a):
+    """n gcds of an r-bit accumulator-like operand against x^r + x^s + 1."""
+    r, n = a.r, a.n
+    nw = (r + 1 + 63) // 64
+    pairs, keep = [], []
+    for i in range(n):
+        T = np.zeros(nw, dtype=np.uint64)
+        s = 1000 + 37 * i
+        for e in (0, s, r):
+            T[e >> 6] |= np.uint64(1 << (e & 63))
+        A = W.random_bits(r, 50 + i)
+        da, db = M.DeviceBuffer.from_array(A), M.DeviceBuffer.from_array(T)
+        keep += [da, db]
+        pairs.append((da, r, db, r + 1))
+    t0 = time.perf_counter()
+    degs, _ = M.gcd_batch(pairs)
+    print(f"gcd: {n} x {r} bits in {time.perf_counter() - t0:.3f} s, degrees {degs[:4]}")
+
+
+def case_scan(a):
+    """A small deep scan: n seeded s at r, degrees k0 = 24 .. a.k."""
+    rng = np.random.default_rng(9)
+    s = rng.integers(3, a.r // 2, size=a.n).astype(np.uint64)
+    t0 = time.perf_counter()
+    lines = M.scan(a.r, s, 24, max(25, a.k), L0=64, Lmax=4096, batch=a.n)
+    print(f"scan: {a.n} s x degrees 25..{a.k} at r={a.r} in {time.perf_counter() - t0:.3f} s:",
+          lines[:3])
+
+
 def case_sieve(a):
     smax = a.r // 2
     M.run_sieve(a.r, a.depth, smax)
@@ -55,7 +84,7 @@ def case_sieve(a):
 
 def main(argv=None):
     ap = argparse.ArgumentParser()
-    ap.add_argument("case", choices=["square", "fft", "mul", "sieve"])
+    ap.add_argument("case", choices=["square", "fft", "mul", "sieve", "gcd", "scan"])
     ap.add_argument("--r", type=int, default=136279841)
     ap.add_argument("--n", type=int, default=8)
     ap.add_argument("--k", type=int, default=3)
@@ -63,7 +92,8 @@ def main(argv=None):
     ap.add_argument("--depth", type=int, default=24)
     a = ap.parse_args(argv)
     t0 = time.perf_counter()
-    {"square": case_square, "fft": case_fft, "mul": case_mul, "sieve": case_sieve}[a.case](a)
+    {"square": case_square, "fft": case_fft, "mul": case_mul, "sieve": case_sieve,
+     "gcd": case_gcd, "scan": case_scan}[a.case](a)
     print(f"{a.case}: done in {time.perf_counter() - t0:.3f} s")
     return 0
 
