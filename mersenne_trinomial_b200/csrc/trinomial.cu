@@ -74,16 +74,25 @@ GF2E_DEV u64 square_word(const u32 *__restrict__ in32, size_t n32, u64 r, u64 h,
     return v;
 }
 
-// Four consecutive output words, one window: XOR the 32-bit input windows
-// starting at in32[b + q] bit `sh` (q = 0..3) into acc.  Five coalesced
-// 32-bit loads serve four words.
-template <bool GUARD>
-GF2E_DEV void window4(const u32 *__restrict__ in32, u32 n32, u32 b, u32 sh, u32 (&acc)[4]) {
-    u32 x[5];
-#pragma unroll
-    for (int q = 0; q < 5; q++) x[q] = (!GUARD || b + q < n32) ? __ldg(in32 + b + q) : 0u;
-#pragma unroll
-    for (int q = 0; q < 4; q++) acc[q] ^= __funnelshift_r(x[q], x[q + 1], sh);
+constexpr int WPT = 8;          // output words per thread on the fast path
+
+// interleave two 16-bit values (low halves of e, o): bit 2i <- e_i,
+// bit 2i+1 <- o_i.  One byte permute places [e.b0, o.b0, e.b1, o.b1], then
+// three delta swaps finish the outer perfect shuffle inside each 16 bits.
+GF2E_DEV u32 shuffle16(u32 x) {
+    u32 t = (x ^ (x >> 4)) & 0x00F000F0u;
+    x ^= t ^ (t << 4);
+    t = (x ^ (x >> 2)) & 0x0C0C0C0Cu;
+    x ^= t ^ (t << 2);
+    t = (x ^ (x >> 1)) & 0x22222222u;
+    x ^= t ^ (t << 1);
+    return x;
+}
+// spread(e) ^ (spread(o) << 1) as one 64-bit word
+GF2E_DEV u64 interleave32(u32 e, u32 o) {
+    u32 lo = shuffle16(__byte_perm(e, o, 0x5140));
+    u32 hi = shuffle16(__byte_perm(e, o, 0x7362));
+    return ((u64)hi << 32) | lo;
 }
 
 // batched squaring: blockIdx.y = state; each thread writes four words.
@@ -99,26 +108,44 @@ GF2E_DEV void window4(const u32 *__restrict__ in32, u32 n32, u32 b, u32 sh, u32 
 // Groups of four words away from every window boundary take this path
 // (32-bit index arithmetic, hoisted offsets, no clipping); the few groups
 // that touch a boundary use the clipped per-word form above.
-template <bool SODD>
-GF2E_DEV void square_group_fast(const u32 *__restrict__ in32, u32 n32, u32 w0, bool t1_on,
-                                bool t3_on, bool t4_on, bool t5_on, u32 K2, u32 K3, u32 K4, u32 K5,
-                                u64 *__restrict__ o) {
-    u32 E[4] = {0, 0, 0, 0}, O[4] = {0, 0, 0, 0};
-    if (t1_on) {
-        uint4 a = __ldg(reinterpret_cast<const uint4 *>(in32 + w0));
-        E[0] = a.x; E[1] = a.y; E[2] = a.z; E[3] = a.w;
-    }
-    window4<false>(in32, n32, w0 + (K2 >> 5), K2 & 31, O);
-    if (t3_on) window4<false>(in32, n32, w0 + (K3 >> 5), K3 & 31, SODD ? E : O);
-    if (t4_on) window4<true>(in32, n32, w0 + (K4 >> 5), K4 & 31, SODD ? O : E);
-    if (t5_on) window4<true>(in32, n32, w0 + (K5 >> 5), K5 & 31, E);
-    u64 v[4];
+// One window for the WPT words of a lane in a warp tile (words
+// w0 + lane + 32q): two coalesced 32-bit loads and a funnel shift per word.
+template <bool GUARD>
+GF2E_DEV void window_strided(const u32 *__restrict__ in32, u32 n32, u32 b, u32 sh,
+                             u32 (&acc)[WPT]) {
 #pragma unroll
-    for (int q = 0; q < 4; q++) v[q] = spread32(E[q]) ^ (spread32(O[q]) << 1);
-    reinterpret_cast<ulonglong2 *>(o + w0)[0] = make_ulonglong2(v[0], v[1]);
-    reinterpret_cast<ulonglong2 *>(o + w0)[1] = make_ulonglong2(v[2], v[3]);
+    for (int q = 0; q < WPT; q++) {
+        const u32 i = b + 32 * q;
+        u32 lo = (!GUARD || i < n32) ? __ldg(in32 + i) : 0u;
+        u32 hi = (!GUARD || i + 1 < n32) ? __ldg(in32 + i + 1) : 0u;
+        acc[q] ^= __funnelshift_r(lo, hi, sh);
+    }
 }
 
+// A clean warp tile of 32*WPT words: lane handles words w0 + lane + 32q, so
+// every load and store instruction of the warp touches consecutive words.
+template <bool SODD>
+GF2E_DEV void square_tile_fast(const u32 *__restrict__ in32, u32 n32, u32 w0, u32 lane,
+                               bool t1_on, bool t3_on, bool t4_on, bool t5_on, u32 K2, u32 K3,
+                               u32 K4, u32 K5, u64 *__restrict__ o) {
+    u32 E[WPT], O[WPT];
+    const u32 wl = w0 + lane;
+#pragma unroll
+    for (int q = 0; q < WPT; q++) {
+        E[q] = t1_on ? __ldg(in32 + wl + 32 * q) : 0u;
+        O[q] = 0;
+    }
+    window_strided<false>(in32, n32, wl + (K2 >> 5), K2 & 31, O);
+    if (t3_on) window_strided<false>(in32, n32, wl + (K3 >> 5), K3 & 31, SODD ? E : O);
+    if (t4_on) window_strided<true>(in32, n32, wl + (K4 >> 5), K4 & 31, SODD ? O : E);
+    if (t5_on) window_strided<true>(in32, n32, wl + (K5 >> 5), K5 & 31, E);
+#pragma unroll
+    for (int q = 0; q < WPT; q++) o[wl + 32 * q] = interleave32(E[q], O[q]);
+}
+
+// Batched squaring: blockIdx.y = state, each thread WPT consecutive words.
+// All clean-group conditions use 32-bit arithmetic (bit positions < 2^32
+// for r < 2^31); larger r take the clipped per-word path throughout.
 __global__ void __launch_bounds__(256, 4)
 k_square_batch(const u64 *__restrict__ in, u64 *__restrict__ out, size_t stride,
                u64 r, const u64 *__restrict__ s_arr, u64 s_uniform) {
@@ -135,29 +162,38 @@ k_square_batch(const u64 *__restrict__ in, u64 *__restrict__ out, size_t stride,
     const u32 K4 = (u32)(h + ((r - s) >> 1));              // S >> (r-s-1)
     const u32 K5 = (u32)(h + ((r - 2 * s) >> 1));          // (S >> (r-s-1)) << s
     const bool sodd = (s & 1) != 0;
-    const u32 ngroups = (nw + 3) >> 2;
-    for (u32 g = blockIdx.x * blockDim.x + threadIdx.x; g < ngroups;
-         g += gridDim.x * blockDim.x) {
-        const u32 w0 = 4 * g;
-        const u64 b0 = (u64)w0 << 6, b3 = b0 + 192;
-        const bool t1_on = 32 * (u64)(w0 + 4) <= h, t1_off = 32 * (u64)w0 >= h;
-        const bool t4_on = b3 + 1 < s, t4_off = b0 + 1 >= s;
-        const bool t5_on = b0 >= s && b3 + 1 < 2 * s;
-        const bool t5_off = b3 + 64 <= s || b0 + 1 >= 2 * s;
-        // S<<(s+1): whole windows above bit 0 of S, or entirely below it (zero)
-        const bool t3_on = 32 * (u64)w0 >= ((s + 1) >> 1);
-        const bool t3_off = b3 + 64 <= s + 1;
-        const bool clean = (w0 + 5 <= nw) && (t1_on || t1_off) && (t3_on || t3_off) &&
-                           (t4_on || t4_off) && (t5_on || t5_off) && r < (1ull << 31);
+    const bool small_r = r < (1ull << 31);
+    const u32 s32 = (u32)s, h32 = (u32)h, c3 = (u32)((s + 1) >> 1);
+    // warp tiles of TW words; the clean test is the same for the whole warp
+    constexpr u32 TW = 32 * WPT;
+    const u32 lane = threadIdx.x & 31;
+    const u32 ntiles = (nw + TW - 1) / TW;
+    const u32 warps_total = (gridDim.x * blockDim.x) >> 5;
+    for (u32 t = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; t < ntiles; t += warps_total) {
+        const u32 w0 = TW * t;
+        bool clean = false, t1_on = false, t3_on = false, t4_on = false, t5_on = false;
+        if (small_r && w0 + TW + 1 <= nw) {
+            const u32 b0 = w0 << 6, bl = b0 + 64 * (TW - 1);      // first/last word bit
+            t1_on = 32 * (w0 + TW) <= h32;
+            const bool t1_off = 32 * w0 >= h32;
+            t4_on = bl + 1 < s32;
+            const bool t4_off = b0 + 1 >= s32;
+            t5_on = b0 >= s32 && bl + 1 < 2 * s32;
+            const bool t5_off = bl + 64 <= s32 || b0 + 1 >= 2 * s32;
+            t3_on = 32 * w0 >= c3;
+            const bool t3_off = bl + 64 <= s32 + 1;
+            clean = (t1_on || t1_off) && (t3_on || t3_off) && (t4_on || t4_off) &&
+                    (t5_on || t5_off);
+        }
         if (clean) {
             if (sodd)
-                square_group_fast<true>(in32, n32, w0, t1_on, t3_on, t4_on, t5_on, K2, K3, K4,
-                                        K5, o);
+                square_tile_fast<true>(in32, n32, w0, lane, t1_on, t3_on, t4_on, t5_on, K2, K3,
+                                       K4, K5, o);
             else
-                square_group_fast<false>(in32, n32, w0, t1_on, t3_on, t4_on, t5_on, K2, K3, K4,
-                                         K5, o);
+                square_tile_fast<false>(in32, n32, w0, lane, t1_on, t3_on, t4_on, t5_on, K2, K3,
+                                        K4, K5, o);
         } else {
-            for (u32 w = w0; w < w0 + 4 && w < nw; w++)
+            for (u32 w = w0 + lane; w < w0 + TW && w < nw; w += 32)
                 o[w] = square_word(in32, n32, r, h, s, w);
         }
     }
@@ -236,7 +272,7 @@ int launch_square(const u64 *in, u64 *out, size_t stride, int nstates, u64 r,
                   const u64 *s_dev, u64 s, cudaStream_t st) {
     const size_t nw = (size_t)((r + 63) >> 6);
     const int threads = 256;
-    size_t bx = (nw + 2 * threads - 1) / (2 * threads);
+    size_t bx = (nw + (size_t)WPT * threads - 1) / ((size_t)WPT * threads);
     if (bx > 65535) bx = 65535;
     dim3 grid((unsigned)bx, (unsigned)nstates);
     k_square_batch<<<grid, threads, 0, st>>>(in, out, stride, r, s_dev, s);
