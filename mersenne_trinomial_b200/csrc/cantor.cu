@@ -30,7 +30,7 @@ constexpr int TILE_LOG = 12;
 constexpr int TILE = 1 << TILE_LOG;        // elements per shared-memory tile
 constexpr int CMIN = 4;                    // minimum contiguous columns (32 B)
 constexpr int MAXOPS = 96;
-constexpr int FFT_THREADS = 256;
+constexpr int FFT_THREADS = 512;           // 2 CTAs x 64 registers per SM
 constexpr int NTWTAB = 4;                  // byte tables: t < 2^32
 
 enum OpType : u32 { TAY_F = 0, TAY_I = 1, BF_F = 2, BF_I = 3 };
@@ -55,6 +55,105 @@ GF2E_DEV u64 twiddle(const u64 *__restrict__ tab, u64 t) {
     return w;
 }
 
+// Tile rows are XOR-swizzled in shared memory so that the rows a warp
+// touches at power-of-two distances fall in different banks.  The swizzle
+// only permutes rows inside aligned groups of 16, so it is a bijection on
+// any power-of-two row count.
+GF2E_DEV u32 srow(u32 row) { return row ^ (((row >> 4) ^ (row >> 8) ^ (row >> 12)) & 15); }
+GF2E_DEV u32 sidx(u32 row, u32 col, u32 c_log) { return (srow(row) << c_log) + col; }
+
+// A stage applies K consecutive Taylor levels in registers.  Row quarters
+// q*2^(K-1) .. q (q = 2^lg rows): each thread holds the 2^(K+1) rows
+// row0 + j*q of one column, with row0 = blk * q * 2^(K+1) + i, i < q.
+// Forward goes from the largest blocks down, inverse the other way.
+template <bool FWD, int K>
+GF2E_DEV void taylor_stage(u64 *sm, u32 lg, u32 c_log, u32 tile_elems) {
+    constexpr int R = 2 << K;                       // rows per thread
+    const u32 C = 1u << c_log, q = 1u << lg;
+    const u32 ngroups = tile_elems / R;
+    for (u32 g = threadIdx.x; g < ngroups; g += FFT_THREADS) {
+        const u32 col = g & (C - 1), rest = g >> c_log;
+        const u32 i = rest & (q - 1), blk = rest >> lg;
+        const u32 row0 = (blk << (lg + K + 1)) + i;
+        u64 v[R];
+#pragma unroll
+        for (int j = 0; j < R; j++) v[j] = sm[sidx(row0 + j * q, col, c_log)];
+        if (FWD) {
+#pragma unroll
+            for (int lev = K - 1; lev >= 0; lev--) {
+                const int Q = 1 << lev;
+#pragma unroll
+                for (int o = 0; o < R; o += 4 * Q)
+#pragma unroll
+                    for (int ii = 0; ii < Q; ii++) {
+                        v[o + 2 * Q + ii] ^= v[o + 3 * Q + ii];
+                        v[o + Q + ii] ^= v[o + 2 * Q + ii];
+                    }
+            }
+        } else {
+#pragma unroll
+            for (int lev = 0; lev < K; lev++) {
+                const int Q = 1 << lev;
+#pragma unroll
+                for (int o = 0; o < R; o += 4 * Q)
+#pragma unroll
+                    for (int ii = 0; ii < Q; ii++) {
+                        v[o + Q + ii] ^= v[o + 2 * Q + ii];
+                        v[o + 2 * Q + ii] ^= v[o + 3 * Q + ii];
+                    }
+            }
+        }
+#pragma unroll
+        for (int j = 0; j < R; j++) sm[sidx(row0 + j * q, col, c_log)] = v[j];
+    }
+}
+
+// A stage of K consecutive butterfly levels in registers: row distances
+// D*2^(K-1) .. D (D = 2^lg rows, physical level Llo for distance D).  A
+// thread holds the 2^K rows row0 + j*D of one column.  The twiddle of the
+// pair at j in level Llo+lev is W[(Q0 + j) >> (lev+1)], Q0 = (base >> Llo) +
+// blk*2^K; Q0 is a multiple of 2^K, so by linearity of W it is
+// W[Q0 >> (lev+1)] ^ W[j >> (lev+1)], the second term from the first byte
+// table (j < 8).
+template <bool FWD, int K>
+GF2E_DEV void bfly_stage(u64 *sm, const u64 *__restrict__ tab, u32 lg, u32 Llo, u32 c_log,
+                         u32 tile_elems, u64 base) {
+    constexpr int R = 1 << K;
+    const u32 C = 1u << c_log, D = 1u << lg;
+    const u32 ngroups = tile_elems / R;
+    for (u32 g = threadIdx.x; g < ngroups; g += FFT_THREADS) {
+        const u32 col = g & (C - 1), rest = g >> c_log;
+        const u32 i = rest & (D - 1), blk = rest >> lg;
+        const u32 row0 = (blk << (lg + K)) + i;
+        const u64 Q0 = (base >> Llo) + ((u64)blk << K);
+        u64 v[R];
+#pragma unroll
+        for (int j = 0; j < R; j++) v[j] = sm[sidx(row0 + j * D, col, c_log)];
+#pragma unroll
+        for (int step = 0; step < K; step++) {
+            const int lev = FWD ? K - 1 - step : step;
+            const int Dj = 1 << lev;
+            const u64 tb = twiddle(tab, Q0 >> (lev + 1));
+#pragma unroll
+            for (int j = 0; j < R; j++) {
+                if (j & Dj) continue;
+                const u64 tw = tb ^ ((j >> (lev + 1)) ? __ldg(tab + (j >> (lev + 1))) : 0ull);
+                if (FWD) {
+                    u64 e = v[j] ^ gf64_mul(tw, v[j + Dj]);
+                    v[j + Dj] ^= e;
+                    v[j] = e;
+                } else {
+                    u64 hh = v[j] ^ v[j + Dj];
+                    v[j] ^= gf64_mul(tw, hh);
+                    v[j + Dj] = hh;
+                }
+            }
+        }
+#pragma unroll
+        for (int j = 0; j < R; j++) sm[sidx(row0 + j * D, col, c_log)] = v[j];
+    }
+}
+
 // Batch description for one pass: blockIdx.y selects the transform
 // (f + y*fstride) and its operand (src32 + y*sstride32).  xor0 is XORed into
 // chunk 0 of every packed operand (the running product multiplies by F + x).
@@ -67,7 +166,7 @@ struct Batch {
 // One pass over all tiles.  src32/nchunks: when non-null the tile is loaded
 // from 32-bit chunks of an operand (packing fused into the first pass),
 // zero beyond nchunks.
-__global__ void __launch_bounds__(FFT_THREADS)
+__global__ void __launch_bounds__(FFT_THREADS, 2)
 k_fft_pass(u64 *__restrict__ f, const u64 *__restrict__ tab, const Pass P, u64 ntiles,
            const u32 *__restrict__ src32, u64 nchunks, const Batch bt) {
     extern __shared__ u64 sm[];
@@ -109,56 +208,32 @@ k_fft_pass(u64 *__restrict__ f, const u64 *__restrict__ tab, const Pass P, u64 n
 #pragma unroll
             for (int j = 0; j < EPT; j++) {
                 u32 e = threadIdx.x + j * FFT_THREADS;
-                if (e < tile_elems) sm[e] = v[j];
+                if (e < tile_elems) sm[sidx(e >> P.c_log, e & (C - 1), P.c_log)] = v[j];
             }
         }
         __syncthreads();
         for (u32 k = 0; k < P.nops; k++) {
             const u32 op = P.ops[k];
-            const u32 type = op & 3, lg = (op >> 2) & 63, L = op >> 8;
-            if (type <= TAY_I) {
-                const u32 qr = 1u << lg;
-                const u32 ntrip = tile_elems >> 2;
-                for (u32 tau = threadIdx.x; tau < ntrip; tau += FFT_THREADS) {
-                    u32 col = tau & (C - 1), tt = tau >> P.c_log;
-                    u32 blk = tt >> lg, i = tt & (qr - 1);
-                    u32 r1 = (blk << (lg + 2)) + qr + i;
-                    u32 i1 = (r1 << P.c_log) + col, i2 = i1 + (qr << P.c_log),
-                        i3 = i2 + (qr << P.c_log);
-                    u64 a = sm[i1], b = sm[i2], c = sm[i3];
-                    if (type == TAY_F) { b ^= c; a ^= b; }
-                    else { a ^= b; b ^= c; }
-                    sm[i1] = a;
-                    sm[i2] = b;
-                }
-            } else {
-                const u32 D = 1u << lg;
-                const u32 npair = tile_elems >> 1;
-                for (u32 tau = threadIdx.x; tau < npair; tau += FFT_THREADS) {
-                    u32 col = tau & (C - 1), pp = tau >> P.c_log;
-                    u32 ra = ((pp >> lg) << (lg + 1)) + (pp & (D - 1));
-                    u32 ia = (ra << P.c_log) + col, ib = ia + (D << P.c_log);
-                    // physical index of (row ra, column 0); the window of a
-                    // multi-window tile is folded into the row count
-                    u64 phys = base + (u64)ra * P.CH;
-                    u64 tw = twiddle(tab, phys >> (L + 1));
-                    u64 e1 = sm[ia], e2 = sm[ib];
-                    if (type == BF_F) {
-                        u64 e = e1 ^ gf64_mul(tw, e2);
-                        sm[ia] = e;
-                        sm[ib] = e ^ e2;
-                    } else {
-                        u64 hh = e1 ^ e2;
-                        sm[ia] = e1 ^ gf64_mul(tw, hh);
-                        sm[ib] = hh;
-                    }
-                }
+            const u32 type = op & 3, lg = (op >> 2) & 63, L = (op >> 8) & 127;
+            const u32 K = ((op >> 15) & 3) + 1;
+            switch (type * 4 + K) {
+            case TAY_F * 4 + 1: taylor_stage<true, 1>(sm, lg, P.c_log, tile_elems); break;
+            case TAY_F * 4 + 2: taylor_stage<true, 2>(sm, lg, P.c_log, tile_elems); break;
+            case TAY_F * 4 + 3: taylor_stage<true, 3>(sm, lg, P.c_log, tile_elems); break;
+            case TAY_I * 4 + 1: taylor_stage<false, 1>(sm, lg, P.c_log, tile_elems); break;
+            case TAY_I * 4 + 2: taylor_stage<false, 2>(sm, lg, P.c_log, tile_elems); break;
+            case TAY_I * 4 + 3: taylor_stage<false, 3>(sm, lg, P.c_log, tile_elems); break;
+            case BF_F * 4 + 1: bfly_stage<true, 1>(sm, tab, lg, L, P.c_log, tile_elems, base); break;
+            case BF_F * 4 + 2: bfly_stage<true, 2>(sm, tab, lg, L, P.c_log, tile_elems, base); break;
+            case BF_I * 4 + 1: bfly_stage<false, 1>(sm, tab, lg, L, P.c_log, tile_elems, base); break;
+            case BF_I * 4 + 2: bfly_stage<false, 2>(sm, tab, lg, L, P.c_log, tile_elems, base); break;
+            default: break;                    // butterfly stages hold at most 2 levels
             }
             __syncthreads();
         }
         for (u32 e = threadIdx.x; e < tile_elems; e += FFT_THREADS) {
             u32 row = e >> P.c_log, col = e & (C - 1);
-            f[base + (u64)row * P.CH + col] = sm[e];
+            f[base + (u64)row * P.CH + col] = sm[sidx(row, col, P.c_log)];
         }
         __syncthreads();
     }
@@ -280,6 +355,35 @@ struct PlanImpl {
     std::vector<u64> ntiles_fwd, ntiles_inv;
 };
 
+// Merge runs of up to three single-level ops of one kind into register
+// stages: forward kinds come with the level (lg) falling by one per op,
+// inverse kinds with it rising; a stage is encoded by its lowest lg and L
+// and its level count K (bits 15-16 hold K-1).
+void merge_stages(Pass &p) {
+    u32 out[MAXOPS];
+    u32 n = 0;
+    for (u32 k = 0; k < p.nops;) {
+        const u32 op = p.ops[k], type = op & 3, lg = (op >> 2) & 63, L = (op >> 8) & 127;
+        const bool fwd = (type == TAY_F || type == BF_F);
+        u32 run = 1;
+        const u32 max_run = (type >= BF_F) ? 2 : 3;   // register budget of a stage
+        while (run < max_run && k + run < p.nops) {
+            const u32 o2 = p.ops[k + run];
+            const u32 lg2 = (o2 >> 2) & 63, L2 = (o2 >> 8) & 127;
+            const int want = fwd ? -(int)run : (int)run;
+            if ((o2 & 3) != type || (int)lg2 - (int)lg != want) break;
+            if (type >= BF_F && (int)L2 - (int)L != want) break;
+            run++;
+        }
+        const u32 lo_lg = fwd ? lg - (run - 1) : lg;
+        const u32 lo_L = (type >= BF_F) ? (fwd ? L - (run - 1) : L) : 0;
+        out[n++] = mkop(type, lo_lg, lo_L) | ((run - 1) << 15);
+        k += run;
+    }
+    for (u32 k = 0; k < n; k++) p.ops[k] = out[k];
+    p.nops = n;
+}
+
 u64 pass_tiles(const Pass &p, u64 n) {
     u64 elems = ((u64)1 << (p.ns_log + p.c_log + p.wpt_log));
     return n / elems;
@@ -372,6 +476,8 @@ void build_passes(PlanImpl &P) {
     for (size_t i = inv.size() - 1; i-- > 0;) inv_all.push_back(inv[i]);
     P.fwd = fwd;
     P.inv = inv_all;
+    for (auto &p : P.fwd) merge_stages(p);
+    for (auto &p : P.inv) merge_stages(p);
     for (auto &p : P.fwd) P.ntiles_fwd.push_back(pass_tiles(p, n));
     for (auto &p : P.inv) P.ntiles_inv.push_back(pass_tiles(p, n));
 }

@@ -59,6 +59,13 @@ struct gf2e_scanner {
     std::vector<int64_t> degs;
     std::vector<gf2e_gcd_job> jobs;
     u64 degree_steps = 0, sd_pairs = 0;
+    // the per-degree launches (squaring, transforms, products, folds) are
+    // replayed from CUDA graphs, one per (resident count, F buffer)
+    cudaStream_t own = nullptr;
+    cudaEvent_t ev_in = nullptr, ev_out = nullptr;
+    struct GraphKey { int nact; const u64 *F; };
+    std::vector<std::pair<GraphKey, cudaGraphExec_t>> graphs;
+    bool use_graphs = true;
 };
 
 namespace {
@@ -139,20 +146,52 @@ int fill_slots(gf2e_scanner &S, cudaStream_t st) {
     return GF2E_OK;
 }
 
-// one degree for all resident s, then the interval-end gcds
-int degree_step(gf2e_scanner &S, cudaStream_t st) {
-    const int na = S.nact;
-    GF2E_TRY(gf2e::trin_square_states(S.F, S.Fs, S.stride, na, S.r, S.sdev, st));
-    std::swap(S.F, S.Fs);
+// the launches of one degree for `na` resident s (F -> Fs squared; the
+// product then reads Fs, which becomes F)
+int degree_kernels(gf2e_scanner &S, int na, u64 *F, u64 *Fs, cudaStream_t st) {
+    GF2E_TRY(gf2e::trin_square_states(F, Fs, S.stride, na, S.r, S.sdev, st));
     GF2E_TRY(gf2e::fft_fwd_packed_batch(S.plan, S.FA, S.n, reinterpret_cast<const u32 *>(S.ACC),
                                         2 * S.stride, S.nchunks, 0, na, st));
-    GF2E_TRY(gf2e::fft_fwd_packed_batch(S.plan, S.FB, S.n, reinterpret_cast<const u32 *>(S.F),
+    GF2E_TRY(gf2e::fft_fwd_packed_batch(S.plan, S.FB, S.n, reinterpret_cast<const u32 *>(Fs),
                                         2 * S.stride, S.nchunks, 2, na, st));
     GF2E_TRY(gf2e::pointwise(S.FA, S.FB, S.n * na, st));
     GF2E_TRY(gf2e::fft_run_batch(S.plan, false, S.FA, S.n, na, st));
     GF2E_TRY(gf2e::overlap_add_batch(S.FA, S.n, 2 * S.nchunks - 1, S.P, S.pstride, S.ow, na, st));
     GF2E_TRY(gf2e::trin_reduce_batch(S.P, S.pstride, S.ow, 2 * S.r - 1, S.ACC, S.stride, S.r,
                                      S.sdev, na, st));
+    return GF2E_OK;
+}
+
+int launch_degree(gf2e_scanner &S, cudaStream_t st) {
+    const int na = S.nact;
+    if (!S.use_graphs || st != S.own) return degree_kernels(S, na, S.F, S.Fs, st);
+    for (auto &g : S.graphs)
+        if (g.first.nact == na && g.first.F == S.F)
+            return gf2e::cuda_status(cudaGraphLaunch(g.second, st), "degree graph launch");
+    cudaGraph_t graph = nullptr;
+    cudaError_t e = cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal);
+    if (e != cudaSuccess) return gf2e::cuda_status(e, "degree graph capture");
+    int status = degree_kernels(S, na, S.F, S.Fs, st);
+    e = cudaStreamEndCapture(st, &graph);
+    if (status != GF2E_OK) { if (graph) cudaGraphDestroy(graph); return status; }
+    if (e != cudaSuccess) return gf2e::cuda_status(e, "degree graph end capture");
+    cudaGraphExec_t exec = nullptr;
+    e = cudaGraphInstantiate(&exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (e != cudaSuccess) return gf2e::cuda_status(e, "degree graph instantiate");
+    if (S.graphs.size() >= 64) {                 // bounded cache
+        cudaGraphExecDestroy(S.graphs.front().second);
+        S.graphs.erase(S.graphs.begin());
+    }
+    S.graphs.push_back({gf2e_scanner::GraphKey{na, S.F}, exec});
+    return gf2e::cuda_status(cudaGraphLaunch(exec, st), "degree graph launch");
+}
+
+// one degree for all resident s, then the interval-end gcds
+int degree_step(gf2e_scanner &S, cudaStream_t st) {
+    const int na = S.nact;
+    GF2E_TRY(launch_degree(S, st));
+    std::swap(S.F, S.Fs);
     S.degree_steps++;
     S.sd_pairs += (u64)na;
     std::vector<int> due;
@@ -265,6 +304,14 @@ int gf2e_scanner_create(uint64_t r, int slots, gf2e_scanner **out) {
         delete S;
         return st;
     }
+    e = cudaStreamCreateWithFlags(&S->own, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&S->ev_in, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&S->ev_out, cudaEventDisableTiming);
+    if (e != cudaSuccess) {
+        gf2e_scanner_destroy(S);
+        return gf2e::cuda_status(e, "scanner stream");
+    }
+    if (const char *env = getenv("GF2E_SCAN_GRAPHS")) S->use_graphs = env[0] != '0';
     S->slot.resize(B);
     S->shost.assign(B, 0);
     S->thost.assign(g.tw, 0);
@@ -277,6 +324,11 @@ int gf2e_scanner_create(uint64_t r, int slots, gf2e_scanner **out) {
 
 int gf2e_scanner_destroy(gf2e_scanner *S) {
     if (!S) return GF2E_OK;
+    if (S->own) cudaStreamSynchronize(S->own);
+    for (auto &g : S->graphs) cudaGraphExecDestroy(g.second);
+    if (S->ev_in) cudaEventDestroy(S->ev_in);
+    if (S->ev_out) cudaEventDestroy(S->ev_out);
+    if (S->own) cudaStreamDestroy(S->own);
     cudaFree(S->gws);
     cudaFree(S->dmem);
     delete S;
@@ -301,10 +353,18 @@ int gf2e_scanner_submit(gf2e_scanner *S, const uint64_t *s_host, int ns, uint64_
 
 int gf2e_scanner_step(gf2e_scanner *S, int degrees, void *stream) {
     if (!S || degrees < 0) return gf2e::invalid("scanner step: bad arguments");
-    cudaStream_t st = (cudaStream_t)stream;
-    GF2E_TRY(fill_slots(*S, st));
-    for (int i = 0; i < degrees && S->nact > 0; i++) GF2E_TRY(degree_step(*S, st));
-    return GF2E_OK;
+    // work runs on the scanner's own stream (graphs are captured there),
+    // ordered after and before the caller's stream
+    cudaStream_t caller = (cudaStream_t)stream;
+    cudaError_t e = cudaEventRecord(S->ev_in, caller);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(S->own, S->ev_in, 0);
+    if (e != cudaSuccess) return gf2e::cuda_status(e, "scanner stream order");
+    int st = fill_slots(*S, S->own);
+    for (int i = 0; st == GF2E_OK && i < degrees && S->nact > 0; i++) st = degree_step(*S, S->own);
+    e = cudaEventRecord(S->ev_out, S->own);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(caller, S->ev_out, 0);
+    if (st != GF2E_OK) return st;
+    return gf2e::cuda_status(e, "scanner stream order");
 }
 
 int gf2e_scanner_status(const gf2e_scanner *S, int *queued, int *resident, int *finished,
