@@ -325,6 +325,57 @@ int gf2e_trin_reduce_T0(gf2e_trin *ctx, uint64_t *dst_dev, uint64_t L,
 /* ACC <- ACC * (F + x) mod T (TrinGPU::accumulate). */
 int gf2e_trin_accumulate(gf2e_trin *ctx, void *stream);
 
+/* ======================================================================
+ * Tuning and the autotuner.  Replaces the reference's runtime FFT knobs
+ * (gf2c_taylor_lv / gf2c_bfly_lv, gf2_cantor_cuda.h:24-60, environment
+ * GF2C_TAYLOR_LV / GF2C_BFLY_LV) and tsfactor's "--bench" FFT autotune
+ * (tsfactor.cu:1986-2080): every candidate is verified on the device
+ * against the default configuration (forward transform word-equal, inverse
+ * round trip) before it is timed, the fastest is left active, and its
+ * settings are returned (and printed by the Python tool as export lines).
+ *
+ * The tuning is process-wide.  FFT plans and the sieve read it when they
+ * are created / launched, so a change affects plans made afterwards (the
+ * internal plan cache is keyed by it).  Environment overrides read on first
+ * use: GF2E_FFT_TILE_LOG, GF2E_FFT_CMIN, GF2E_FFT_TAYLOR_LV,
+ * GF2E_FFT_BFLY_LV, GF2E_SIEVE_STRIP_LOG.
+ * ====================================================================== */
+typedef struct gf2e_tune {
+    int fft_tile_log;    /* log2 elements per shared-memory tile, 11..13 */
+    int fft_cmin;        /* least contiguous columns per tile row: 1, 2, 4, 8, 16 */
+    int fft_taylor_lv;   /* Taylor levels fused per register stage, 1..3 */
+    int fft_bfly_lv;     /* butterfly levels fused per register stage, 1..2 */
+    int sieve_strip_log; /* log2 best[] entries per strip CTA, 10..14 */
+} gf2e_tune;
+
+int gf2e_tune_default(gf2e_tune *t);          /* built-in defaults */
+int gf2e_tune_get(gf2e_tune *t);              /* current (env applied) */
+int gf2e_tune_set(const gf2e_tune *t);        /* validated; INVALID if out of range */
+
+/* FFT autotune at size 2^m: candidates over tile size, column floor and
+ * stage depths.  best_ms = fwd + inv time of the winner.  report (may be
+ * NULL) receives one line per candidate: "tile cmin tlv blv ms ok". */
+int gf2e_fft_autotune(int m, int reps, gf2e_tune *best, double *best_ms,
+                      char *report, size_t report_cap);
+
+/* Sieve strip-width autotune: runs gf2e_sieve_run(r, 2, dmax, smax) with
+ * each strip width, checks the best[] array is identical to the default's,
+ * keeps the fastest.  Needs free device memory for two best[] arrays. */
+int gf2e_sieve_autotune(uint64_t r, int dmax, uint64_t smax, int reps,
+                        gf2e_tune *best, double *best_ms, char *report,
+                        size_t report_cap);
+
+/* gcd interval schedule for the deep scan (trinomial_scan.cu:175 uses
+ * L0 = 64 doubling to 4096).  Given the measured cost of one scanned degree
+ * (t_degree) and of one interval-end gcd (t_gcd), in any common unit, picks
+ * L0 and Lmax (powers of two, L0 <= Lmax) minimising the expected cost of
+ * scanning one survivor of a k0-deep sieve up to maxd, under the model that
+ * the least factor degree d exceeds D with probability k0 / D.  Pure host
+ * arithmetic. */
+int gf2e_scan_choose_interval(uint64_t k0, uint64_t maxd, double t_degree,
+                              double t_gcd, uint64_t *L0, uint64_t *Lmax,
+                              double *expected_cost);
+
 #ifdef __cplusplus
 }
 #endif

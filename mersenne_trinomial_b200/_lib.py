@@ -47,6 +47,14 @@ class MulJob(C.Structure):
                 ("bbits", C.c_uint64), ("out_dev", C.c_void_p)]
 
 
+class Tune(C.Structure):
+    _fields_ = [("fft_tile_log", C.c_int), ("fft_cmin", C.c_int), ("fft_taylor_lv", C.c_int),
+                ("fft_bfly_lv", C.c_int), ("sieve_strip_log", C.c_int)]
+
+    def as_dict(self) -> dict:
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
 _lib = None
 _lock = threading.Lock()
 
@@ -117,6 +125,14 @@ SIGNATURES = {
     "gf2e_trin_mul_dev": (_i32, [_vp, _vp, _vp, _vp]),
     "gf2e_trin_reduce_T0": (_i32, [_vp, _vp, _u64, _vp]),
     "gf2e_trin_accumulate": (_i32, [_vp, _vp]),
+    "gf2e_tune_default": (_i32, [_P(Tune)]),
+    "gf2e_tune_get": (_i32, [_P(Tune)]),
+    "gf2e_tune_set": (_i32, [_P(Tune)]),
+    "gf2e_fft_autotune": (_i32, [_i32, _i32, _P(Tune), _P(C.c_double), C.c_char_p, _sz]),
+    "gf2e_sieve_autotune": (_i32, [_u64, _i32, _u64, _i32, _P(Tune), _P(C.c_double),
+                                   C.c_char_p, _sz]),
+    "gf2e_scan_choose_interval": (_i32, [_u64, _u64, C.c_double, C.c_double, _P(_u64),
+                                         _P(_u64), _P(C.c_double)]),
 }
 
 

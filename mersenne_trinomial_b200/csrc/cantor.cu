@@ -26,9 +26,8 @@
 
 namespace {
 
-constexpr int TILE_LOG = 12;
-constexpr int TILE = 1 << TILE_LOG;        // elements per shared-memory tile
-constexpr int CMIN = 4;                    // minimum contiguous columns (32 B)
+constexpr int TILE_LOG_MIN = 11;           // shared-memory tile sizes a plan may use:
+constexpr int TILE_LOG_MAX = 13;           // 2^11..2^13 elements (16..64 KB)
 constexpr int MAXOPS = 96;
 constexpr int FFT_THREADS = 512;           // 2 CTAs x 64 registers per SM
 constexpr int NTWTAB = 4;                  // byte tables: t < 2^32
@@ -166,6 +165,7 @@ struct Batch {
 // One pass over all tiles.  src32/nchunks: when non-null the tile is loaded
 // from 32-bit chunks of an operand (packing fused into the first pass),
 // zero beyond nchunks.
+template <int TL>
 __global__ void __launch_bounds__(FFT_THREADS, 2)
 k_fft_pass(u64 *__restrict__ f, const u64 *__restrict__ tab, const Pass P, u64 ntiles,
            const u32 *__restrict__ src32, u64 nchunks, const Batch bt) {
@@ -186,13 +186,15 @@ k_fft_pass(u64 *__restrict__ f, const u64 *__restrict__ tab, const Pass P, u64 n
             u64 win = tile / cgroups, cg = tile - win * cgroups;
             base = win * ((u64)NS * P.CH) + cg * C;
         }
-        // load: every thread issues all of its loads before the first use
-        {
-            constexpr int EPT = TILE / FFT_THREADS;
-            u64 v[EPT];
+        // load: every thread issues a batch of loads before the first use
+        constexpr int EPT = (1 << TL) / FFT_THREADS;
+        constexpr int BATCH = EPT < 8 ? EPT : 8;
 #pragma unroll
-            for (int j = 0; j < EPT; j++) {
-                u32 e = threadIdx.x + j * FFT_THREADS;
+        for (int j0 = 0; j0 < EPT; j0 += BATCH) {
+            u64 v[BATCH];
+#pragma unroll
+            for (int j = 0; j < BATCH; j++) {
+                u32 e = threadIdx.x + (j0 + j) * FFT_THREADS;
                 v[j] = 0;
                 if (e < tile_elems) {
                     u32 row = e >> P.c_log, col = e & (C - 1);
@@ -206,8 +208,8 @@ k_fft_pass(u64 *__restrict__ f, const u64 *__restrict__ tab, const Pass P, u64 n
                 }
             }
 #pragma unroll
-            for (int j = 0; j < EPT; j++) {
-                u32 e = threadIdx.x + j * FFT_THREADS;
+            for (int j = 0; j < BATCH; j++) {
+                u32 e = threadIdx.x + (j0 + j) * FFT_THREADS;
                 if (e < tile_elems) sm[sidx(e >> P.c_log, e & (C - 1), P.c_log)] = v[j];
             }
         }
@@ -321,16 +323,17 @@ const u64 *basis_host() {
 }
 
 // smallest column count fitting the tile, or 0 if the group does not fit
-u32 choose_c(u64 CH, u64 NS) {
-    if (NS > (u64)TILE) return 0;
-    u64 c = std::min<u64>(CH, (u64)TILE / NS);
-    if (c < CMIN && c != CH) return 0;
+u32 choose_c(u64 CH, u64 NS, const gf2e_tune &cfg) {
+    const u64 tile = (u64)1 << cfg.fft_tile_log;
+    if (NS > tile) return 0;
+    u64 c = std::min<u64>(CH, tile / NS);
+    if (c < (u64)cfg.fft_cmin && c != CH) return 0;
     return (u32)c;
 }
 
 int ilog2u(u64 v) { return 63 - __builtin_clzll(v); }
 
-Pass make_pass(u64 CH, u64 NS, u32 C, u64 n) {
+Pass make_pass(u64 CH, u64 NS, u32 C, u64 n, const gf2e_tune &cfg) {
     Pass p;
     memset(&p, 0, sizeof p);
     p.CH = CH;
@@ -339,7 +342,7 @@ Pass make_pass(u64 CH, u64 NS, u32 C, u64 n) {
     // whole windows: pack several into one tile (never more than exist)
     if ((u64)C == CH) {
         u64 win_elems = NS * CH;
-        u64 wpt = std::min<u64>((u64)TILE / win_elems, n / win_elems);
+        u64 wpt = std::min<u64>(((u64)1 << cfg.fft_tile_log) / win_elems, n / win_elems);
         if (wpt < 1) wpt = 1;
         p.wpt_log = (u32)ilog2u(wpt);
     }
@@ -349,6 +352,7 @@ Pass make_pass(u64 CH, u64 NS, u32 C, u64 n) {
 struct PlanImpl {
     int m = 0;
     u64 n = 0;
+    gf2e_tune cfg{};                     // tile size and stage depths the passes use
     u64 *d_tab = nullptr;                // owned NTWTAB x 256 twiddle byte tables
     const u64 *tab = nullptr;            // tables the passes read (d_tab or caller's)
     std::vector<Pass> fwd, inv;
@@ -359,14 +363,14 @@ struct PlanImpl {
 // stages: forward kinds come with the level (lg) falling by one per op,
 // inverse kinds with it rising; a stage is encoded by its lowest lg and L
 // and its level count K (bits 15-16 hold K-1).
-void merge_stages(Pass &p) {
+void merge_stages(Pass &p, const gf2e_tune &cfg) {
     u32 out[MAXOPS];
     u32 n = 0;
     for (u32 k = 0; k < p.nops;) {
         const u32 op = p.ops[k], type = op & 3, lg = (op >> 2) & 63, L = (op >> 8) & 127;
         const bool fwd = (type == TAY_F || type == BF_F);
         u32 run = 1;
-        const u32 max_run = (type >= BF_F) ? 2 : 3;   // register budget of a stage
+        const u32 max_run = (u32)((type >= BF_F) ? cfg.fft_bfly_lv : cfg.fft_taylor_lv);
         while (run < max_run && k + run < p.nops) {
             const u32 o2 = p.ops[k + run];
             const u32 lg2 = (o2 >> 2) & 63, L2 = (o2 >> 8) & 127;
@@ -392,13 +396,17 @@ u64 pass_tiles(const Pass &p, u64 n) {
 void build_passes(PlanImpl &P) {
     const int m = P.m;
     const u64 n = P.n;
+    const gf2e_tune &cfg = P.cfg;
+    const u64 TILE = (u64)1 << cfg.fft_tile_log;
+    auto choose = [&](u64 CH, u64 NS) { return choose_c(CH, NS, cfg); };
+    auto mk = [&](u64 CH, u64 NS, u32 C) { return make_pass(CH, NS, C, n, cfg); };
     // deep depth L0: smallest L0 at which n >> L0 rows x C columns fit
     int L0 = 0;
     u32 Cd = 0;
     for (L0 = 0; L0 <= m; L0++) {
         u64 rows = n >> L0;
-        if (rows > (u64)TILE) continue;
-        Cd = choose_c((u64)1 << L0, rows);
+        if (rows > TILE) continue;
+        Cd = choose((u64)1 << L0, rows);
         if (Cd) break;
     }
     if (L0 > m - 1) L0 = m - 1;            // n <= 2: degenerate
@@ -413,11 +421,11 @@ void build_passes(PlanImpl &P) {
             for (int b_lo = 2; b_lo <= b_hi; b_lo++) {
                 u64 CH = (u64)1 << (b_lo - 2 + L);
                 u64 NS = (u64)1 << (b_hi - b_lo + 2);
-                if (b_hi - b_lo + 1 <= MAXOPS && choose_c(CH, NS)) { best_lo = b_lo; break; }
+                if (b_hi - b_lo + 1 <= MAXOPS && choose(CH, NS)) { best_lo = b_lo; break; }
             }
             u64 CH = (u64)1 << (best_lo - 2 + L);
             u64 NS = (u64)1 << (b_hi - best_lo + 2);
-            Pass pf = make_pass(CH, NS, choose_c(CH, NS), n);
+            Pass pf = mk(CH, NS, choose(CH, NS));
             Pass pi = pf;
             for (int b = b_hi; b >= best_lo; b--) pf.ops[pf.nops++] = mkop(TAY_F, b - best_lo, 0);
             for (int b = best_lo; b <= b_hi; b++) pi.ops[pi.nops++] = mkop(TAY_I, b - best_lo, 0);
@@ -430,7 +438,7 @@ void build_passes(PlanImpl &P) {
     {
         const int mp = m - L0;
         u64 CH = (u64)1 << L0, NS = n >> L0;
-        Pass pf = make_pass(CH, NS, Cd, n);
+        Pass pf = mk(CH, NS, Cd);
         Pass pi = pf;
         for (int Lp = 0; Lp <= mp - 2; Lp++)
             for (int e = mp - 2; e >= Lp; e--) pf.ops[pf.nops++] = mkop(TAY_F, e, 0);
@@ -449,7 +457,7 @@ void build_passes(PlanImpl &P) {
             int best_hi = L_lo;
             for (int L_hi = L0 - 1; L_hi >= L_lo; L_hi--) {
                 u64 CH = (u64)1 << L_lo, NS = (u64)1 << (L_hi - L_lo + 1);
-                if (choose_c(CH, NS)) { best_hi = L_hi; break; }
+                if (choose(CH, NS)) { best_hi = L_hi; break; }
             }
             groups.push_back({L_lo, best_hi});
             L_lo = best_hi + 1;
@@ -458,7 +466,7 @@ void build_passes(PlanImpl &P) {
     for (size_t gi = groups.size(); gi-- > 0;) {          // forward: top group first
         int L_lo = groups[gi].first, L_hi = groups[gi].second;
         u64 CH = (u64)1 << L_lo, NS = (u64)1 << (L_hi - L_lo + 1);
-        Pass pf = make_pass(CH, NS, choose_c(CH, NS), n);
+        Pass pf = mk(CH, NS, choose(CH, NS));
         for (int L = L_hi; L >= L_lo; L--) pf.ops[pf.nops++] = mkop(BF_F, L - L_lo, L);
         fwd.push_back(pf);
     }
@@ -466,7 +474,7 @@ void build_passes(PlanImpl &P) {
     for (size_t gi = 0; gi < groups.size(); gi++) {       // inverse: bottom group first
         int L_lo = groups[gi].first, L_hi = groups[gi].second;
         u64 CH = (u64)1 << L_lo, NS = (u64)1 << (L_hi - L_lo + 1);
-        Pass pi = make_pass(CH, NS, choose_c(CH, NS), n);
+        Pass pi = mk(CH, NS, choose(CH, NS));
         for (int L = L_lo; L <= L_hi; L++) pi.ops[pi.nops++] = mkop(BF_I, L - L_lo, L);
         inv_b.push_back(pi);
     }
@@ -476,8 +484,8 @@ void build_passes(PlanImpl &P) {
     for (size_t i = inv.size() - 1; i-- > 0;) inv_all.push_back(inv[i]);
     P.fwd = fwd;
     P.inv = inv_all;
-    for (auto &p : P.fwd) merge_stages(p);
-    for (auto &p : P.inv) merge_stages(p);
+    for (auto &p : P.fwd) merge_stages(p, cfg);
+    for (auto &p : P.inv) merge_stages(p, cfg);
     for (auto &p : P.fwd) P.ntiles_fwd.push_back(pass_tiles(p, n));
     for (auto &p : P.inv) P.ntiles_inv.push_back(pass_tiles(p, n));
 }
@@ -491,8 +499,12 @@ int run_passes(const PlanImpl &P, bool forward, u64 *f, const u32 *src32, u64 nc
         size_t smem = elems * sizeof(u64);
         u64 per = std::max<u64>(1, (u64)gf2e::sm_count() * 8 / (u64)batch);
         dim3 grid((unsigned)std::min<u64>(nt[i], per), (unsigned)batch);
-        k_fft_pass<<<grid, FFT_THREADS, smem, st>>>(f, P.tab, ps[i], nt[i],
-                                                    (i == 0) ? src32 : nullptr, nchunks, bt);
+        const u32 *s32 = (i == 0) ? src32 : nullptr;
+        switch (P.cfg.fft_tile_log) {
+        case 11: k_fft_pass<11><<<grid, FFT_THREADS, smem, st>>>(f, P.tab, ps[i], nt[i], s32, nchunks, bt); break;
+        case 12: k_fft_pass<12><<<grid, FFT_THREADS, smem, st>>>(f, P.tab, ps[i], nt[i], s32, nchunks, bt); break;
+        default: k_fft_pass<13><<<grid, FFT_THREADS, smem, st>>>(f, P.tab, ps[i], nt[i], s32, nchunks, bt); break;
+        }
         GF2E_CHECK_LAUNCH("k_fft_pass");
     }
     return GF2E_OK;
@@ -525,8 +537,14 @@ static int allow_tile_smem() {
     int dev = 0;
     cudaGetDevice(&dev);
     if (dev >= 0 && dev < 64 && !done[dev]) {
-        cudaError_t e = cudaFuncSetAttribute(k_fft_pass, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             TILE * (int)sizeof(u64));
+        cudaError_t e = cudaFuncSetAttribute(k_fft_pass<11>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (1 << 11) * (int)sizeof(u64));
+        if (e == cudaSuccess)
+            e = cudaFuncSetAttribute(k_fft_pass<12>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (1 << 12) * (int)sizeof(u64));
+        if (e == cudaSuccess)
+            e = cudaFuncSetAttribute(k_fft_pass<13>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (1 << 13) * (int)sizeof(u64));
         if (e != cudaSuccess) return cuda_status(e, "k_fft_pass smem attribute");
         done[dev] = true;
     }
@@ -534,7 +552,8 @@ static int allow_tile_smem() {
 }
 
 // plan whose passes read the caller's twiddle tables; no device allocation
-int fft_plan_create_tables(int m, const u64 *tab_dev, gf2e_fft_plan **out) {
+int fft_plan_create_tables_cfg(int m, const u64 *tab_dev, const gf2e_tune &cfg,
+                               gf2e_fft_plan **out) {
     if (m < 1 || m > 30) return invalid("FFT size exponent m=%d outside 1..30", m);
     if (!basis_host()) return invalid("Cantor basis construction failed");
     GF2E_TRY(allow_tile_smem());
@@ -542,12 +561,18 @@ int fft_plan_create_tables(int m, const u64 *tab_dev, gf2e_fft_plan **out) {
     p->impl.m = m;
     p->impl.n = (u64)1 << m;
     p->impl.tab = tab_dev;
+    p->impl.cfg = cfg;
     build_passes(p->impl);
     *out = p;
     return GF2E_OK;
 }
 
-int fft_plan_create(int m, gf2e_fft_plan **out) {
+int fft_plan_create_tables(int m, const u64 *tab_dev, gf2e_fft_plan **out) {
+    return fft_plan_create_tables_cfg(m, tab_dev, tune_current(), out);
+}
+
+// plan with its own twiddle tables and an explicit tuning
+int fft_plan_create_cfg(int m, const gf2e_tune &cfg, gf2e_fft_plan **out) {
     if (m < 1 || m > 30) return invalid("FFT size exponent m=%d outside 1..30", m);
     if (!basis_host()) return invalid("Cantor basis construction failed");
     std::vector<u64> tab(NTWTAB * 256, 0);
@@ -560,10 +585,14 @@ int fft_plan_create(int m, gf2e_fft_plan **out) {
         cudaFree(d_tab);
         return cuda_status(e, "fft plan twiddle tables");
     }
-    int st = fft_plan_create_tables(m, d_tab, out);
+    int st = fft_plan_create_tables_cfg(m, d_tab, cfg, out);
     if (st != GF2E_OK) { cudaFree(d_tab); return st; }
     (*out)->impl.d_tab = d_tab;
     return GF2E_OK;
+}
+
+int fft_plan_create(int m, gf2e_fft_plan **out) {
+    return fft_plan_create_cfg(m, tune_current(), out);
 }
 
 int fft_fwd_packed(const gf2e_fft_plan *plan, u64 *f, const u32 *src32, u64 nchunks,
@@ -647,15 +676,19 @@ int mul(const gf2e_fft_plan *plan, const u64 *a, u64 abits, const u64 *b, u64 bb
 // plan cache shared by the batch API and the trinomial context
 gf2e_fft_plan *cached_plan(int m) {
     static std::mutex mu;
-    static std::map<std::pair<int, int>, gf2e_fft_plan *> cache;
+    static std::map<std::pair<int, u64>, gf2e_fft_plan *> cache;
     int dev = 0;
     cudaGetDevice(&dev);
+    // plans are keyed by device, size and the tuning in force when made
+    const gf2e_tune c = tune_current();
+    const u64 key = (u64)m | ((u64)c.fft_tile_log << 8) | ((u64)c.fft_cmin << 16) |
+                    ((u64)c.fft_taylor_lv << 32) | ((u64)c.fft_bfly_lv << 40);
     std::lock_guard<std::mutex> lk(mu);
-    auto it = cache.find({dev, m});
+    auto it = cache.find({dev, key});
     if (it != cache.end()) return it->second;
     gf2e_fft_plan *p = nullptr;
     if (fft_plan_create(m, &p) != GF2E_OK) return nullptr;
-    cache[{dev, m}] = p;
+    cache[{dev, key}] = p;
     return p;
 }
 

@@ -39,6 +39,9 @@ inline int invalid(const char *fmt, ...) {
 int grid_for(size_t work, int threads, int ctas_per_sm = 8);
 int sm_count();
 
+// process-wide tuning in force (defaults, then environment overrides)
+gf2e_tune tune_current();
+
 }  // namespace gf2e
 
 #define GF2E_CHECK_LAUNCH(what)                                              \

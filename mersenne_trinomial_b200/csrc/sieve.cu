@@ -19,11 +19,11 @@
 //               beta^0..beta^d (O(d^2) word ops instead of O(d^2) field
 //               multiplies; the minimal polynomial is unique so the mask is
 //               identical).  Progressions are routed by length:
-//                 n < STRIP          -> strip list (applied in shared memory)
+//                 n < strip width    -> strip list (applied in shared memory)
 //                 <= INLINE marks    -> marked at once with atomicMin
 //                 otherwise          -> heavy list (grid-stride atomicMin)
 //   k_heavy     all heavy progressions of all degrees, one launch.
-//   k_strip     each CTA owns a STRIP-wide slice of best[], applies every
+//   k_strip     each CTA owns a strip-wide slice of best[], applies every
 //               short-period progression with shared-memory atomics and
 //               writes the slice back once (last writer, so plain min).
 // All degrees are enqueued on one stream with no host round trip; the only
@@ -36,7 +36,8 @@
 namespace {
 
 constexpr int DMAX = 24;
-constexpr u64 STRIP = 4096;               // best[] entries per strip CTA (32 KB smem)
+constexpr int STRIP_LOG_MAX = 14;         // strip CTAs own 2^10..2^14 entries of best[]
+                                          // (8..128 KB of shared memory), tunable
 constexpr u64 INLINE = 32;                // marks done inline by the class thread
 constexpr u64 SCAP = 1ull << 17;          // strip-list capacity
 constexpr u64 HCAP = 1ull << 21;          // heavy-list capacity
@@ -128,6 +129,7 @@ struct DegreeArgs {
     u64 M, rmod, smax;
     int nsub;
     u64 subq[6];
+    u64 strip;                            // strip width (entries of best[] per CTA)
 };
 
 __global__ void __launch_bounds__(256)
@@ -186,7 +188,7 @@ k_classes(const u32 *__restrict__ A, const u32 *__restrict__ L, const DegreeArgs
         }
         const unsigned long long key = ((u64)d << 48) | mask;
         my_marks += count;
-        if (n < STRIP) {
+        if (n < a.strip) {
             unsigned long long slot = atomicAdd(&cnt->nstrip, 1ull);
             if (slot < SCAP) strip[slot] = Prog{first, n, key};
             else atomicAdd(&cnt->overflow, 1ull);
@@ -224,8 +226,8 @@ __global__ void k_heavy(const Prog *__restrict__ heavy, const Counters *__restri
 // short-period progressions, one STRIP-wide slice of best[] per CTA
 __global__ void __launch_bounds__(512)
 k_strip(const Prog *__restrict__ strip, const Counters *__restrict__ cnt, u64 smax,
-        unsigned long long *__restrict__ best) {
-    __shared__ unsigned long long sb[STRIP];
+        unsigned long long *__restrict__ best, const u64 STRIP) {
+    extern __shared__ unsigned long long sb[];
     u64 ns = cnt->nstrip;
     if (ns > SCAP) ns = SCAP;
     const u64 nstrips = (smax + 1 + STRIP - 1) / STRIP;
@@ -347,6 +349,8 @@ int gf2e_sieve_run(uint64_t r, int dmin, int dmax, uint64_t smax, uint64_t *best
     if (ws_bytes < lay.total)
         return gf2e::invalid("sieve workspace %zu < %zu bytes", ws_bytes, lay.total);
     // host-side checks and setup for every degree before any launch
+    const int strip_log = gf2e::tune_current().sieve_strip_log;
+    const u64 strip_w = (u64)1 << strip_log;
     std::vector<DegreeArgs> args;
     for (int d = dmin; d <= dmax; d++) {
         DegreeArgs a;
@@ -356,6 +360,7 @@ int gf2e_sieve_run(uint64_t r, int dmin, int dmax, uint64_t smax, uint64_t *best
         a.q = (u32)cached_primitive(d);
         a.rmod = r % a.M;
         a.smax = smax;
+        a.strip = strip_w;
         if (h_gcd(a.rmod ? a.rmod : a.M, a.M) != 1) {
             gf2e::set_error("d=%d: gcd(r, 2^d-1) != 1; unsupported r", d);
             return GF2E_ERR_UNSUPPORTED_R;
@@ -365,6 +370,17 @@ int gf2e_sieve_run(uint64_t r, int dmin, int dmax, uint64_t smax, uint64_t *best
         a.nsub = np;
         for (int i = 0; i < np; i++) a.subq[i] = a.M / (((u64)1 << (d / ps[i])) - 1);
         args.push_back(a);
+    }
+    {   // k_strip may take up to 2^STRIP_LOG_MAX entries of shared memory
+        static bool attr_done[64] = {false};
+        int dev = 0;
+        cudaGetDevice(&dev);
+        if (dev >= 0 && dev < 64 && !attr_done[dev]) {
+            cudaError_t e = cudaFuncSetAttribute(k_strip, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                 (int)(sizeof(u64) << STRIP_LOG_MAX));
+            if (e != cudaSuccess) return gf2e::cuda_status(e, "k_strip smem attribute");
+            attr_done[dev] = true;
+        }
     }
     cudaStream_t st = (cudaStream_t)stream;
     char *ws = (char *)workspace;
@@ -385,8 +401,9 @@ int gf2e_sieve_run(uint64_t r, int dmin, int dmax, uint64_t smax, uint64_t *best
     }
     k_heavy<<<gf2e::sm_count() * 16, 256, 0, st>>>(heavy, cnt, smax, best);
     GF2E_CHECK_LAUNCH("k_heavy");
-    u64 nstrips = (smax + STRIP) / STRIP;
-    k_strip<<<gf2e::grid_for(nstrips * 512, 512, 2), 512, 0, st>>>(strip, cnt, smax, best);
+    u64 nstrips = (smax + strip_w) / strip_w;
+    k_strip<<<gf2e::grid_for(nstrips * 512, 512, 2), 512, strip_w * sizeof(u64), st>>>(
+        strip, cnt, smax, best, strip_w);
     GF2E_CHECK_LAUNCH("k_strip");
     // status: overflow / internal failures (one small read, synchronizes)
     unsigned long long flags[4];
