@@ -326,6 +326,36 @@ int gf2e_trin_reduce_T0(gf2e_trin *ctx, uint64_t *dst_dev, uint64_t L,
 int gf2e_trin_accumulate(gf2e_trin *ctx, void *stream);
 
 /* ======================================================================
+ * Subquadratic gcd for r-bit operands (half-gcd).  Replaces the interval
+ * gcd the reference delegates to NTL at r = 136279841 (GF2X GCD,
+ * gf2_gcd_ntl.cpp:32-42; hybrid HGCD gf2_gcd_ntl.cpp:360-452) with the same
+ * contract as gf2e_gcd_batch: deg_host[i] = deg gcd (0 means gcd = 1), and
+ * the gcd itself in g_dev when it fits g_cap_words.  Operands are read, not
+ * modified.  Each job runs the half-gcd recursion on its own stream and host
+ * thread, up to max_parallel jobs at once (a single gcd is latency-bound;
+ * independent ones overlap on the GPU).  Device memory comes from a private
+ * stream-ordered pool (about 40 words per operand word per job in flight).
+ * Synchronous: returns when every job is done.  stats (may be NULL) sums the
+ * work counters of all jobs.
+ * ====================================================================== */
+typedef struct gf2e_hgcd_stats {
+    int64_t nodes;            /* half-gcd calls */
+    int64_t base_cases;       /* one-CTA Lehmer base cases */
+    int64_t base_rounds;      /* Lehmer rounds inside them */
+    int64_t fft_products;     /* sum-of-two-products done with the FFT */
+    int64_t school_products;  /* ... done with the schoolbook kernel */
+    int64_t division_steps;
+    int64_t probes;           /* device-to-host degree reads */
+    int64_t us_base;          /* host wall time (us) in base cases */
+    int64_t us_products;      /* ... in matrix products (incl. degree reads) */
+    int64_t us_division;      /* ... in division steps */
+    int64_t us_small_gcd;     /* ... in the final quadratic gcd */
+} gf2e_hgcd_stats;
+
+int gf2e_gcd_large(const gf2e_gcd_job *jobs, int njobs, int64_t *deg_host,
+                   int max_parallel, gf2e_hgcd_stats *stats, void *stream);
+
+/* ======================================================================
  * Tuning and the autotuner.  Replaces the reference's runtime FFT knobs
  * (gf2c_taylor_lv / gf2c_bfly_lv, gf2_cantor_cuda.h:24-60, environment
  * GF2C_TAYLOR_LV / GF2C_BFLY_LV) and tsfactor's "--bench" FFT autotune

@@ -47,6 +47,15 @@ class MulJob(C.Structure):
                 ("bbits", C.c_uint64), ("out_dev", C.c_void_p)]
 
 
+class HgcdStats(C.Structure):
+    _fields_ = [(k, C.c_int64) for k in ("nodes", "base_cases", "base_rounds", "fft_products",
+                                        "school_products", "division_steps", "probes", "us_base",
+                                        "us_products", "us_division", "us_small_gcd")]
+
+    def as_dict(self) -> dict:
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
 class Tune(C.Structure):
     _fields_ = [("fft_tile_log", C.c_int), ("fft_cmin", C.c_int), ("fft_taylor_lv", C.c_int),
                 ("fft_bfly_lv", C.c_int), ("sieve_strip_log", C.c_int)]
@@ -125,6 +134,7 @@ SIGNATURES = {
     "gf2e_trin_mul_dev": (_i32, [_vp, _vp, _vp, _vp]),
     "gf2e_trin_reduce_T0": (_i32, [_vp, _vp, _u64, _vp]),
     "gf2e_trin_accumulate": (_i32, [_vp, _vp]),
+    "gf2e_gcd_large": (_i32, [_vp, _i32, _vp, _i32, _P(HgcdStats), _vp]),
     "gf2e_tune_default": (_i32, [_P(Tune)]),
     "gf2e_tune_get": (_i32, [_P(Tune)]),
     "gf2e_tune_set": (_i32, [_P(Tune)]),

@@ -1,0 +1,1053 @@
+// hgcd.cu -- subquadratic GF(2)[x] gcd (half-gcd) for r-bit operands.
+//
+// The reference computes the interval gcd gcd(ACC, T) at r = 136279841 with
+// NTL's GF2X GCD (gf2_gcd_ntl.cpp:32-42; a half-gcd over gf2x products,
+// ~62 s per gcd on 6 CPU cores) or its hybrid HGCD with GPU multiplies
+// (gf2_gcd_ntl.cpp:360-452, GpuMulHook gf2_gcd.h:155-190).  The quadratic
+// GPU gcd (gcd.cu) is fine to ~10^6 bits; this file is the r-bit path.
+//
+// Algorithm (the classical polynomial half-gcd; every matrix is unimodular
+// over GF(2), so the gcd is preserved whatever the degrees do, and the
+// degree bookkeeping only decides the amount of work):
+//
+//   hgcd(a, b), deg a = n > deg b, m = ceil(n/2)
+//     returns M with (a', b') = M (a, b), deg a' >= m > deg b'
+//     if deg b < m: I
+//     if n <= H0:   one-CTA Lehmer kernel (64-bit windows, stop at deg b < m)
+//     M1 = hgcd(a quo x^m, b quo x^m);  (c, d) = M1 (a, b)
+//     if deg d < m: M1
+//     one division step c = q d + e; M1 <- [[0,1],[1,q]] M1; (c, d) <- (d, e)
+//     if deg d < m: M1
+//     k = 2m - deg c;  M2 = hgcd(c quo x^k, d quo x^k);  M2 M1
+//
+//   gcd(a, b): while deg b >= G0: M = hgcd(a, b); (a, b) = M (a, b); one
+//   division step.  Then the quadratic Lehmer gcd (gcd.cu) finishes.
+//
+// B200 mapping.  The recursion is host-driven on one stream per gcd; degrees
+// are read back with one small probe per node.  Products are sums of two
+// products (matrix x vector and matrix x matrix): a schoolbook carry-less
+// kernel split over output words and input chunks (atomicXor partials) below
+// a size threshold, the Cantor FFT above it (transforms of a and b shared by
+// both rows).  Temporaries come from a private stream-ordered memory pool.
+// A single gcd is latency-bound (the quotient sequence is sequential), so
+// independent gcds run concurrently, one host thread and stream each.
+#include "gf2e_internal.cuh"
+
+#include <algorithm>
+#include <atomic>
+#include <chrono>
+#include <cstring>
+#include <memory>
+#include <mutex>
+#include <thread>
+#include <vector>
+
+namespace gf2e {
+int mul_fft_m(u64 abits, u64 bbits);
+gf2e_fft_plan *cached_plan(int m);
+int fft_fwd_packed(const gf2e_fft_plan *plan, u64 *f, const u32 *src32, u64 nchunks,
+                   cudaStream_t st);
+int fft_run(const gf2e_fft_plan *plan, bool forward, u64 *f, cudaStream_t st);
+int overlap_add(const u64 *F, u64 nchunks, u64 *out, u64 ow, cudaStream_t st);
+u64 fft_plan_n(const gf2e_fft_plan *plan);
+}  // namespace gf2e
+
+namespace {
+
+constexpr int BASE_THREADS = 256;
+
+// ------------------------------------------------------------------ device
+GF2E_DEV void clmul64(u64 a, u64 b, u64 &lo, u64 &hi) {
+    const u32 a0 = (u32)a, a1 = (u32)(a >> 32), b0 = (u32)b, b1 = (u32)(b >> 32);
+    const u64 L = clmul32(a0, b0), H = clmul32(a1, b1);
+    const u64 Mid = clmul32(a0 ^ a1, b0 ^ b1) ^ L ^ H;
+    lo = L ^ (Mid << 32);
+    hi = H ^ (Mid >> 32);
+}
+
+GF2E_DEV int deg64(u64 v) { return v ? 63 - __clzll(v) : -1; }
+
+// degree and the 64-bit top window (bit 63 = leading coefficient) of up to
+// four polynomials; warp w scans polynomial w downwards from word nw-1
+struct ProbeArgs {
+    const u64 *p[4];
+    u64 nw[4];
+};
+__global__ void k_probe(ProbeArgs a, int np, long long *out) {
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (w >= np) return;
+    const u64 *X = a.p[w];
+    long long top = -1;
+    for (long long base = (long long)a.nw[w] - 1; base >= 0 && top < 0; base -= 32) {
+        long long i = base - lane;
+        u64 v = (i >= 0) ? X[i] : 0;
+        unsigned ball = __ballot_sync(0xffffffffu, v != 0);
+        if (ball) top = base - (__ffs(ball) - 1);
+    }
+    if (lane == 0) {
+        long long deg = -1;
+        u64 win = 0;
+        if (top >= 0) {
+            const u64 hiw = X[top];
+            const int t = 63 - __clzll(hiw);
+            deg = top * 64 + t;
+            win = hiw << (63 - t);
+            if (t < 63 && top > 0) win |= X[top - 1] >> (t + 1);
+        }
+        out[2 * w] = deg;
+        out[2 * w + 1] = (long long)win;
+    }
+}
+
+// dst = src quo x^k (dst has nd words)
+__global__ void k_shr(const u64 *__restrict__ src, u64 ns, u64 k, u64 *__restrict__ dst, u64 nd) {
+    const u64 ks = k >> 6;
+    const unsigned kb = (unsigned)(k & 63);
+    for (u64 w = (u64)blockIdx.x * blockDim.x + threadIdx.x; w < nd;
+         w += (u64)gridDim.x * blockDim.x) {
+        u64 lo = (w + ks < ns) ? src[w + ks] : 0, hi = (w + ks + 1 < ns) ? src[w + ks + 1] : 0;
+        dst[w] = funnel64(lo, hi, kb);
+    }
+}
+
+// out = x1*y1 + x2*y2 (schoolbook).  Thread = two adjacent output words,
+// blockIdx.y = a chunk of the x index; partial sums are XORed into out,
+// which must be zero on entry.
+__global__ void k_mul2(const u64 *__restrict__ x1, u64 nx1, const u64 *__restrict__ y1, u64 ny1,
+                       const u64 *__restrict__ x2, u64 nx2, const u64 *__restrict__ y2, u64 ny2,
+                       unsigned long long *__restrict__ out, u64 nout, u64 chunk) {
+    const u64 w = 2 * ((u64)blockIdx.x * blockDim.x + threadIdx.x);
+    if (w >= nout) return;
+    const u64 i0 = (u64)blockIdx.y * chunk;
+    u64 r0 = 0, r1 = 0;
+    for (int pr = 0; pr < 2; pr++) {
+        const u64 *x = pr ? x2 : x1, *y = pr ? y2 : y1;
+        const u64 nx = pr ? nx2 : nx1, ny = pr ? ny2 : ny1;
+        if (!x || !nx || !ny) continue;
+        const u64 i1 = min(nx, i0 + chunk);
+        for (u64 i = i0; i < i1; i++) {
+            const u64 xi = x[i];
+            if (!xi) continue;
+            u64 lo, hi;
+            // j = w-1-i: hi -> word w
+            if (w >= i + 1 && w - 1 - i < ny) { clmul64(xi, y[w - 1 - i], lo, hi); r0 ^= hi; }
+            // j = w-i: lo -> w, hi -> w+1
+            if (w >= i && w - i < ny) { clmul64(xi, y[w - i], lo, hi); r0 ^= lo; r1 ^= hi; }
+            // j = w+1-i: lo -> w+1
+            if (w + 1 >= i && w + 1 - i < ny) { clmul64(xi, y[w + 1 - i], lo, hi); r1 ^= lo; }
+        }
+    }
+    if (r0) atomicXor(out + w, (unsigned long long)r0);
+    if (r1 && w + 1 < nout) atomicXor(out + w + 1, (unsigned long long)r1);
+}
+
+// out = x ^ ((q * y) << s) for out words [0, nout); x read below nx (x may be out)
+__global__ void k_axpy_q(u64 *out, u64 nout, const u64 *x, u64 nx, const u64 *__restrict__ y,
+                         u64 ny, u64 q, u64 s) {
+    const u64 sw = s >> 6;
+    const unsigned sb = (unsigned)(s & 63);
+    for (u64 w = (u64)blockIdx.x * blockDim.x + threadIdx.x; w < nout;
+         w += (u64)gridDim.x * blockDim.x) {
+        // word j of P = q*y: lo(q*y[j]) ^ hi(q*y[j-1])
+        auto Pw = [&](long long j) -> u64 {
+            if (j < 0 || j > (long long)ny) return 0;
+            u64 v = 0, lo, hi;
+            if (j < (long long)ny) { clmul64(q, y[j], lo, hi); v ^= lo; }
+            if (j >= 1) { clmul64(q, y[j - 1], lo, hi); v ^= hi; }
+            return v;
+        };
+        const long long j = (long long)w - (long long)sw;
+        u64 sh = sb ? ((Pw(j) << sb) | (Pw(j - 1) >> (64 - sb))) : Pw(j);
+        out[w] = (w < nx ? x[w] : 0) ^ sh;
+    }
+}
+
+// out = X1*Y1 ^ X2*Y2 pointwise in GF(2^64)
+__global__ void k_pw_muladd(u64 *out, const u64 *x1,
+                            const u64 *__restrict__ y1, const u64 *__restrict__ x2,
+                            const u64 *__restrict__ y2, u64 n) {
+    for (u64 k = (u64)blockIdx.x * blockDim.x + threadIdx.x; k < n;
+         k += (u64)gridDim.x * blockDim.x) {
+        u64 v = gf64_mul(x1[k], y1[k]);
+        if (x2) v ^= gf64_mul(x2[k], y2[k]);
+        out[k] = v;
+    }
+}
+
+// ---- base case: Lehmer half-gcd in one CTA, operands in shared memory ----
+struct Masked { u64 p[4]; };
+GF2E_DEV Masked mask32(u32 a) {
+    Masked m;
+    m.p[0] = a & 0x11111111u; m.p[1] = a & 0x22222222u;
+    m.p[2] = a & 0x44444444u; m.p[3] = a & 0x88888888u;
+    return m;
+}
+GF2E_DEV u64 clmul_masked(const Masked &a, const Masked &b) {
+    const u64 M0 = 0x1111111111111111ull;
+    u64 c0 = (a.p[0] * b.p[0]) ^ (a.p[1] * b.p[3]) ^ (a.p[2] * b.p[2]) ^ (a.p[3] * b.p[1]);
+    u64 c1 = (a.p[0] * b.p[1]) ^ (a.p[1] * b.p[0]) ^ (a.p[2] * b.p[3]) ^ (a.p[3] * b.p[2]);
+    u64 c2 = (a.p[0] * b.p[2]) ^ (a.p[1] * b.p[1]) ^ (a.p[2] * b.p[0]) ^ (a.p[3] * b.p[3]);
+    u64 c3 = (a.p[0] * b.p[3]) ^ (a.p[1] * b.p[2]) ^ (a.p[2] * b.p[1]) ^ (a.p[3] * b.p[0]);
+    return (c0 & M0) ^ (c1 & (M0 << 1)) ^ (c2 & (M0 << 2)) ^ (c3 & (M0 << 3));
+}
+// x (64 bits) times m (<= 32 bits): (lo 64, hi 32)
+GF2E_DEV void mul64x32(u64 x, const Masked &m, u64 &lo, u64 &hi) {
+    u64 p0 = clmul_masked(mask32((u32)x), m), p1 = clmul_masked(mask32((u32)(x >> 32)), m);
+    lo = p0 ^ (p1 << 32);
+    hi = p1 >> 32;
+}
+
+GF2E_DEV u64 win_at(const u64 *X, long long nw, long long pos) {   // bits pos..pos+63
+    long long i = pos >> 6;
+    unsigned sh = (unsigned)(pos & 63);
+    u64 a = (i >= 0 && i < nw) ? X[i] : 0, b = (i + 1 < nw) ? X[i + 1] : 0;
+    return funnel64(a, b, sh);
+}
+
+struct BaseOut {
+    long long deg_a, deg_b;     // degrees of the reduced pair
+    long long rounds;
+    int status;
+};
+
+// warp-wide degree of X below word `top` (inclusive); all 32 lanes return it
+GF2E_DEV long long warp_degree(const u64 *X, long long top) {
+    const int lane = threadIdx.x & 31;
+    for (long long base = top; base >= 0; base -= 32) {
+        long long i = base - lane;
+        u64 v = (i >= 0) ? X[i] : 0;
+        unsigned ball = __ballot_sync(0xffffffffu, v != 0);
+        if (ball) {
+            int l = __ffs(ball) - 1;
+            u64 vv = __shfl_sync(0xffffffffu, v, l);
+            return (base - l) * 64 + 63 - __clzll(vv);
+        }
+    }
+    return -1;
+}
+
+// (a', b') = M (a, b) with deg a' >= m > deg b'; M written to four arrays of
+// mw words (row-major M00 M01 M10 M11).
+//
+// Each round, thread 0 runs Euclid steps on the 64-bit top windows of A and
+// B (Lehmer), accumulating a 2x2 matrix of degree <= 31 while the bits it
+// decides on are exact and the half-gcd stop (deg B < m) is not reached; the
+// CTA then applies the matrix to A, B and to the accumulated rows.  When the
+// final windows are exact at their leading bits the new degrees are known
+// without a scan; otherwise warp 0 scans down from the old top word.
+// Shared memory: V[4][W] (two buffers of A, B), R[2][4][mw] (two buffers of
+// the rows), carries C[2W + 4mw].
+__global__ void __launch_bounds__(BASE_THREADS)
+k_hgcd_base(const u64 *__restrict__ a, long long da0, const u64 *__restrict__ b, long long db0,
+            long long m, u64 W, u64 mw, u64 *__restrict__ Mout, BaseOut *res) {
+    extern __shared__ u64 sh[];
+    u64 *V = sh;
+    u64 *R = sh + 4 * W;
+    u64 *hiv = R + 8 * mw;
+    u64 *hir = hiv + 2 * W;
+    __shared__ int s_va, s_vb, s_ra, s_buf, s_mode, s_done, s_status;
+    __shared__ long long s_da, s_db, s_md, s_k, s_rounds, s_top;
+    __shared__ u32 s_m[4];
+    const int tid = threadIdx.x;
+    for (u64 i = tid; i < 2 * W; i += BASE_THREADS) {
+        u64 v;
+        if (i < W) v = (i <= (u64)(da0 >> 6)) ? a[i] : 0;
+        else { u64 j = i - W; v = (db0 >= 0 && j <= (u64)(db0 >> 6)) ? b[j] : 0; }
+        V[i] = v;
+    }
+    for (u64 i = tid; i < 8 * mw; i += BASE_THREADS) R[i] = (i == 0 || i == 3 * mw) ? 1 : 0;
+    if (tid == 0) {
+        s_va = 0; s_vb = 1; s_buf = 0;     // A = V[s_va], B = V[s_vb]; rows in R[s_buf]
+        s_ra = 0;                          // row block of A (B's is s_ra ^ 1)
+        s_top = 0;
+        s_da = da0; s_db = db0; s_md = 0; s_done = 0;
+        s_status = GF2E_ERR_INTERNAL;
+    }
+    __syncthreads();
+    const long long max_rounds = 2 * (da0 + 2) + 16;
+    long long known_a = 1, known_b = 1;          // warp 0 only: degrees known exactly
+    for (long long round = 0;; round++) {
+        if (tid < 32) {
+            // finish the previous round: degrees the windows did not settle
+            if (round > 0) {
+                if (!known_a) { long long d = warp_degree(V + (u64)s_va * W, s_top); if (tid == 0) s_da = d; }
+                if (!known_b) { long long d = warp_degree(V + (u64)s_vb * W, s_top); if (tid == 0) s_db = d; }
+            }
+            if (tid == 0) {
+                long long da = s_da, db = s_db;
+                if (da < db) {                           // keep deg A >= deg B (rows too)
+                    int t = s_va; s_va = s_vb; s_vb = t;
+                    s_ra ^= 1;
+                    s_da = db; s_db = da;
+                    da = s_da; db = s_db;
+                }
+                s_mode = 0;
+                if (db < m || round > max_rounds) {
+                    s_done = 1;
+                    s_status = (round > max_rounds) ? GF2E_ERR_TIMEOUT : GF2E_OK;
+                    s_rounds = round;
+                } else {
+                    const u64 *A = V + (u64)s_va * W, *B = V + (u64)s_vb * W;
+                    const long long lo = da >= 63 ? da - 63 : 0;
+                    u64 wa = win_at(A, (long long)W, lo), wb = win_at(B, (long long)W, lo);
+                    u32 ma0 = 1, ma1 = 0, mb0 = 0, mb1 = 1;
+                    int dga = (int)(da - lo), dgb = deg64(wb), dma = 0, dmb = 0, steps = 0;
+                    const bool exact = (lo == 0);
+                    const int dstop = (int)max(-1LL, m - lo);      // window degree of deg m
+                    for (int it = 0; it < 256; it++) {
+                        if (dgb < 0) break;
+                        if (dga < dgb) {
+                            u64 t = wa; wa = wb; wb = t;
+                            u32 x = ma0; ma0 = mb0; mb0 = x;
+                            x = ma1; ma1 = mb1; mb1 = x;
+                            int y = dga; dga = dgb; dgb = y;
+                            y = dma; dma = dmb; dmb = y;
+                        }
+                        if (!exact && (dgb < dmb || dga < dma)) break;   // undecided bits
+                        if (dgb < dstop) break;                          // half-gcd stop
+                        const int k = dga - dgb;
+                        const int ndm = max(dma, dmb + k);
+                        if (ndm > 31) break;
+                        wa ^= wb << k;
+                        ma0 ^= mb0 << k;
+                        ma1 ^= mb1 << k;
+                        dma = ndm;
+                        dga = deg64(wa);
+                        steps++;
+                    }
+                    if (steps == 0) {
+                        s_mode = 1;                                // A ^= B << (da - db)
+                        s_k = da - db;
+                        known_a = 0;
+                        known_b = 1;
+                    } else {
+                        s_m[0] = ma0; s_m[1] = ma1; s_m[2] = mb0; s_m[3] = mb1;
+                        // exact leading bits give the new degrees directly
+                        known_a = (exact || dga >= dma) ? 1 : 0;
+                        known_b = (exact || (dgb >= 0 && dgb >= dmb)) ? 1 : 0;
+                        if (known_a) s_da = dga < 0 ? -1 : dga + lo;
+                        if (known_b) s_db = dgb < 0 ? -1 : dgb + lo;
+                    }
+                    s_top = da >> 6;
+                }
+            }
+            known_a = __shfl_sync(0xffffffffu, known_a, 0);
+            known_b = __shfl_sync(0xffffffffu, known_b, 0);
+        }
+        __syncthreads();
+        if (s_done) break;
+        const int va = s_va, vb = s_vb, buf = s_buf, nb = buf ^ 1, ra = s_ra, rb = s_ra ^ 1;
+        const long long nwv = s_top + 1;                        // live vector words
+        const long long nwm = min((long long)mw, s_md + 2);     // live matrix words
+        int spare[2], ns = 0;
+        for (int i = 0; i < 4 && ns < 2; i++)
+            if (i != va && i != vb) spare[ns++] = i;
+        const u64 *A = V + (u64)va * W, *B = V + (u64)vb * W;
+        u64 *A2 = V + (u64)spare[0] * W, *B2 = V + (u64)spare[1] * W;
+        const u64 *Ra0 = R + (u64)(buf * 4 + 2 * ra) * mw, *Ra1 = R + (u64)(buf * 4 + 2 * ra + 1) * mw;
+        const u64 *Rb0 = R + (u64)(buf * 4 + 2 * rb) * mw, *Rb1 = R + (u64)(buf * 4 + 2 * rb + 1) * mw;
+        u64 *Na0 = R + (u64)(nb * 4 + 0) * mw, *Na1 = R + (u64)(nb * 4 + 1) * mw;
+        u64 *Nb0 = R + (u64)(nb * 4 + 2) * mw, *Nb1 = R + (u64)(nb * 4 + 3) * mw;
+        if (s_mode == 1) {
+            const long long k = s_k, ks = k >> 6;
+            const unsigned kb = (unsigned)(k & 63);
+            for (long long w = tid; w < nwv; w += BASE_THREADS) {
+                u64 hi = (w >= ks) ? B[w - ks] : 0, lo2 = (w >= ks + 1) ? B[w - ks - 1] : 0;
+                A2[w] = A[w] ^ (kb ? ((hi << kb) | (lo2 >> (64 - kb))) : hi);
+                B2[w] = B[w];
+            }
+            for (long long w = tid; w < (long long)mw; w += BASE_THREADS) {
+                u64 h0 = (w >= ks) ? Rb0[w - ks] : 0, l0 = (w >= ks + 1) ? Rb0[w - ks - 1] : 0;
+                u64 h1 = (w >= ks) ? Rb1[w - ks] : 0, l1 = (w >= ks + 1) ? Rb1[w - ks - 1] : 0;
+                Na0[w] = Ra0[w] ^ (kb ? ((h0 << kb) | (l0 >> (64 - kb))) : h0);
+                Na1[w] = Ra1[w] ^ (kb ? ((h1 << kb) | (l1 >> (64 - kb))) : h1);
+                Nb0[w] = Rb0[w];
+                Nb1[w] = Rb1[w];
+            }
+            __syncthreads();
+            if (tid == 0) s_md = min((long long)mw - 2, s_md + ks + 1);
+        } else {
+            const Masked m0 = mask32(s_m[0]), m1 = mask32(s_m[1]), m2 = mask32(s_m[2]),
+                         m3 = mask32(s_m[3]);
+            for (long long w = tid; w < nwv; w += BASE_THREADS) {
+                u64 x = A[w], y = B[w];
+                u64 l0, h0, l1, h1, l2, h2, l3, h3;
+                mul64x32(x, m0, l0, h0); mul64x32(y, m1, l1, h1);
+                mul64x32(x, m2, l2, h2); mul64x32(y, m3, l3, h3);
+                A2[w] = l0 ^ l1;
+                B2[w] = l2 ^ l3;
+                hiv[2 * w] = h0 ^ h1;
+                hiv[2 * w + 1] = h2 ^ h3;
+            }
+            for (long long w = tid; w < nwm; w += BASE_THREADS) {
+                u64 x0 = Ra0[w], y0 = Rb0[w], x1 = Ra1[w], y1 = Rb1[w];
+                u64 l0, h0, l1, h1;
+                mul64x32(x0, m0, l0, h0); mul64x32(y0, m1, l1, h1);
+                Na0[w] = l0 ^ l1; hir[4 * w + 0] = h0 ^ h1;
+                mul64x32(x1, m0, l0, h0); mul64x32(y1, m1, l1, h1);
+                Na1[w] = l0 ^ l1; hir[4 * w + 1] = h0 ^ h1;
+                mul64x32(x0, m2, l0, h0); mul64x32(y0, m3, l1, h1);
+                Nb0[w] = l0 ^ l1; hir[4 * w + 2] = h0 ^ h1;
+                mul64x32(x1, m2, l0, h0); mul64x32(y1, m3, l1, h1);
+                Nb1[w] = l0 ^ l1; hir[4 * w + 3] = h0 ^ h1;
+            }
+            for (long long w = nwm + tid; w < (long long)mw; w += BASE_THREADS) {
+                Na0[w] = 0; Na1[w] = 0; Nb0[w] = 0; Nb1[w] = 0;
+            }
+            __syncthreads();
+            // carries of word w-1 (the new vectors have degree < the old top)
+            for (long long w = 1 + tid; w < nwv; w += BASE_THREADS) {
+                A2[w] ^= hiv[2 * (w - 1)];
+                B2[w] ^= hiv[2 * (w - 1) + 1];
+            }
+            for (long long w = 1 + tid; w <= nwm && w < (long long)mw; w += BASE_THREADS) {
+                Na0[w] ^= hir[4 * (w - 1) + 0];
+                Na1[w] ^= hir[4 * (w - 1) + 1];
+                Nb0[w] ^= hir[4 * (w - 1) + 2];
+                Nb1[w] ^= hir[4 * (w - 1) + 3];
+            }
+            if (tid == 0) s_md = min((long long)mw - 2, s_md + 1);
+        }
+        // words of the new vectors above the live range stay as they were
+        // (zero) only if both old buffers were zero there: clear them
+        for (long long w = nwv + tid; w < (long long)W; w += BASE_THREADS) { A2[w] = 0; B2[w] = 0; }
+        __syncthreads();
+        if (tid == 0) {
+            s_va = spare[0]; s_vb = spare[1];
+            s_buf = nb;
+            s_ra = 0;                        // new rows are written in (A, B) order
+        }
+        __syncthreads();
+    }
+    // matrix out, rows in (A, B) order
+    const int buf = s_buf, ra = s_ra;
+    for (u64 w = tid; w < 2 * mw; w += BASE_THREADS) {
+        Mout[w] = R[(u64)(buf * 4 + 2 * ra) * mw + w];
+        Mout[2 * mw + w] = R[(u64)(buf * 4 + 2 * (ra ^ 1)) * mw + w];
+    }
+    if (tid == 0) {
+        res->deg_a = s_da;
+        res->deg_b = s_db;
+        res->rounds = s_rounds;
+        res->status = s_status;
+    }
+}
+
+// ------------------------------------------------------------------ host
+struct Fail {
+    int st;
+};
+inline void ck(int st) {
+    if (st != GF2E_OK) throw Fail{st};
+}
+inline void ckc(cudaError_t e, const char *what) {
+    if (e != cudaSuccess) throw Fail{gf2e::cuda_status(e, what)};
+}
+
+struct Pool {
+    cudaMemPool_t pool = nullptr;
+};
+
+// device buffer from the stream-ordered pool, freed on the same stream
+struct DBuf {
+    u64 *p = nullptr;
+    size_t words = 0;
+    cudaStream_t st = nullptr;
+    ~DBuf() {
+        if (p) cudaFreeAsync(p, st);
+    }
+};
+typedef std::shared_ptr<DBuf> Buf;
+
+// polynomial on the device: deg exact for remainders, an upper bound for
+// matrix entries (words() covers every nonzero word either way)
+struct Poly {
+    Buf b;
+    long long deg = -1;
+    u64 *p() const { return b ? b->p : nullptr; }
+    u64 words() const { return deg < 0 ? 0 : (u64)(deg >> 6) + 1; }
+};
+
+struct Mat {
+    Poly e[4];          // M00 M01 M10 M11
+    bool ident = false;
+};
+
+struct Tunables {
+    long long base_bits = 1 << 14;       // n <= base_bits: one-CTA base kernel
+    long long fft_bits = 1 << 21;        // products above this many bits use the FFT
+    long long small_gcd_bits = 1 << 15;  // finish with the quadratic gcd below this
+};
+
+Tunables tunables() {
+    Tunables t;
+    if (const char *e = getenv("GF2E_HGCD_BASE_BITS")) t.base_bits = atoll(e);
+    if (const char *e = getenv("GF2E_HGCD_FFT_BITS")) t.fft_bits = atoll(e);
+    if (const char *e = getenv("GF2E_HGCD_SMALL_BITS")) t.small_gcd_bits = atoll(e);
+    t.base_bits = std::max(256LL, std::min(t.base_bits, 1LL << 16));
+    t.small_gcd_bits = std::max(t.small_gcd_bits, 2 * t.base_bits);
+    return t;
+}
+
+struct Stats {
+    long long nodes = 0, bases = 0, base_rounds = 0, fft_mul2 = 0, school_mul2 = 0, divsteps = 0,
+              probes = 0;
+    double us_base = 0, us_products = 0, us_division = 0, us_small = 0;
+};
+
+// adds the wall time of a scope to a counter
+struct Timer {
+    double &acc;
+    std::chrono::steady_clock::time_point t0;
+    explicit Timer(double &a) : acc(a), t0(std::chrono::steady_clock::now()) {}
+    ~Timer() {
+        acc += std::chrono::duration<double, std::micro>(std::chrono::steady_clock::now() - t0).count();
+    }
+};
+
+class Hgcd {
+public:
+    Hgcd(cudaStream_t st, cudaMemPool_t pool) : st_(st), pool_(pool), tn_(tunables()) {
+        ckc(cudaMallocHost(&h_probe_, 16 * sizeof(long long)), "hgcd probe host buffer");
+        d_probe_ = alloc(16);
+        d_res_ = alloc(8);
+    }
+    ~Hgcd() {
+        if (h_probe_) cudaFreeHost(h_probe_);
+    }
+    Stats stats;
+
+    Buf alloc(size_t words) {
+        auto b = std::make_shared<DBuf>();
+        b->st = st_;
+        b->words = std::max<size_t>(words, 1);
+        void *p = nullptr;
+        ckc(cudaMallocFromPoolAsync(&p, b->words * 8, pool_, st_), "hgcd pool allocation");
+        b->p = (u64 *)p;
+        return b;
+    }
+    Poly zeros(size_t words) {
+        Poly r;
+        r.b = alloc(words);
+        ckc(cudaMemsetAsync(r.b->p, 0, r.b->words * 8, st_), "hgcd memset");
+        return r;
+    }
+    Poly from_device(const u64 *src, u64 bits) {
+        const size_t nw = (size_t)((bits + 63) >> 6);
+        Poly r = zeros(nw + 1);
+        if (nw) ckc(cudaMemcpyAsync(r.p(), src, nw * 8, cudaMemcpyDeviceToDevice, st_), "hgcd copy");
+        r.deg = (long long)nw * 64 - 1;    // bound until probed
+        probe({&r});
+        return r;
+    }
+    Poly constant1() {
+        Poly r = zeros(1);
+        u64 one = 1;
+        ckc(cudaMemcpyAsync(r.p(), &one, 8, cudaMemcpyHostToDevice, st_), "hgcd const");
+        ckc(cudaStreamSynchronize(st_), "hgcd const sync");
+        r.deg = 0;
+        return r;
+    }
+
+    // exact degrees (and top windows) of up to four polynomials whose
+    // current deg is an upper bound
+    void probe(std::initializer_list<Poly *> ps, u64 *wins = nullptr) {
+        ProbeArgs a;
+        memset(&a, 0, sizeof a);
+        int n = 0;
+        for (Poly *p : ps) {
+            a.p[n] = p->p();
+            a.nw[n] = p->p() ? p->words() : 0;
+            n++;
+        }
+        k_probe<<<1, 32 * n, 0, st_>>>(a, n, (long long *)d_probe_->p);
+        ckc(cudaGetLastError(), "k_probe");
+        ckc(cudaMemcpyAsync(h_probe_, d_probe_->p, 2 * n * sizeof(long long),
+                            cudaMemcpyDeviceToHost, st_), "probe read");
+        ckc(cudaStreamSynchronize(st_), "probe sync");
+        stats.probes++;
+        int i = 0;
+        for (Poly *p : ps) {
+            p->deg = h_probe_[2 * i];
+            if (wins) wins[i] = (u64)h_probe_[2 * i + 1];
+            i++;
+        }
+    }
+
+    Poly shr(const Poly &x, long long k) {
+        Poly r;
+        if (x.deg < k) { r.deg = -1; r.b = alloc(1); return r; }
+        r.deg = x.deg - k;
+        const u64 nd = r.words();
+        r.b = alloc(nd);
+        k_shr<<<gf2e::grid_for(nd, 256), 256, 0, st_>>>(x.p(), x.words(), (u64)k, r.p(), nd);
+        ckc(cudaGetLastError(), "k_shr");
+        return r;
+    }
+
+    // x1*y1 + x2*y2 (x2/y2 may be empty); deg of the result is a bound
+    Poly mul2(const Poly &x1, const Poly &y1, const Poly &x2, const Poly &y2) {
+        const bool t1 = x1.deg >= 0 && y1.deg >= 0, t2 = x2.deg >= 0 && y2.deg >= 0;
+        long long dmax = -1;
+        if (t1) dmax = std::max(dmax, x1.deg + y1.deg);
+        if (t2) dmax = std::max(dmax, x2.deg + y2.deg);
+        Poly r;
+        if (dmax < 0) { r.b = alloc(1); r.deg = -1; return r; }
+        const u64 nout = (u64)(dmax >> 6) + 2;
+        if (dmax + 1 > tn_.fft_bits) {
+            r = fft_mul2(t1 ? &x1 : nullptr, t1 ? &y1 : nullptr, t2 ? &x2 : nullptr,
+                         t2 ? &y2 : nullptr, nout);
+        } else {
+            r = zeros(nout);
+            const u64 nxm = std::max(t1 ? x1.words() : 0, t2 ? x2.words() : 0);
+            const u64 chunk = 32;
+            dim3 grid((unsigned)((nout / 2 + 1 + 127) / 128), (unsigned)((nxm + chunk - 1) / chunk));
+            k_mul2<<<grid, 128, 0, st_>>>(t1 ? x1.p() : nullptr, t1 ? x1.words() : 0,
+                                          t1 ? y1.p() : nullptr, t1 ? y1.words() : 0,
+                                          t2 ? x2.p() : nullptr, t2 ? x2.words() : 0,
+                                          t2 ? y2.p() : nullptr, t2 ? y2.words() : 0,
+                                          (unsigned long long *)r.p(), nout, chunk);
+            ckc(cudaGetLastError(), "k_mul2");
+            stats.school_mul2++;
+        }
+        r.deg = dmax;
+        return r;
+    }
+
+    // FFT form of mul2: transforms of the four operands, one pointwise
+    // multiply-add, one inverse transform, overlap-add
+    Poly fft_mul2(const Poly *x1, const Poly *y1, const Poly *x2, const Poly *y2, u64 nout) {
+        u64 need = 0;
+        auto chunks = [](const Poly *p) { return p ? ((u64)p->deg + 1 + 31) / 32 : 0; };
+        if (x1) need = std::max(need, chunks(x1) + chunks(y1) - 1);
+        if (x2) need = std::max(need, chunks(x2) + chunks(y2) - 1);
+        int m = 1;
+        while (((u64)1 << m) < need) m++;
+        gf2e_fft_plan *plan = gf2e::cached_plan(m);
+        if (!plan) throw Fail{GF2E_ERR_CUDA};
+        const u64 n = (u64)1 << m;
+        Buf F[4];
+        const Poly *ops[4] = {x1, y1, x2, y2};
+        for (int i = 0; i < 4; i++) {
+            if (!ops[i]) continue;
+            F[i] = alloc(n);
+            ck(gf2e::fft_fwd_packed(plan, F[i]->p, reinterpret_cast<const u32 *>(ops[i]->p()),
+                                    chunks(ops[i]), st_));
+        }
+        u64 *f0 = F[0] ? F[0]->p : F[2]->p;
+        u64 *g0 = F[0] ? F[1]->p : F[3]->p;
+        k_pw_muladd<<<gf2e::grid_for(n, 256), 256, 0, st_>>>(
+            f0, f0, g0, (F[0] && F[2]) ? F[2]->p : nullptr, (F[0] && F[2]) ? F[3]->p : nullptr, n);
+        ckc(cudaGetLastError(), "k_pw_muladd");
+        ck(gf2e::fft_run(plan, false, f0, st_));
+        Poly r;
+        r.b = alloc(nout);
+        ck(gf2e::overlap_add(f0, need, r.p(), nout, st_));
+        stats.fft_mul2++;
+        return r;
+    }
+
+    // (c, d) = M (a, b); exact degrees
+    void mat_vec(const Mat &M, const Poly &a, const Poly &b, Poly &c, Poly &d) {
+        Timer tm(stats.us_products);
+        if (M.ident) {
+            c = a;
+            d = b;
+            return;
+        }
+        if (std::max(M.e[0].deg + a.deg, M.e[1].deg + b.deg) + 1 > tn_.fft_bits) {
+            fft_mat_vec(M, a, b, c, d);
+        } else {
+            c = mul2(M.e[0], a, M.e[1], b);
+            d = mul2(M.e[2], a, M.e[3], b);
+        }
+        probe({&c, &d});
+    }
+
+    // FFT matrix x vector: the transforms of a and b serve both rows
+    void fft_mat_vec(const Mat &M, const Poly &a, const Poly &b, Poly &c, Poly &d) {
+        auto chunks = [](const Poly &p) { return p.deg < 0 ? 0 : ((u64)p.deg + 1 + 31) / 32; };
+        u64 need = 1;
+        for (int i = 0; i < 4; i++) {
+            const Poly &v = (i & 1) ? b : a;
+            if (M.e[i].deg >= 0 && v.deg >= 0) need = std::max(need, chunks(M.e[i]) + chunks(v) - 1);
+        }
+        int m = 1;
+        while (((u64)1 << m) < need) m++;
+        gf2e_fft_plan *plan = gf2e::cached_plan(m);
+        if (!plan) throw Fail{GF2E_ERR_CUDA};
+        const u64 n = (u64)1 << m;
+        Buf Fa = alloc(n), Fb = alloc(n), Fm[4];
+        auto fwd = [&](const Poly &p, u64 *f) {
+            if (p.deg < 0) ckc(cudaMemsetAsync(f, 0, n * 8, st_), "fft zero operand");
+            else ck(gf2e::fft_fwd_packed(plan, f, reinterpret_cast<const u32 *>(p.p()), chunks(p), st_));
+        };
+        fwd(a, Fa->p);
+        fwd(b, Fb->p);
+        for (int i = 0; i < 4; i++) {
+            Fm[i] = alloc(n);
+            fwd(M.e[i], Fm[i]->p);
+        }
+        for (int row = 0; row < 2; row++) {
+            u64 *o = Fm[2 * row]->p;
+            k_pw_muladd<<<gf2e::grid_for(n, 256), 256, 0, st_>>>(o, Fm[2 * row]->p, Fa->p,
+                                                                 Fm[2 * row + 1]->p, Fb->p, n);
+            ckc(cudaGetLastError(), "k_pw_muladd");
+            ck(gf2e::fft_run(plan, false, o, st_));
+            long long dmax = std::max(M.e[2 * row].deg + a.deg, M.e[2 * row + 1].deg + b.deg);
+            Poly &out = row ? d : c;
+            out = Poly();
+            if (dmax < 0) { out.b = alloc(1); out.deg = -1; continue; }
+            const u64 nout = (u64)(dmax >> 6) + 2;
+            out.b = alloc(nout);
+            ck(gf2e::overlap_add(o, need, out.p(), nout, st_));
+            out.deg = (long long)nout * 64 - 1;
+        }
+        stats.fft_mul2 += 2;
+    }
+
+    // M2 * M1 (degree bounds)
+    Mat mat_mul(const Mat &M2, const Mat &M1) {
+        Timer tm(stats.us_products);
+        if (M2.ident) return M1;
+        if (M1.ident) return M2;
+        Mat r;
+        for (int i = 0; i < 2; i++)
+            for (int j = 0; j < 2; j++)
+                r.e[2 * i + j] = mul2(M2.e[2 * i], M1.e[j], M2.e[2 * i + 1], M1.e[2 + j]);
+        return r;
+    }
+
+    Mat identity() {
+        Mat I;
+        I.ident = true;
+        return I;
+    }
+    Mat materialize(const Mat &M) {
+        if (!M.ident) return M;
+        Mat r;
+        r.e[0] = constant1();
+        r.e[3] = constant1();
+        r.e[1].b = alloc(1); r.e[1].deg = -1;
+        r.e[2].b = alloc(1); r.e[2].deg = -1;
+        ckc(cudaMemsetAsync(r.e[1].p(), 0, 8, st_), "zero");
+        ckc(cudaMemsetAsync(r.e[2].p(), 0, 8, st_), "zero");
+        return r;
+    }
+
+    // out = x ^ ((q y) << s), new buffer sized for the bound
+    Poly axpy(const Poly &x, const Poly &y, u64 q, long long s, long long deg_bound) {
+        Poly r;
+        const long long dq = deg64_host(q);
+        long long d = x.deg;
+        if (y.deg >= 0 && dq >= 0) d = std::max(d, y.deg + dq + s);
+        d = std::min(d, deg_bound < 0 ? d : deg_bound);
+        if (d < 0) { r.b = alloc(1); r.deg = -1; return r; }
+        const u64 nout = (u64)(d >> 6) + 1;
+        r.b = alloc(nout);
+        k_axpy_q<<<gf2e::grid_for(nout, 256), 256, 0, st_>>>(r.p(), nout, x.p(), x.words(),
+                                                              y.p(), y.words(), q, (u64)s);
+        ckc(cudaGetLastError(), "k_axpy_q");
+        r.deg = d;
+        return r;
+    }
+    static long long deg64_host(u64 v) { return v ? 63 - __builtin_clzll(v) : -1; }
+
+    // (c, d), rows (R0, R1) -> (d, c mod d), rows (R1, R0 + q R1); c, d exact
+    void divstep(Poly &c, Poly &d, Mat *M) {
+        Timer tm(stats.us_division);
+        stats.divsteps++;
+        if (d.deg < 0) throw Fail{gf2e::invalid("hgcd: division by zero")};
+        u64 win[2];
+        Poly cc = c;
+        probe({&cc, &d}, win);
+        u64 wc = win[0];
+        const u64 wd = win[1];
+        Poly r0a, r0b;
+        if (M) { r0a = M->e[0]; r0b = M->e[1]; }
+        bool first = true;
+        for (int guard = 0; cc.deg >= d.deg; guard++) {
+            if (guard > (1 << 22)) throw Fail{gf2e::invalid("hgcd: division did not converge")};
+            const long long delta = cc.deg - d.deg;
+            const int nb = (int)std::min<long long>(delta, 63);   // quotient bits - 1
+            u64 q = 0, r = wc;
+            for (int t = 0; t <= nb; t++)
+                if ((r >> (63 - t)) & 1) {
+                    q |= 1ull << (nb - t);
+                    r ^= wd >> t;
+                }
+            const long long s = delta - nb;
+            // c ^= (q d) << s, in place (the result has lower degree)
+            Poly nc;
+            nc.b = first ? alloc(cc.words()) : cc.b;
+            nc.deg = cc.deg;
+            k_axpy_q<<<gf2e::grid_for(cc.words(), 256), 256, 0, st_>>>(
+                nc.p(), cc.words(), cc.p(), cc.words(), d.p(), d.words(), q, (u64)s);
+            ckc(cudaGetLastError(), "k_axpy_q");
+            if (M) {
+                r0a = axpy(r0a, M->e[2], q, s, -1);
+                r0b = axpy(r0b, M->e[3], q, s, -1);
+            }
+            first = false;
+            cc = nc;
+            probe({&cc}, win);
+            wc = win[0];
+        }
+        if (M) {
+            Poly n0 = M->e[2], n1 = M->e[3];
+            M->e[0] = n0; M->e[1] = n1;
+            M->e[2] = r0a; M->e[3] = r0b;
+        }
+        c = d;
+        d = cc;
+    }
+
+    Mat base(const Poly &a, const Poly &b, long long m) {
+        Timer tm(stats.us_base);
+        stats.bases++;
+        const u64 W = (u64)(a.deg >> 6) + 2;
+        const u64 mw = (u64)((a.deg - m) >> 6) + 3;
+        Buf out = alloc(4 * mw);
+        const size_t smem = (4 * W + 8 * mw + 2 * W + 4 * mw) * 8;
+        {
+            static std::mutex mu;
+            static bool attr[64] = {false};
+            int dev = 0;
+            cudaGetDevice(&dev);
+            std::lock_guard<std::mutex> lk(mu);
+            if (dev >= 0 && dev < 64 && !attr[dev]) {
+                ckc(cudaFuncSetAttribute(k_hgcd_base, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         200 * 1024), "k_hgcd_base smem attribute");
+                attr[dev] = true;
+            }
+        }
+        k_hgcd_base<<<1, BASE_THREADS, smem, st_>>>(a.p(), a.deg, b.p(), b.deg, m, W, mw, out->p,
+                                                    (BaseOut *)d_res_->p);
+        ckc(cudaGetLastError(), "k_hgcd_base");
+        BaseOut res;
+        ckc(cudaMemcpyAsync(&res, d_res_->p, sizeof res, cudaMemcpyDeviceToHost, st_), "base read");
+        ckc(cudaStreamSynchronize(st_), "base sync");
+        if (res.status != GF2E_OK) {
+            gf2e::set_error("hgcd base case status %d", res.status);
+            throw Fail{res.status};
+        }
+        stats.base_rounds += res.rounds;
+        Mat M;
+        const long long dm = a.deg - m;       // entries have degree <= n - m
+        for (int i = 0; i < 4; i++) {         // four views into the output buffer
+            M.e[i].b = alias(out, (size_t)i * mw, mw);
+            M.e[i].deg = std::max(0LL, dm);
+        }
+        return M;
+    }
+
+    // a view into another buffer that keeps it alive
+    Buf alias(const Buf &owner, size_t off, size_t words) {
+        struct View : DBuf {
+            Buf keep;
+            ~View() { p = nullptr; }
+        };
+        auto v = std::make_shared<View>();
+        v->keep = owner;
+        v->p = owner->p + off;
+        v->words = words;
+        v->st = st_;
+        return v;
+    }
+
+    // deg a = n > deg b; exact degrees on entry
+    Mat hgcd(const Poly &a, const Poly &b) {
+        stats.nodes++;
+        const long long n = a.deg, m = (n + 1) / 2;
+        if (b.deg < m) return identity();
+        if (n <= tn_.base_bits) return base(a, b, m);
+        Poly a1 = shr(a, m), b1 = shr(b, m);
+        Mat M1 = hgcd(a1, b1);
+        Poly c, d;
+        mat_vec(M1, a, b, c, d);
+        if (c.deg < d.deg) {                      // not expected; keep the order
+            std::swap(c, d);
+            if (!M1.ident) { std::swap(M1.e[0], M1.e[2]); std::swap(M1.e[1], M1.e[3]); }
+        }
+        if (d.deg < m) return M1;
+        M1 = materialize(M1);
+        divstep(c, d, &M1);
+        if (d.deg < m) return M1;
+        const long long l = c.deg, k = std::max(0LL, 2 * m - l);
+        Poly c1 = shr(c, k), d1 = shr(d, k);
+        Mat M2 = hgcd(c1, d1);
+        return mat_mul(M2, M1);
+    }
+
+    // gcd of two polynomials on the device; returns the gcd (exact degree)
+    Poly gcd(Poly a, Poly b) {
+        for (long long it = 0;; it++) {
+            if (a.deg < b.deg) std::swap(a, b);
+            if (b.deg < 0) return a;
+            if (a.deg < tn_.small_gcd_bits) return small_gcd(a, b);
+            if (a.deg == b.deg) { divstep(a, b, nullptr); continue; }
+            Mat M = hgcd(a, b);
+            if (!M.ident) {
+                Poly c, d;
+                mat_vec(M, a, b, c, d);
+                a = c;
+                b = d;
+                if (a.deg < b.deg) std::swap(a, b);
+            }
+            if (b.deg >= 0) divstep(a, b, nullptr);
+            if (it > 4 * 64) throw Fail{gf2e::invalid("hgcd: no convergence")};
+        }
+    }
+
+    Poly small_gcd(const Poly &a, const Poly &b) {
+        Timer tm(stats.us_small);
+        gf2e_gcd_job job;
+        memset(&job, 0, sizeof job);
+        job.a_dev = a.p();
+        job.abits = (u64)a.deg + 1;
+        job.b_dev = b.p();
+        job.bbits = (u64)b.deg + 1;
+        const u64 gw = (u64)(std::max(a.deg, b.deg) >> 6) + 2;
+        Poly g = zeros(gw);
+        job.g_dev = g.p();
+        job.g_cap_words = gw;
+        size_t need = 0;
+        ck(gf2e_gcd_workspace_size(&job, 1, &need));
+        Buf ws = alloc((need + 7) / 8);
+        int64_t deg = -1;
+        ck(gf2e_gcd_batch(&job, 1, &deg, ws->p, need, st_));
+        g.deg = deg;
+        return g;
+    }
+
+private:
+    cudaStream_t st_;
+    cudaMemPool_t pool_;
+    Tunables tn_;
+    long long *h_probe_ = nullptr;
+    Buf d_probe_, d_res_;
+};
+
+cudaMemPool_t hgcd_pool() {
+    static std::mutex mu;
+    static cudaMemPool_t pools[64] = {};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    std::lock_guard<std::mutex> lk(mu);
+    if (dev < 0 || dev >= 64) return nullptr;
+    if (!pools[dev]) {
+        cudaMemPoolProps props;
+        memset(&props, 0, sizeof props);
+        props.allocType = cudaMemAllocationTypePinned;
+        props.location.type = cudaMemLocationTypeDevice;
+        props.location.id = dev;
+        if (cudaMemPoolCreate(&pools[dev], &props) != cudaSuccess) return nullptr;
+        u64 keep = ~0ull;      // keep freed memory in the pool between gcds
+        cudaMemPoolSetAttribute(pools[dev], cudaMemPoolAttrReleaseThreshold, &keep);
+    }
+    return pools[dev];
+}
+
+int run_one(const gf2e_gcd_job &j, int64_t *deg_out, gf2e_hgcd_stats *stats, cudaStream_t st) {
+    cudaMemPool_t pool = hgcd_pool();
+    if (!pool) return gf2e::cuda_status(cudaErrorMemoryAllocation, "hgcd memory pool");
+    try {
+        Hgcd H(st, pool);
+        Poly a = H.from_device(j.a_dev, j.abits), b = H.from_device(j.b_dev, j.bbits);
+        Poly g = H.gcd(a, b);
+        *deg_out = g.deg < 0 ? 0 : g.deg;
+        if (j.g_dev && j.g_cap_words) {
+            const u64 gw = g.deg < 0 ? 0 : g.words();
+            if (gw <= j.g_cap_words) {
+                ckc(cudaMemsetAsync(j.g_dev, 0, j.g_cap_words * 8, st), "gcd out clear");
+                if (gw) ckc(cudaMemcpyAsync(j.g_dev, g.p(), gw * 8, cudaMemcpyDeviceToDevice, st),
+                            "gcd out");
+            }
+        }
+        ckc(cudaStreamSynchronize(st), "hgcd done");
+        if (stats) {
+            stats->nodes = H.stats.nodes;
+            stats->base_cases = H.stats.bases;
+            stats->base_rounds = H.stats.base_rounds;
+            stats->fft_products = H.stats.fft_mul2;
+            stats->school_products = H.stats.school_mul2;
+            stats->division_steps = H.stats.divsteps;
+            stats->probes = H.stats.probes;
+            stats->us_base = (int64_t)H.stats.us_base;
+            stats->us_products = (int64_t)H.stats.us_products;
+            stats->us_division = (int64_t)H.stats.us_division;
+            stats->us_small_gcd = (int64_t)H.stats.us_small;
+        }
+        return GF2E_OK;
+    } catch (const Fail &f) {
+        cudaStreamSynchronize(st);
+        return f.st;
+    }
+}
+
+}  // namespace
+
+extern "C" {
+
+int gf2e_gcd_large(const gf2e_gcd_job *jobs, int njobs, int64_t *deg_host, int max_parallel,
+                   gf2e_hgcd_stats *stats, void *stream) {
+    if (!jobs || njobs < 1 || !deg_host) return gf2e::invalid("gf2e_gcd_large: bad job list");
+    for (int i = 0; i < njobs; i++)
+        if (!jobs[i].a_dev || !jobs[i].b_dev || !jobs[i].abits || !jobs[i].bbits)
+            return gf2e::invalid("gf2e_gcd_large: empty operand in job %d", i);
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return gf2e::cuda_status(e, "gf2e_gcd_large device");
+    // the caller's stream must have produced the operands before we start
+    cudaEvent_t ready;
+    e = cudaEventCreateWithFlags(&ready, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventRecord(ready, (cudaStream_t)stream);
+    if (e == cudaSuccess) e = cudaEventSynchronize(ready);
+    cudaEventDestroy(ready);
+    if (e != cudaSuccess) return gf2e::cuda_status(e, "gf2e_gcd_large operands");
+    const int nthreads = std::max(1, std::min(njobs, max_parallel < 1 ? 1 : max_parallel));
+    std::atomic<int> next(0), worst(GF2E_OK);
+    std::vector<gf2e_hgcd_stats> st(njobs);
+    memset(st.data(), 0, njobs * sizeof(gf2e_hgcd_stats));
+    auto worker = [&]() {
+        cudaSetDevice(dev);
+        cudaStream_t s;
+        if (cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) != cudaSuccess) {
+            worst = GF2E_ERR_CUDA;
+            return;
+        }
+        for (int i; (i = next.fetch_add(1)) < njobs;) {
+            int64_t d = -1;
+            int rc = run_one(jobs[i], &d, &st[i], s);
+            deg_host[i] = d;
+            if (rc != GF2E_OK) worst = rc;
+        }
+        cudaStreamDestroy(s);
+    };
+    if (nthreads == 1) {
+        worker();
+    } else {
+        std::vector<std::thread> th;
+        for (int t = 0; t < nthreads; t++) th.emplace_back(worker);
+        for (auto &t : th) t.join();
+    }
+    if (stats) {
+        memset(stats, 0, sizeof *stats);
+        for (auto &s : st) {
+            stats->nodes += s.nodes;
+            stats->base_cases += s.base_cases;
+            stats->base_rounds += s.base_rounds;
+            stats->fft_products += s.fft_products;
+            stats->school_products += s.school_products;
+            stats->division_steps += s.division_steps;
+            stats->probes += s.probes;
+            stats->us_base += s.us_base;
+            stats->us_products += s.us_products;
+            stats->us_division += s.us_division;
+            stats->us_small_gcd += s.us_small_gcd;
+        }
+    }
+    return worst.load();
+}
+
+}  // extern "C"

@@ -316,6 +316,32 @@ def gcd_batch(pairs, g_cap_words: int = 0, stream=None):
     return degs, gs
 
 
+def gcd_large(pairs, g_cap_words: int = 0, max_parallel: int = 1, stream=None):
+    """Subquadratic (half-gcd) gcd of every (a_dev, abits, b_dev, bbits) pair,
+    same contract as gcd_batch; for operands of millions of bits up to
+    r = 136279841 (the reference delegates these to NTL, gf2_gcd_ntl.cpp:32-42).
+    Returns (degrees, gcds or None, work counters)."""
+    from ._lib import GcdJob, HgcdStats
+    n = len(pairs)
+    jobs = (GcdJob * n)()
+    outs = []
+    for i, (a, ab, b, bb) in enumerate(pairs):
+        g = DeviceBuffer(8 * g_cap_words) if g_cap_words else None
+        outs.append(g)
+        jobs[i] = GcdJob(_ptr(a), ab, _ptr(b), bb, g.ptr if g else None, g_cap_words)
+    degs = np.zeros(n, dtype=np.int64)
+    st = HgcdStats()
+    call("gf2e_gcd_large", C.cast(jobs, C.c_void_p), n, degs.ctypes.data, max_parallel,
+         C.byref(st), _sp(stream))
+    gs = []
+    for d, g in zip(degs.tolist(), outs):
+        if g is None or d // 64 + 1 > g_cap_words:
+            gs.append(None)
+        else:
+            gs.append(g.to_numpy(g_cap_words))
+    return degs, gs, st.as_dict()
+
+
 def _hex(words) -> str:
     x = 0
     for i, w in enumerate(np.asarray(words, dtype=np.uint64).tolist()):
