@@ -350,6 +350,8 @@ typedef struct gf2e_hgcd_stats {
     int64_t us_products;      /* ... in matrix products (incl. degree reads) */
     int64_t us_division;      /* ... in division steps */
     int64_t us_small_gcd;     /* ... in the final quadratic gcd */
+    int64_t base_cycles_serial;  /* SM cycles of base cases in the serial window phase */
+    int64_t base_cycles_total;   /* SM cycles of base cases in total */
 } gf2e_hgcd_stats;
 
 int gf2e_gcd_large(const gf2e_gcd_job *jobs, int njobs, int64_t *deg_host,

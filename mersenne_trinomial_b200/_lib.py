@@ -50,7 +50,8 @@ class MulJob(C.Structure):
 class HgcdStats(C.Structure):
     _fields_ = [(k, C.c_int64) for k in ("nodes", "base_cases", "base_rounds", "fft_products",
                                         "school_products", "division_steps", "probes", "us_base",
-                                        "us_products", "us_division", "us_small_gcd")]
+                                        "us_products", "us_division", "us_small_gcd",
+                                        "base_cycles_serial", "base_cycles_total")]
 
     def as_dict(self) -> dict:
         return {k: getattr(self, k) for k, _ in self._fields_}

@@ -207,6 +207,7 @@ GF2E_DEV u64 win_at(const u64 *X, long long nw, long long pos) {   // bits pos..
 struct BaseOut {
     long long deg_a, deg_b;     // degrees of the reduced pair
     long long rounds;
+    long long cyc_serial, cyc_total;   // SM clock cycles: thread-0 window phase, whole kernel
     int status;
 };
 
@@ -266,6 +267,8 @@ k_hgcd_base(const u64 *__restrict__ a, long long da0, const u64 *__restrict__ b,
     __syncthreads();
     const long long max_rounds = 2 * (da0 + 2) + 16;
     long long known_a = 1, known_b = 1;          // warp 0 only: degrees known exactly
+    const long long cyc0 = clock64();
+    long long cyc_serial = 0;
     for (long long round = 0;; round++) {
         if (tid < 32) {
             // finish the previous round: degrees the windows did not settle
@@ -274,6 +277,7 @@ k_hgcd_base(const u64 *__restrict__ a, long long da0, const u64 *__restrict__ b,
                 if (!known_b) { long long d = warp_degree(V + (u64)s_vb * W, s_top); if (tid == 0) s_db = d; }
             }
             if (tid == 0) {
+                const long long c0 = clock64();
                 long long da = s_da, db = s_db;
                 if (da < db) {                           // keep deg A >= deg B (rows too)
                     int t = s_va; s_va = s_vb; s_vb = t;
@@ -330,6 +334,7 @@ k_hgcd_base(const u64 *__restrict__ a, long long da0, const u64 *__restrict__ b,
                     }
                     s_top = da >> 6;
                 }
+                cyc_serial += clock64() - c0;
             }
             known_a = __shfl_sync(0xffffffffu, known_a, 0);
             known_b = __shfl_sync(0xffffffffu, known_b, 0);
@@ -429,6 +434,8 @@ k_hgcd_base(const u64 *__restrict__ a, long long da0, const u64 *__restrict__ b,
         res->deg_a = s_da;
         res->deg_b = s_db;
         res->rounds = s_rounds;
+        res->cyc_serial = cyc_serial;
+        res->cyc_total = clock64() - cyc0;
         res->status = s_status;
     }
 }
@@ -491,7 +498,7 @@ Tunables tunables() {
 
 struct Stats {
     long long nodes = 0, bases = 0, base_rounds = 0, fft_mul2 = 0, school_mul2 = 0, divsteps = 0,
-              probes = 0;
+              probes = 0, cyc_serial = 0, cyc_total = 0;
     double us_base = 0, us_products = 0, us_division = 0, us_small = 0;
 };
 
@@ -832,6 +839,8 @@ public:
             throw Fail{res.status};
         }
         stats.base_rounds += res.rounds;
+        stats.cyc_serial += res.cyc_serial;
+        stats.cyc_total += res.cyc_total;
         Mat M;
         const long long dm = a.deg - m;       // entries have degree <= n - m
         for (int i = 0; i < 4; i++) {         // four views into the output buffer
@@ -977,6 +986,8 @@ int run_one(const gf2e_gcd_job &j, int64_t *deg_out, gf2e_hgcd_stats *stats, cud
             stats->us_products = (int64_t)H.stats.us_products;
             stats->us_division = (int64_t)H.stats.us_division;
             stats->us_small_gcd = (int64_t)H.stats.us_small;
+            stats->base_cycles_serial = H.stats.cyc_serial;
+            stats->base_cycles_total = H.stats.cyc_total;
         }
         return GF2E_OK;
     } catch (const Fail &f) {
@@ -1045,6 +1056,8 @@ int gf2e_gcd_large(const gf2e_gcd_job *jobs, int njobs, int64_t *deg_host, int m
             stats->us_products += s.us_products;
             stats->us_division += s.us_division;
             stats->us_small_gcd += s.us_small_gcd;
+            stats->base_cycles_serial += s.base_cycles_serial;
+            stats->base_cycles_total += s.base_cycles_total;
         }
     }
     return worst.load();

@@ -66,7 +66,14 @@ struct gf2e_scanner {
     struct GraphKey { int nact; const u64 *F; };
     std::vector<std::pair<GraphKey, cudaGraphExec_t>> graphs;
     bool use_graphs = true;
+    int gcd_parallel = 16;        // concurrent half-gcds at interval ends (large r)
 };
+
+// operands of at least this many bits take the half-gcd (hgcd.cu) at
+// interval ends; smaller ones the quadratic batched gcd (gcd.cu)
+constexpr u64 GCD_LARGE_BITS = 1ull << 19;
+// device words a concurrent half-gcd job draws from its pool, per operand word
+constexpr size_t HGCD_WORDS_PER_WORD = 48;
 
 namespace {
 
@@ -206,8 +213,13 @@ int degree_step(gf2e_scanner &S, cudaStream_t st) {
         S.jobs[q] = gf2e_gcd_job{S.ACC + S.stride * j, S.r, S.T + S.tw * j, S.r + 1,
                                  S.G + S.gcap * q, S.gcap};
     }
-    GF2E_TRY(gf2e_gcd_batch(S.jobs.data(), (int)due.size(), S.degs.data(), S.gws, S.gws_bytes,
-                            st));
+    if (S.r >= GCD_LARGE_BITS) {
+        const int par = std::max(1, std::min((int)due.size(), S.gcd_parallel));
+        GF2E_TRY(gf2e_gcd_large(S.jobs.data(), (int)due.size(), S.degs.data(), par, nullptr, st));
+    } else {
+        GF2E_TRY(gf2e_gcd_batch(S.jobs.data(), (int)due.size(), S.degs.data(), S.gws,
+                                S.gws_bytes, st));
+    }
     std::vector<int> retire;
     for (size_t q = 0; q < due.size(); q++) {
         int j = due[q];
@@ -263,8 +275,14 @@ int gf2e_scanner_footprint(uint64_t r, int slots, size_t *bytes) {
     if (!bytes || slots < 1 || r < 5) return gf2e::invalid("bad footprint query");
     Geometry g = geometry(r);
     size_t words = device_words(g, slots);
-    // gcd workspace: job table + 4 buffers per job
+    // gcd workspace: job table + 4 buffers per job (quadratic gcd), or the
+    // pools of the concurrent half-gcds
     size_t gw = ((size_t)slots * 96 + 255) + (size_t)slots * 4 * (g.tw + 1) * 8;
+    if (r >= GCD_LARGE_BITS) {
+        int par = 16;
+        if (const char *env = getenv("GF2E_SCAN_GCD_PARALLEL")) par = std::max(1, atoi(env));
+        gw = (size_t)std::min(par, slots) * HGCD_WORDS_PER_WORD * (g.tw + 1) * 8;
+    }
     *bytes = words * 8 + gw;
     return GF2E_OK;
 }
@@ -294,8 +312,9 @@ int gf2e_scanner_create(uint64_t r, int slots, gf2e_scanner **out) {
     S->sdev = S->T + g.tw * B;
     S->G = S->sdev + B;
     std::vector<gf2e_gcd_job> tmp(B, gf2e_gcd_job{S->ACC, r, S->T, r + 1, S->G, g.gcap});
-    int st = gf2e_gcd_workspace_size(tmp.data(), B, &S->gws_bytes);
-    if (st == GF2E_OK) {
+    int st = GF2E_OK;
+    if (r < GCD_LARGE_BITS) st = gf2e_gcd_workspace_size(tmp.data(), B, &S->gws_bytes);
+    if (st == GF2E_OK && r < GCD_LARGE_BITS) {
         e = cudaMalloc(&S->gws, S->gws_bytes);
         if (e != cudaSuccess) st = gf2e::cuda_status(e, "scanner gcd workspace");
     }
@@ -312,6 +331,7 @@ int gf2e_scanner_create(uint64_t r, int slots, gf2e_scanner **out) {
         return gf2e::cuda_status(e, "scanner stream");
     }
     if (const char *env = getenv("GF2E_SCAN_GRAPHS")) S->use_graphs = env[0] != '0';
+    if (const char *env = getenv("GF2E_SCAN_GCD_PARALLEL")) S->gcd_parallel = std::max(1, atoi(env));
     S->slot.resize(B);
     S->shost.assign(B, 0);
     S->thost.assign(g.tw, 0);

@@ -64,3 +64,14 @@ def test_scan_rejects_bad_arguments(engine):
         engine.scan(4423, [2212], 5, 200)
     with pytest.raises(engine.Gf2eError):
         engine.scan(4423, [3], 5, 5)
+
+
+@pytest.mark.timeout(900)
+def test_scan_r136279841_known_answer(engine, oracle):
+    """Config-4 path end to end at r = 136279841: ramp to k0 = 24, running
+    product of (x^(2^k) + x) mod T for k = 25.., half-gcd at the interval
+    end, hit resolution.  The reference's certificate for s = 474 is
+    `474 41 p3991ef16129` (tsfactor_handoff.md:337)."""
+    got = engine.scan(136279841, [474], 24, 200, L0=64, Lmax=4096, batch=1)
+    assert got == ["474 41 p3991ef16129"]
+    assert oracle.factor_divides(136279841, 474, 41, "3991ef16129") == 1
