@@ -439,6 +439,7 @@ def run_extras(torch, M, W):
                            "default": dflt_row[0]["ms"] if dflt_row else None}}
     del bufs, jobs, wsb
     out["deep_scan_r136279841"] = deep_scan_sample(torch, M)
+    out["deep_scan_r136279841_with_gcd"] = deep_scan_gcd_sample(M)
     out["serving"] = serving_sample()
     return out
 
@@ -446,8 +447,8 @@ def run_extras(torch, M, W):
 def deep_scan_sample(torch, M, nsurv=4, degrees=32):
     """Config 4's per-degree leg at full size: F <- F^2 and ACC <- ACC*(F+x)
     mod T for `nsurv` d<=24 survivors of r = 136279841, batched, degrees
-    25..24+degrees.  The interval gcd at this size needs a subquadratic gcd
-    (not built), so the sample stops before the first interval end."""
+    25..24+degrees; the interval-end half-gcds are measured by
+    deep_scan_gcd_sample."""
     import ctypes as C
     from mersenne_trinomial_b200._lib import call
     smax = 200000
@@ -471,7 +472,26 @@ def deep_scan_sample(torch, M, nsurv=4, degrees=32):
     return {"survivors": surv, "degrees": degrees, "ms": ms,
             "sd_pairs_per_s": nsurv * degrees / (ms / 1e3),
             "ms_per_degree_per_s": ms / degrees / nsurv,
-            "note": "square + running product per degree; gcd leg not run at this size"}
+            "note": "square + running product per degree (no interval end in the sample)"}
+
+
+def deep_scan_gcd_sample(M, nsurv=8, maxd=88):
+    """Config 4's full cycle at r = 136279841 on a bounded sample: `nsurv`
+    d<=24 survivors (s = 474 first, the reference's known answer
+    `474 41 p3991ef16129`), ramp to k0 = 24, running products for degrees
+    25..maxd, then the interval-end gcds (concurrent half-gcds) and hit
+    resolution; wall time of the whole scan call."""
+    smax = 200000
+    best = M.run_sieve(R, 24, smax)
+    surv = [474] + [s for s in range(3, smax + 1)
+                    if int(best[s]) == 0xFFFFFFFFFFFFFFFF and s != 474][:nsurv - 1]
+    t0 = time.perf_counter()
+    lines = M.scan(R, surv, 24, maxd, L0=maxd - 24, Lmax=4096, batch=nsurv)
+    wall = time.perf_counter() - t0
+    return {"survivors": surv, "k0": 24, "maxd": maxd, "results": lines, "wall_s": wall,
+            "sd_pairs_per_s": nsurv * (maxd - 24) / wall,
+            "known_answer_474": "474 41 p3991ef16129" in lines,
+            "note": "one interval of 64 degrees then one half-gcd per s (concurrent)"}
 
 
 def serving_sample(n_jobs=16, rate=8.0, seed=1):

@@ -54,7 +54,7 @@ u64 fft_plan_n(const gf2e_fft_plan *plan);
 
 namespace {
 
-constexpr int BASE_THREADS = 256;
+constexpr int BASE_THREADS = 512;
 
 // ------------------------------------------------------------------ device
 GF2E_DEV void clmul64(u64 a, u64 b, u64 &lo, u64 &hi) {
@@ -230,14 +230,16 @@ GF2E_DEV long long warp_degree(const u64 *X, long long top) {
 // (a', b') = M (a, b) with deg a' >= m > deg b'; M written to four arrays of
 // mw words (row-major M00 M01 M10 M11).
 //
-// Each round, thread 0 runs Euclid steps on the 64-bit top windows of A and
-// B (Lehmer), accumulating a 2x2 matrix of degree <= 31 while the bits it
-// decides on are exact and the half-gcd stop (deg B < m) is not reached; the
-// CTA then applies the matrix to A, B and to the accumulated rows.  When the
-// final windows are exact at their leading bits the new degrees are known
-// without a scan; otherwise warp 0 scans down from the old top word.
+// Each round, thread 0 runs Euclid on the 64-bit top windows of A and B
+// (Lehmer): whole quotients, each taken only when every bit it depends on is
+// exact (window bits of a row lie above that row's matrix degree) and the
+// half-gcd stop (deg B < m) is not reached, while the accumulated 2x2 matrix
+// stays within degree 31.  The CTA then applies the matrix to A, B and to the
+// accumulated rows, one output word per thread.  Leading bits that were exact
+// in the windows give the new degrees; otherwise warp 0 scans down from the
+// old top word.  A degree gap the matrix cannot hold is one shift-XOR round.
 // Shared memory: V[4][W] (two buffers of A, B), R[2][4][mw] (two buffers of
-// the rows), carries C[2W + 4mw].
+// the rows), carries of 2W + 4mw words.
 __global__ void __launch_bounds__(BASE_THREADS)
 k_hgcd_base(const u64 *__restrict__ a, long long da0, const u64 *__restrict__ b, long long db0,
             long long m, u64 W, u64 mw, u64 *__restrict__ Mout, BaseOut *res) {
@@ -246,197 +248,213 @@ k_hgcd_base(const u64 *__restrict__ a, long long da0, const u64 *__restrict__ b,
     u64 *R = sh + 4 * W;
     u64 *hiv = R + 8 * mw;
     u64 *hir = hiv + 2 * W;
-    __shared__ int s_va, s_vb, s_ra, s_buf, s_mode, s_done, s_status;
-    __shared__ long long s_da, s_db, s_md, s_k, s_rounds, s_top;
+    __shared__ int s_va, s_vb, s_ra, s_buf, s_mode, s_done;
+    __shared__ long long s_md, s_k, s_top;
     __shared__ u32 s_m[4];
     const int tid = threadIdx.x;
-    for (u64 i = tid; i < 2 * W; i += BASE_THREADS) {
-        u64 v;
+    for (u64 i = tid; i < 4 * W; i += BASE_THREADS) {
+        u64 v = 0;
         if (i < W) v = (i <= (u64)(da0 >> 6)) ? a[i] : 0;
-        else { u64 j = i - W; v = (db0 >= 0 && j <= (u64)(db0 >> 6)) ? b[j] : 0; }
+        else if (i < 2 * W) { u64 j = i - W; v = (db0 >= 0 && j <= (u64)(db0 >> 6)) ? b[j] : 0; }
         V[i] = v;
     }
     for (u64 i = tid; i < 8 * mw; i += BASE_THREADS) R[i] = (i == 0 || i == 3 * mw) ? 1 : 0;
     if (tid == 0) {
-        s_va = 0; s_vb = 1; s_buf = 0;     // A = V[s_va], B = V[s_vb]; rows in R[s_buf]
-        s_ra = 0;                          // row block of A (B's is s_ra ^ 1)
-        s_top = 0;
-        s_da = da0; s_db = db0; s_md = 0; s_done = 0;
-        s_status = GF2E_ERR_INTERNAL;
+        s_va = 0; s_vb = 1; s_ra = 0; s_buf = 0;
+        s_md = 0; s_done = 0; s_top = 0;
     }
     __syncthreads();
+    // warp-0 registers: degrees, buffer roles, round bookkeeping
+    long long da = da0, db = db0;
+    int va = 0, vb = 1, ra = 0, status = GF2E_ERR_INTERNAL;
+    bool known_a = true, known_b = true;
+    long long top = 0, rounds = 0;
     const long long max_rounds = 2 * (da0 + 2) + 16;
-    long long known_a = 1, known_b = 1;          // warp 0 only: degrees known exactly
     const long long cyc0 = clock64();
     long long cyc_serial = 0;
     for (long long round = 0;; round++) {
         if (tid < 32) {
-            // finish the previous round: degrees the windows did not settle
             if (round > 0) {
-                if (!known_a) { long long d = warp_degree(V + (u64)s_va * W, s_top); if (tid == 0) s_da = d; }
-                if (!known_b) { long long d = warp_degree(V + (u64)s_vb * W, s_top); if (tid == 0) s_db = d; }
+                // the spare buffers hold the new A, B; rows were written in (A, B) order
+                int spare[2], ns = 0;
+                for (int i = 0; i < 4 && ns < 2; i++)
+                    if (i != va && i != vb) spare[ns++] = i;
+                va = spare[0]; vb = spare[1]; ra = 0;
+                if (!known_a) da = warp_degree(V + (u64)va * W, top);
+                if (!known_b) db = warp_degree(V + (u64)vb * W, top);
             }
             if (tid == 0) {
                 const long long c0 = clock64();
-                long long da = s_da, db = s_db;
-                if (da < db) {                           // keep deg A >= deg B (rows too)
-                    int t = s_va; s_va = s_vb; s_vb = t;
-                    s_ra ^= 1;
-                    s_da = db; s_db = da;
-                    da = s_da; db = s_db;
+                if (da < db) {
+                    long long t = da; da = db; db = t;
+                    int x = va; va = vb; vb = x;
+                    ra ^= 1;
                 }
-                s_mode = 0;
+                int mode = 0;
+                bool done = false;
                 if (db < m || round > max_rounds) {
-                    s_done = 1;
-                    s_status = (round > max_rounds) ? GF2E_ERR_TIMEOUT : GF2E_OK;
-                    s_rounds = round;
+                    done = true;
+                    status = (round > max_rounds) ? GF2E_ERR_TIMEOUT : GF2E_OK;
+                    rounds = round;
                 } else {
-                    const u64 *A = V + (u64)s_va * W, *B = V + (u64)s_vb * W;
+                    const u64 *A = V + (u64)va * W, *B = V + (u64)vb * W;
                     const long long lo = da >= 63 ? da - 63 : 0;
                     u64 wa = win_at(A, (long long)W, lo), wb = win_at(B, (long long)W, lo);
                     u32 ma0 = 1, ma1 = 0, mb0 = 0, mb1 = 1;
                     int dga = (int)(da - lo), dgb = deg64(wb), dma = 0, dmb = 0, steps = 0;
                     const bool exact = (lo == 0);
-                    const int dstop = (int)max(-1LL, m - lo);      // window degree of deg m
-                    for (int it = 0; it < 256; it++) {
-                        if (dgb < 0) break;
-                        if (dga < dgb) {
-                            u64 t = wa; wa = wb; wb = t;
-                            u32 x = ma0; ma0 = mb0; mb0 = x;
-                            x = ma1; ma1 = mb1; mb1 = x;
-                            int y = dga; dga = dgb; dgb = y;
-                            y = dma; dma = dmb; dmb = y;
-                        }
-                        if (!exact && (dgb < dmb || dga < dma)) break;   // undecided bits
-                        if (dgb < dstop) break;                          // half-gcd stop
-                        const int k = dga - dgb;
-                        const int ndm = max(dma, dmb + k);
-                        if (ndm > 31) break;
-                        wa ^= wb << k;
-                        ma0 ^= mb0 << k;
-                        ma1 ^= mb1 << k;
+                    const int dstop = (int)max(-1LL, m - lo);      // window degree of x^m
+                    for (int it = 0; it < 64; it++) {
+                        if (dgb < 0 || dgb < dstop) break;          // b = 0 / half-gcd stop
+                        const int dq = dga - dgb;
+                        const int ndm = max(dma, dmb + dq);
+                        if (ndm > 31) break;                         // matrix degree bound
+                        if (!exact && dgb < max(dma, dmb + dq)) break;   // quotient not exact
+#pragma unroll 1
+                        do {                                         // a <- a mod b
+                            const int k = dga - dgb;
+                            wa ^= wb << k;
+                            ma0 ^= mb0 << k;
+                            ma1 ^= mb1 << k;
+                            dga = deg64(wa);
+                        } while (dga >= dgb);
                         dma = ndm;
-                        dga = deg64(wa);
+                        u64 t = wa; wa = wb; wb = t;                 // (a, b) <- (b, a mod b)
+                        u32 y = ma0; ma0 = mb0; mb0 = y;
+                        y = ma1; ma1 = mb1; mb1 = y;
+                        int z = dga; dga = dgb; dgb = z;
+                        z = dma; dma = dmb; dmb = z;
                         steps++;
                     }
+                    top = da >> 6;
                     if (steps == 0) {
-                        s_mode = 1;                                // A ^= B << (da - db)
+                        mode = 1;                                    // A ^= B << (da - db)
                         s_k = da - db;
-                        known_a = 0;
-                        known_b = 1;
+                        known_a = false;
+                        known_b = true;
                     } else {
                         s_m[0] = ma0; s_m[1] = ma1; s_m[2] = mb0; s_m[3] = mb1;
-                        // exact leading bits give the new degrees directly
-                        known_a = (exact || dga >= dma) ? 1 : 0;
-                        known_b = (exact || (dgb >= 0 && dgb >= dmb)) ? 1 : 0;
-                        if (known_a) s_da = dga < 0 ? -1 : dga + lo;
-                        if (known_b) s_db = dgb < 0 ? -1 : dgb + lo;
+                        known_a = true;                              // the old b's exact lead
+                        da = dga + lo;
+                        known_b = exact || (dgb >= 0 && dgb >= dmb);
+                        if (known_b) db = dgb < 0 ? -1 : dgb + lo;
                     }
-                    s_top = da >> 6;
                 }
+                s_mode = mode;
+                s_done = done;
+                s_va = va; s_vb = vb; s_ra = ra; s_top = top;
                 cyc_serial += clock64() - c0;
             }
+            // share thread 0's decisions with the rest of warp 0
+            da = __shfl_sync(0xffffffffu, da, 0);
+            db = __shfl_sync(0xffffffffu, db, 0);
+            va = __shfl_sync(0xffffffffu, va, 0);
+            vb = __shfl_sync(0xffffffffu, vb, 0);
+            ra = __shfl_sync(0xffffffffu, ra, 0);
+            top = __shfl_sync(0xffffffffu, top, 0);
             known_a = __shfl_sync(0xffffffffu, known_a, 0);
             known_b = __shfl_sync(0xffffffffu, known_b, 0);
         }
         __syncthreads();
         if (s_done) break;
-        const int va = s_va, vb = s_vb, buf = s_buf, nb = buf ^ 1, ra = s_ra, rb = s_ra ^ 1;
-        const long long nwv = s_top + 1;                        // live vector words
-        const long long nwm = min((long long)mw, s_md + 2);     // live matrix words
+        const int cva = s_va, cvb = s_vb, buf = s_buf, nb = buf ^ 1, cra = s_ra, crb = s_ra ^ 1;
+        const long long nwv = s_top + 1;                       // live vector words
+        const long long nwm = min((long long)mw, s_md + 2);    // live matrix words
         int spare[2], ns = 0;
         for (int i = 0; i < 4 && ns < 2; i++)
-            if (i != va && i != vb) spare[ns++] = i;
-        const u64 *A = V + (u64)va * W, *B = V + (u64)vb * W;
-        u64 *A2 = V + (u64)spare[0] * W, *B2 = V + (u64)spare[1] * W;
-        const u64 *Ra0 = R + (u64)(buf * 4 + 2 * ra) * mw, *Ra1 = R + (u64)(buf * 4 + 2 * ra + 1) * mw;
-        const u64 *Rb0 = R + (u64)(buf * 4 + 2 * rb) * mw, *Rb1 = R + (u64)(buf * 4 + 2 * rb + 1) * mw;
-        u64 *Na0 = R + (u64)(nb * 4 + 0) * mw, *Na1 = R + (u64)(nb * 4 + 1) * mw;
-        u64 *Nb0 = R + (u64)(nb * 4 + 2) * mw, *Nb1 = R + (u64)(nb * 4 + 3) * mw;
+            if (i != cva && i != cvb) spare[ns++] = i;
+        const u64 *VA = V + (u64)cva * W, *VB = V + (u64)cvb * W;
+        u64 *V2a = V + (u64)spare[0] * W, *V2b = V + (u64)spare[1] * W;
+        const u64 *RA = R + (u64)(buf * 4 + 2 * cra) * mw;     // row of A: col c at RA + c*mw
+        const u64 *RB = R + (u64)(buf * 4 + 2 * crb) * mw;
+        u64 *N = R + (u64)nb * 4 * mw;                          // new rows, entry e at N + e*mw
         if (s_mode == 1) {
             const long long k = s_k, ks = k >> 6;
             const unsigned kb = (unsigned)(k & 63);
-            for (long long w = tid; w < nwv; w += BASE_THREADS) {
-                u64 hi = (w >= ks) ? B[w - ks] : 0, lo2 = (w >= ks + 1) ? B[w - ks - 1] : 0;
-                A2[w] = A[w] ^ (kb ? ((hi << kb) | (lo2 >> (64 - kb))) : hi);
-                B2[w] = B[w];
+            auto shl = [&](const u64 *X, long long w) -> u64 {
+                u64 h = (w >= ks) ? X[w - ks] : 0, l = (w >= ks + 1) ? X[w - ks - 1] : 0;
+                return kb ? ((h << kb) | (l >> (64 - kb))) : h;
+            };
+            for (long long w = tid; w < (long long)W; w += BASE_THREADS) {
+                V2a[w] = (w < nwv) ? (VA[w] ^ shl(VB, w)) : 0;
+                V2b[w] = (w < nwv) ? VB[w] : 0;
             }
             for (long long w = tid; w < (long long)mw; w += BASE_THREADS) {
-                u64 h0 = (w >= ks) ? Rb0[w - ks] : 0, l0 = (w >= ks + 1) ? Rb0[w - ks - 1] : 0;
-                u64 h1 = (w >= ks) ? Rb1[w - ks] : 0, l1 = (w >= ks + 1) ? Rb1[w - ks - 1] : 0;
-                Na0[w] = Ra0[w] ^ (kb ? ((h0 << kb) | (l0 >> (64 - kb))) : h0);
-                Na1[w] = Ra1[w] ^ (kb ? ((h1 << kb) | (l1 >> (64 - kb))) : h1);
-                Nb0[w] = Rb0[w];
-                Nb1[w] = Rb1[w];
+                N[0 * mw + w] = RA[w] ^ shl(RB, w);
+                N[1 * mw + w] = RA[mw + w] ^ shl(RB + mw, w);
+                N[2 * mw + w] = RB[w];
+                N[3 * mw + w] = RB[mw + w];
             }
             __syncthreads();
             if (tid == 0) s_md = min((long long)mw - 2, s_md + ks + 1);
         } else {
-            const Masked m0 = mask32(s_m[0]), m1 = mask32(s_m[1]), m2 = mask32(s_m[2]),
-                         m3 = mask32(s_m[3]);
-            for (long long w = tid; w < nwv; w += BASE_THREADS) {
-                u64 x = A[w], y = B[w];
-                u64 l0, h0, l1, h1, l2, h2, l3, h3;
-                mul64x32(x, m0, l0, h0); mul64x32(y, m1, l1, h1);
-                mul64x32(x, m2, l2, h2); mul64x32(y, m3, l3, h3);
-                A2[w] = l0 ^ l1;
-                B2[w] = l2 ^ l3;
-                hiv[2 * w] = h0 ^ h1;
-                hiv[2 * w + 1] = h2 ^ h3;
-            }
-            for (long long w = tid; w < nwm; w += BASE_THREADS) {
-                u64 x0 = Ra0[w], y0 = Rb0[w], x1 = Ra1[w], y1 = Rb1[w];
-                u64 l0, h0, l1, h1;
-                mul64x32(x0, m0, l0, h0); mul64x32(y0, m1, l1, h1);
-                Na0[w] = l0 ^ l1; hir[4 * w + 0] = h0 ^ h1;
-                mul64x32(x1, m0, l0, h0); mul64x32(y1, m1, l1, h1);
-                Na1[w] = l0 ^ l1; hir[4 * w + 1] = h0 ^ h1;
-                mul64x32(x0, m2, l0, h0); mul64x32(y0, m3, l1, h1);
-                Nb0[w] = l0 ^ l1; hir[4 * w + 2] = h0 ^ h1;
-                mul64x32(x1, m2, l0, h0); mul64x32(y1, m3, l1, h1);
-                Nb1[w] = l0 ^ l1; hir[4 * w + 3] = h0 ^ h1;
+            const Masked k0 = mask32(s_m[0]), k1 = mask32(s_m[1]), k2 = mask32(s_m[2]),
+                         k3 = mask32(s_m[3]);
+            // items: 2 vectors x nwv words, then 4 row entries x nwm words
+            const long long nvi = 2 * nwv, nitems = nvi + 4 * nwm;
+            for (long long it = tid; it < nitems; it += BASE_THREADS) {
+                u64 lo0, hi0, lo1, hi1;
+                if (it < nvi) {
+                    const bool v = it >= nwv;
+                    const long long w = v ? it - nwv : it;
+                    mul64x32(VA[w], v ? k2 : k0, lo0, hi0);
+                    mul64x32(VB[w], v ? k3 : k1, lo1, hi1);
+                    (v ? V2b : V2a)[w] = lo0 ^ lo1;
+                    hiv[(v ? W : 0) + w] = hi0 ^ hi1;
+                } else {
+                    const long long j = it - nvi;
+                    const int e = (int)(j / nwm);
+                    const long long w = j - (long long)e * nwm;
+                    const bool row = e >> 1;
+                    const u64 col = (u64)(e & 1) * mw;
+                    mul64x32(RA[col + w], row ? k2 : k0, lo0, hi0);
+                    mul64x32(RB[col + w], row ? k3 : k1, lo1, hi1);
+                    N[(u64)e * mw + w] = lo0 ^ lo1;
+                    hir[(u64)e * mw + w] = hi0 ^ hi1;
+                }
             }
             for (long long w = nwm + tid; w < (long long)mw; w += BASE_THREADS) {
-                Na0[w] = 0; Na1[w] = 0; Nb0[w] = 0; Nb1[w] = 0;
+                N[0 * mw + w] = 0; N[1 * mw + w] = 0; N[2 * mw + w] = 0; N[3 * mw + w] = 0;
+            }
+            for (long long w = nwv + tid; w < (long long)W; w += BASE_THREADS) {
+                V2a[w] = 0; V2b[w] = 0;
             }
             __syncthreads();
-            // carries of word w-1 (the new vectors have degree < the old top)
-            for (long long w = 1 + tid; w < nwv; w += BASE_THREADS) {
-                A2[w] ^= hiv[2 * (w - 1)];
-                B2[w] ^= hiv[2 * (w - 1) + 1];
+            // carries out of word w-1 (the new vectors stay below the old top word)
+            for (long long it = tid; it < nitems; it += BASE_THREADS) {
+                if (it < nvi) {
+                    const bool v = it >= nwv;
+                    const long long w = v ? it - nwv : it;
+                    if (w >= 1) (v ? V2b : V2a)[w] ^= hiv[(v ? W : 0) + w - 1];
+                } else {
+                    const long long j = it - nvi;
+                    const int e = (int)(j / nwm);
+                    const long long w = j - (long long)e * nwm;
+                    if (w >= 1) N[(u64)e * mw + w] ^= hir[(u64)e * mw + w - 1];
+                }
             }
-            for (long long w = 1 + tid; w <= nwm && w < (long long)mw; w += BASE_THREADS) {
-                Na0[w] ^= hir[4 * (w - 1) + 0];
-                Na1[w] ^= hir[4 * (w - 1) + 1];
-                Nb0[w] ^= hir[4 * (w - 1) + 2];
-                Nb1[w] ^= hir[4 * (w - 1) + 3];
-            }
+            // the growth word of the rows takes the carry out of the last live word
+            if (nwm < (long long)mw)
+                for (int e = tid; e < 4; e += BASE_THREADS)
+                    N[(u64)e * mw + nwm] ^= hir[(u64)e * mw + nwm - 1];
             if (tid == 0) s_md = min((long long)mw - 2, s_md + 1);
         }
-        // words of the new vectors above the live range stay as they were
-        // (zero) only if both old buffers were zero there: clear them
-        for (long long w = nwv + tid; w < (long long)W; w += BASE_THREADS) { A2[w] = 0; B2[w] = 0; }
-        __syncthreads();
-        if (tid == 0) {
-            s_va = spare[0]; s_vb = spare[1];
-            s_buf = nb;
-            s_ra = 0;                        // new rows are written in (A, B) order
-        }
+        if (tid == 0) s_buf = nb;
         __syncthreads();
     }
     // matrix out, rows in (A, B) order
-    const int buf = s_buf, ra = s_ra;
+    const int buf = s_buf, fra = s_ra;
     for (u64 w = tid; w < 2 * mw; w += BASE_THREADS) {
-        Mout[w] = R[(u64)(buf * 4 + 2 * ra) * mw + w];
-        Mout[2 * mw + w] = R[(u64)(buf * 4 + 2 * (ra ^ 1)) * mw + w];
+        Mout[w] = R[(u64)(buf * 4 + 2 * fra) * mw + w];
+        Mout[2 * mw + w] = R[(u64)(buf * 4 + 2 * (fra ^ 1)) * mw + w];
     }
     if (tid == 0) {
-        res->deg_a = s_da;
-        res->deg_b = s_db;
-        res->rounds = s_rounds;
+        res->deg_a = da;
+        res->deg_b = db;
+        res->rounds = rounds;
         res->cyc_serial = cyc_serial;
         res->cyc_total = clock64() - cyc0;
-        res->status = s_status;
+        res->status = status;
     }
 }
 
@@ -482,7 +500,7 @@ struct Mat {
 
 struct Tunables {
     long long base_bits = 1 << 14;       // n <= base_bits: one-CTA base kernel
-    long long fft_bits = 1 << 21;        // products above this many bits use the FFT
+    long long fft_bits = 1 << 19;        // products above this many bits use the FFT
     long long small_gcd_bits = 1 << 15;  // finish with the quadratic gcd below this
 };
 
