@@ -5,6 +5,8 @@ capture (inputs larger than L2, a few GB at most, a handful of launches).
     python -m mersenne_trinomial_b200.profile_cases fft [--m M]
     python -m mersenne_trinomial_b200.profile_cases sieve [--r R] [--depth D]
     python -m mersenne_trinomial_b200.profile_cases mul [--m M]
+    python -m mersenne_trinomial_b200.profile_cases gcd|hgcd [--r R]
+    python -m mersenne_trinomial_b200.profile_cases scan [--r R --n N --k K]
 """
 from __future__ import annotations
 
@@ -77,6 +79,29 @@ def case_scan(a):
           lines[:3])
 
 
+def case_hgcd(a):
+    """One half-gcd of a scan-like accumulator against x^r + x^s + 1."""
+    r, s = a.r, 1001
+    T = M.TrinGPU()
+    T.init(r)
+    T.set_s(s)
+    T.set_x()
+    T.reset_acc()
+    for k in range(1, 40):
+        T.square_A()
+        if k > 24:
+            T.accumulate()
+    acc = T.read("ACC")
+    T.fini()
+    tri = np.zeros((r + 1 + 63) // 64, dtype=np.uint64)
+    for e in (0, s, r):
+        tri[e >> 6] |= np.uint64(1 << (e & 63))
+    da, db = M.DeviceBuffer.from_array(acc), M.DeviceBuffer.from_array(tri)
+    t0 = time.perf_counter()
+    degs, _, st = M.gcd_large([(da, r, db, r + 1)])
+    print(f"hgcd: {r} bits in {time.perf_counter() - t0:.3f} s, degree {degs[0]}, {st}")
+
+
 def case_sieve(a):
     smax = a.r // 2
     M.run_sieve(a.r, a.depth, smax)
@@ -84,7 +109,7 @@ def case_sieve(a):
 
 def main(argv=None):
     ap = argparse.ArgumentParser()
-    ap.add_argument("case", choices=["square", "fft", "mul", "sieve", "gcd", "scan"])
+    ap.add_argument("case", choices=["square", "fft", "mul", "sieve", "gcd", "hgcd", "scan"])
     ap.add_argument("--r", type=int, default=136279841)
     ap.add_argument("--n", type=int, default=8)
     ap.add_argument("--k", type=int, default=3)
@@ -93,7 +118,7 @@ def main(argv=None):
     a = ap.parse_args(argv)
     t0 = time.perf_counter()
     {"square": case_square, "fft": case_fft, "mul": case_mul, "sieve": case_sieve,
-     "gcd": case_gcd, "scan": case_scan}[a.case](a)
+     "gcd": case_gcd, "hgcd": case_hgcd, "scan": case_scan}[a.case](a)
     print(f"{a.case}: done in {time.perf_counter() - t0:.3f} s")
     return 0
 
