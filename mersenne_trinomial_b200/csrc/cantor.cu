@@ -65,8 +65,12 @@ GF2E_DEV u32 sidx(u32 row, u32 col, u32 c_log) { return (srow(row) << c_log) + c
 // q*2^(K-1) .. q (q = 2^lg rows): each thread holds the 2^(K+1) rows
 // row0 + j*q of one column, with row0 = blk * q * 2^(K+1) + i, i < q.
 // Forward goes from the largest blocks down, inverse the other way.
+//
+// Shared-memory indices: row0 has no bits in [lg, lg+K+1) and the swizzle is
+// linear over XOR, so the index of row row0 + j*q is the group's base index
+// XOR off[j] = srow(j << lg) << c_log, a per-stage table built once per CTA.
 template <bool FWD, int K>
-GF2E_DEV void taylor_stage(u64 *sm, u32 lg, u32 c_log, u32 tile_elems) {
+GF2E_DEV void taylor_stage(u64 *sm, const u32 *off, u32 lg, u32 c_log, u32 tile_elems) {
     constexpr int R = 2 << K;                       // rows per thread
     const u32 C = 1u << c_log, q = 1u << lg;
     const u32 ngroups = tile_elems / R;
@@ -74,9 +78,10 @@ GF2E_DEV void taylor_stage(u64 *sm, u32 lg, u32 c_log, u32 tile_elems) {
         const u32 col = g & (C - 1), rest = g >> c_log;
         const u32 i = rest & (q - 1), blk = rest >> lg;
         const u32 row0 = (blk << (lg + K + 1)) + i;
+        const u32 b0 = (srow(row0) << c_log) | col;
         u64 v[R];
 #pragma unroll
-        for (int j = 0; j < R; j++) v[j] = sm[sidx(row0 + j * q, col, c_log)];
+        for (int j = 0; j < R; j++) v[j] = sm[b0 ^ off[j]];
         if (FWD) {
 #pragma unroll
             for (int lev = K - 1; lev >= 0; lev--) {
@@ -103,7 +108,7 @@ GF2E_DEV void taylor_stage(u64 *sm, u32 lg, u32 c_log, u32 tile_elems) {
             }
         }
 #pragma unroll
-        for (int j = 0; j < R; j++) sm[sidx(row0 + j * q, col, c_log)] = v[j];
+        for (int j = 0; j < R; j++) sm[b0 ^ off[j]] = v[j];
     }
 }
 
@@ -115,8 +120,8 @@ GF2E_DEV void taylor_stage(u64 *sm, u32 lg, u32 c_log, u32 tile_elems) {
 // W[Q0 >> (lev+1)] ^ W[j >> (lev+1)], the second term from the first byte
 // table (j < 8).
 template <bool FWD, int K>
-GF2E_DEV void bfly_stage(u64 *sm, const u64 *__restrict__ tab, u32 lg, u32 Llo, u32 c_log,
-                         u32 tile_elems, u64 base) {
+GF2E_DEV void bfly_stage(u64 *sm, const u32 *off, const u64 *__restrict__ tab, u32 lg, u32 Llo,
+                         u32 c_log, u32 tile_elems, u64 base) {
     constexpr int R = 1 << K;
     const u32 C = 1u << c_log, D = 1u << lg;
     const u32 ngroups = tile_elems / R;
@@ -124,10 +129,11 @@ GF2E_DEV void bfly_stage(u64 *sm, const u64 *__restrict__ tab, u32 lg, u32 Llo, 
         const u32 col = g & (C - 1), rest = g >> c_log;
         const u32 i = rest & (D - 1), blk = rest >> lg;
         const u32 row0 = (blk << (lg + K)) + i;
+        const u32 b0 = (srow(row0) << c_log) | col;
         const u64 Q0 = (base >> Llo) + ((u64)blk << K);
         u64 v[R];
 #pragma unroll
-        for (int j = 0; j < R; j++) v[j] = sm[sidx(row0 + j * D, col, c_log)];
+        for (int j = 0; j < R; j++) v[j] = sm[b0 ^ off[j]];
 #pragma unroll
         for (int step = 0; step < K; step++) {
             const int lev = FWD ? K - 1 - step : step;
@@ -149,7 +155,7 @@ GF2E_DEV void bfly_stage(u64 *sm, const u64 *__restrict__ tab, u32 lg, u32 Llo, 
             }
         }
 #pragma unroll
-        for (int j = 0; j < R; j++) sm[sidx(row0 + j * D, col, c_log)] = v[j];
+        for (int j = 0; j < R; j++) sm[b0 ^ off[j]] = v[j];
     }
 }
 
@@ -170,6 +176,8 @@ __global__ void __launch_bounds__(FFT_THREADS, 2)
 k_fft_pass(u64 *__restrict__ f, const u64 *__restrict__ tab, const Pass P, u64 ntiles,
            const u32 *__restrict__ src32, u64 nchunks, const Batch bt) {
     extern __shared__ u64 sm[];
+    __shared__ u32 s_off[MAXOPS * 16];               // per stage: srow(j << lg) << c_log
+    __shared__ u32 s_loff[16];                       // load/store rows: srow(j << rs) << c_log
     f += (u64)blockIdx.y * bt.fstride;
     if (src32) src32 += (u64)blockIdx.y * bt.sstride32;
     const u32 C = 1u << P.c_log;
@@ -177,6 +185,23 @@ k_fft_pass(u64 *__restrict__ f, const u64 *__restrict__ tab, const Pass P, u64 n
     const u32 rows_total = NS << P.wpt_log;          // rows in the tile (all windows)
     const u32 tile_elems = rows_total * C;
     const u64 cgroups = P.CH >> P.c_log;             // column groups per window
+    // element e = tid + j*FFT_THREADS of the tile is (row_t + j << rs, col_t)
+    // when a row holds at most FFT_THREADS columns; its swizzled index is the
+    // thread's base index XOR s_loff[j] (rows and the swizzle are linear)
+    constexpr u32 THREADS_LOG = 9;
+    static_assert((1 << THREADS_LOG) == FFT_THREADS, "thread count");
+    const bool fast = P.c_log <= THREADS_LOG;
+    const u32 rs = fast ? THREADS_LOG - P.c_log : 0;
+    const u32 row_t = threadIdx.x >> P.c_log, col_t = threadIdx.x & (C - 1);
+    const u32 sb_t = (srow(row_t) << P.c_log) | col_t;
+    for (u32 t = threadIdx.x; t < P.nops * 16; t += FFT_THREADS) {
+        const u32 lg = (P.ops[t >> 4] >> 2) & 63;
+        s_off[t] = srow((t & 15) << lg) << P.c_log;
+    }
+    if (threadIdx.x < 16) s_loff[threadIdx.x] = srow(threadIdx.x << rs) << P.c_log;
+    __syncthreads();
+    constexpr int EPT = (1 << TL) / FFT_THREADS;
+    constexpr int BATCH = EPT < 8 ? EPT : 8;
 
     for (u64 tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
         u64 base;
@@ -186,19 +211,19 @@ k_fft_pass(u64 *__restrict__ f, const u64 *__restrict__ tab, const Pass P, u64 n
             u64 win = tile / cgroups, cg = tile - win * cgroups;
             base = win * ((u64)NS * P.CH) + cg * C;
         }
+        const u64 g_t = base + (u64)row_t * P.CH + col_t;       // fast path: element j = 0
+        const u64 g_step = P.CH << rs;
         // load: every thread issues a batch of loads before the first use
-        constexpr int EPT = (1 << TL) / FFT_THREADS;
-        constexpr int BATCH = EPT < 8 ? EPT : 8;
 #pragma unroll
         for (int j0 = 0; j0 < EPT; j0 += BATCH) {
             u64 v[BATCH];
 #pragma unroll
             for (int j = 0; j < BATCH; j++) {
-                u32 e = threadIdx.x + (j0 + j) * FFT_THREADS;
+                const u32 e = threadIdx.x + (j0 + j) * FFT_THREADS;
                 v[j] = 0;
                 if (e < tile_elems) {
-                    u32 row = e >> P.c_log, col = e & (C - 1);
-                    u64 g = base + (u64)row * P.CH + col;
+                    const u64 g = fast ? g_t + (u64)(j0 + j) * g_step
+                                       : base + (u64)(e >> P.c_log) * P.CH + (e & (C - 1));
                     if (src32) {
                         v[j] = (g < nchunks) ? (u64)__ldg(src32 + g) : 0ull;
                         if (g == 0) v[j] ^= bt.xor0;
@@ -209,8 +234,9 @@ k_fft_pass(u64 *__restrict__ f, const u64 *__restrict__ tab, const Pass P, u64 n
             }
 #pragma unroll
             for (int j = 0; j < BATCH; j++) {
-                u32 e = threadIdx.x + (j0 + j) * FFT_THREADS;
-                if (e < tile_elems) sm[sidx(e >> P.c_log, e & (C - 1), P.c_log)] = v[j];
+                const u32 e = threadIdx.x + (j0 + j) * FFT_THREADS;
+                if (e < tile_elems)
+                    sm[fast ? (sb_t ^ s_loff[j0 + j]) : sidx(e >> P.c_log, e & (C - 1), P.c_log)] = v[j];
             }
         }
         __syncthreads();
@@ -218,24 +244,33 @@ k_fft_pass(u64 *__restrict__ f, const u64 *__restrict__ tab, const Pass P, u64 n
             const u32 op = P.ops[k];
             const u32 type = op & 3, lg = (op >> 2) & 63, L = (op >> 8) & 127;
             const u32 K = ((op >> 15) & 3) + 1;
+            const u32 *off = s_off + k * 16;
             switch (type * 4 + K) {
-            case TAY_F * 4 + 1: taylor_stage<true, 1>(sm, lg, P.c_log, tile_elems); break;
-            case TAY_F * 4 + 2: taylor_stage<true, 2>(sm, lg, P.c_log, tile_elems); break;
-            case TAY_F * 4 + 3: taylor_stage<true, 3>(sm, lg, P.c_log, tile_elems); break;
-            case TAY_I * 4 + 1: taylor_stage<false, 1>(sm, lg, P.c_log, tile_elems); break;
-            case TAY_I * 4 + 2: taylor_stage<false, 2>(sm, lg, P.c_log, tile_elems); break;
-            case TAY_I * 4 + 3: taylor_stage<false, 3>(sm, lg, P.c_log, tile_elems); break;
-            case BF_F * 4 + 1: bfly_stage<true, 1>(sm, tab, lg, L, P.c_log, tile_elems, base); break;
-            case BF_F * 4 + 2: bfly_stage<true, 2>(sm, tab, lg, L, P.c_log, tile_elems, base); break;
-            case BF_I * 4 + 1: bfly_stage<false, 1>(sm, tab, lg, L, P.c_log, tile_elems, base); break;
-            case BF_I * 4 + 2: bfly_stage<false, 2>(sm, tab, lg, L, P.c_log, tile_elems, base); break;
+            case TAY_F * 4 + 1: taylor_stage<true, 1>(sm, off, lg, P.c_log, tile_elems); break;
+            case TAY_F * 4 + 2: taylor_stage<true, 2>(sm, off, lg, P.c_log, tile_elems); break;
+            case TAY_F * 4 + 3: taylor_stage<true, 3>(sm, off, lg, P.c_log, tile_elems); break;
+            case TAY_I * 4 + 1: taylor_stage<false, 1>(sm, off, lg, P.c_log, tile_elems); break;
+            case TAY_I * 4 + 2: taylor_stage<false, 2>(sm, off, lg, P.c_log, tile_elems); break;
+            case TAY_I * 4 + 3: taylor_stage<false, 3>(sm, off, lg, P.c_log, tile_elems); break;
+            case BF_F * 4 + 1: bfly_stage<true, 1>(sm, off, tab, lg, L, P.c_log, tile_elems, base); break;
+            case BF_F * 4 + 2: bfly_stage<true, 2>(sm, off, tab, lg, L, P.c_log, tile_elems, base); break;
+            case BF_I * 4 + 1: bfly_stage<false, 1>(sm, off, tab, lg, L, P.c_log, tile_elems, base); break;
+            case BF_I * 4 + 2: bfly_stage<false, 2>(sm, off, tab, lg, L, P.c_log, tile_elems, base); break;
             default: break;                    // butterfly stages hold at most 2 levels
             }
             __syncthreads();
         }
-        for (u32 e = threadIdx.x; e < tile_elems; e += FFT_THREADS) {
-            u32 row = e >> P.c_log, col = e & (C - 1);
-            f[base + (u64)row * P.CH + col] = sm[sidx(row, col, P.c_log)];
+        if (fast) {
+#pragma unroll
+            for (int j = 0; j < EPT; j++) {
+                const u32 e = threadIdx.x + j * FFT_THREADS;
+                if (e < tile_elems) f[g_t + (u64)j * g_step] = sm[sb_t ^ s_loff[j]];
+            }
+        } else {
+            for (u32 e = threadIdx.x; e < tile_elems; e += FFT_THREADS) {
+                u32 row = e >> P.c_log, col = e & (C - 1);
+                f[base + (u64)row * P.CH + col] = sm[sidx(row, col, P.c_log)];
+            }
         }
         __syncthreads();
     }

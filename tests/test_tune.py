@@ -22,7 +22,7 @@ def model_cost(k0, maxd, t_deg, t_gcd, L0, Lmax):
 def test_tune_defaults_and_validation(engine):
     from mersenne_trinomial_b200 import autotune as A
     d = A.tune_default()
-    assert d == {"fft_tile_log": 12, "fft_cmin": 4, "fft_taylor_lv": 3, "fft_bfly_lv": 2,
+    assert d == {"fft_tile_log": 13, "fft_cmin": 8, "fft_taylor_lv": 3, "fft_bfly_lv": 2,
                  "sieve_strip_log": 12}
     saved = A.tune_get()
     try:
@@ -55,7 +55,7 @@ def test_tune_environment_overrides(engine):
                              "GF2E_SIEVE_STRIP_LOG": "13"})
     assert got["fft_tile_log"] == 11 and got["fft_bfly_lv"] == 1 and got["sieve_strip_log"] == 13
     got, err = _tune_in_child({"GF2E_FFT_TILE_LOG": "99"})
-    assert got["fft_tile_log"] == 12 and "ignoring" in err
+    assert got["fft_tile_log"] == 13 and "ignoring" in err
 
 
 @pytest.mark.parametrize("k0,maxd,t_deg,t_gcd", [
