@@ -249,6 +249,18 @@ int gf2e_scan(uint64_t r, const uint64_t *s_host, int ns, uint64_t k0, uint64_t 
               uint64_t L0, uint64_t Lmax, int batch, gf2e_scan_result *results_host,
               uint64_t *masks_host, size_t mask_cap_words, void *stream);
 
+/* gf2e_scan with the multi-level blocking DDF of the reference's tsfactor
+ * (tsfactor.cu:1-27, k_horner_fused/k_mulx_xor 71-126, do_block 999-1019):
+ * block = m even in 2..62 degrees per step (1 = gf2e_scan): per s the m
+ * elementary symmetric functions of the block's Frobenius iterates stay on
+ * the device, each block costs one Horner pass, one modmul and m*m
+ * squarings.  Intervals are rounded up to whole blocks; results are those
+ * of gf2e_scan (a factor found past maxd in the last block reports "u"). */
+int gf2e_scan_blocked(uint64_t r, const uint64_t *s_host, int ns, uint64_t k0, uint64_t maxd,
+                      uint64_t L0, uint64_t Lmax, int batch, int block,
+                      gf2e_scan_result *results_host, uint64_t *masks_host,
+                      size_t mask_cap_words, void *stream);
+
 /* The steppable engine behind gf2e_scan, for callers that interleave work
  * (the serving loop): one scanner per r keeps `slots` s values resident on
  * the device; submitted s wait in a queue and enter freed slots; each step
@@ -259,6 +271,10 @@ int gf2e_scan(uint64_t r, const uint64_t *s_host, int ns, uint64_t k0, uint64_t 
 typedef struct gf2e_scanner gf2e_scanner;
 int gf2e_scanner_footprint(uint64_t r, int slots, size_t *device_bytes);
 int gf2e_scanner_create(uint64_t r, int slots, gf2e_scanner **scanner);
+/* Blocked-DDF scanner (see gf2e_scan_blocked); step(degrees) advances
+ * ceil(degrees / block) blocks.  block = 1 is gf2e_scanner_create. */
+int gf2e_scanner_footprint_blocked(uint64_t r, int slots, int block, size_t *device_bytes);
+int gf2e_scanner_create_blocked(uint64_t r, int slots, int block, gf2e_scanner **scanner);
 int gf2e_scanner_destroy(gf2e_scanner *scanner);
 int gf2e_scanner_submit(gf2e_scanner *scanner, const uint64_t *s_host, int ns, uint64_t k0,
                         uint64_t maxd, uint64_t L0, uint64_t Lmax, uint64_t tag0);

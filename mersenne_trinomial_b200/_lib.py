@@ -120,6 +120,10 @@ SIGNATURES = {
     "gf2e_server_release": (_i32, [_vp, _u64]),
     "gf2e_scanner_footprint": (_i32, [_u64, _i32, _P(_sz)]),
     "gf2e_scanner_create": (_i32, [_u64, _i32, _P(_vp)]),
+    "gf2e_scanner_footprint_blocked": (_i32, [_u64, _i32, _i32, _P(_sz)]),
+    "gf2e_scanner_create_blocked": (_i32, [_u64, _i32, _i32, _P(_vp)]),
+    "gf2e_scan_blocked": (_i32, [_u64, _vp, _i32, _u64, _u64, _u64, _u64, _i32, _i32,
+                                 _P(ScanResult), _vp, _sz, _vp]),
     "gf2e_scanner_destroy": (_i32, [_vp]),
     "gf2e_scanner_submit": (_i32, [_vp, _vp, _i32, _u64, _u64, _u64, _u64, _u64]),
     "gf2e_scanner_step": (_i32, [_vp, _i32, _vp]),

@@ -11,6 +11,21 @@
 // host, retires finished s and refills their slots from the queue (or
 // compacts the slots when the queue is empty).  Per-s state stays on the
 // device between steps, so different jobs' s values share every launch.
+//
+// Blocked mode (block size m > 1) is the multi-level blocking DDF of the
+// reference's tsfactor (tsfactor.cu:1-27, 71-126, 296-365; after gf2x
+// factor.cpp): per s it keeps h[j] = e_{j+1}(y_0..y_{m-1}), the elementary
+// symmetric functions of the Frobenius iterates y_t = x^(2^(i+t)) mod T of
+// the current block of degrees [i, i+m-1].  Then
+//   C = x^m + h[0] x^(m-1) + ... + h[m-1] = prod_t (x + x^(2^(i+t)))  (mod T)
+// is one shift-XOR pass (Horner at x), ACC *= C is one modmul per block, and
+// h[j] <- h[j]^(2^m) advances the block (Frobenius commutes with e_k): per
+// degree m squarings and 1/m modmul instead of one modmul.  ACC after q
+// blocks is the same residue as after q*m single degrees, so the gcds and
+// results are the per-degree scanner's.  Initial h for the block at degree 0
+// follows E_j(X) = (X + x) E_{j-1}^(2)(X) with E_j = prod_{t<j} (X + x^(2^t))
+// (squarings and multiplications by x only); it is then advanced by k0 + 1
+// Frobenius steps.
 #include "gf2e_internal.cuh"
 
 #include <algorithm>
@@ -67,6 +82,11 @@ struct gf2e_scanner {
     std::vector<std::pair<GraphKey, cudaGraphExec_t>> graphs;
     bool use_graphs = true;
     int gcd_parallel = 16;        // concurrent half-gcds at interval ends (large r)
+    // blocked mode: m residues h per slot (slot j's at H + (j*m + t)*stride),
+    // their squaring scratch, the block product C per slot, s per h state
+    int m = 1;
+    u64 *H = nullptr, *HS = nullptr, *C = nullptr, *sH = nullptr;
+    std::vector<u64> shH;
 };
 
 // operands of at least this many bits take the half-gcd (hgcd.cu) at
@@ -97,8 +117,86 @@ Geometry geometry(u64 r) {
     return g;
 }
 
-size_t device_words(const Geometry &g, int B) {
-    return 3 * g.stride * B + 2 * g.n * B + g.pstride * B + g.tw * B + B + g.gcap * B;
+size_t device_words(const Geometry &g, int B, int m = 1) {
+    size_t w = 3 * g.stride * B + 2 * g.n * B + g.pstride * B + g.tw * B + B + g.gcap * B;
+    if (m > 1) w += 2 * (size_t)m * g.stride * B + g.stride * B + (size_t)m * B;
+    return w;
+}
+
+// word w of x * v mod x^r + x^s + 1 (v a residue, bits >= r zero)
+__device__ __forceinline__ u64 mulx_word(const u64 *v, u64 r, u64 s, u64 w) {
+    const u64 a = v[w], b = w ? v[w - 1] : 0;
+    u64 out = (a << 1) | (b >> 63);
+    const u64 wrap = (v[(r - 1) >> 6] >> ((r - 1) & 63)) & 1;      // coefficient of x^(r-1)
+    if (w == (r >> 6)) out &= ~(1ull << (r & 63));                  // x^r -> x^s + 1
+    if (w == 0) out ^= wrap;
+    if (w == (s >> 6)) out ^= wrap << (s & 63);
+    return out;
+}
+
+// one step of E_j = (X + x) E_{j-1}^(2): h[t] <- S[t] + x S[t-1] (+ x at
+// t = 0) for t < j, where S[t] = h[t]^2 (S[j-1] = 0); state t = blockIdx.y
+__global__ void k_esym_step(u64 *__restrict__ Hs, const u64 *__restrict__ Sq, size_t stride,
+                            int j, u64 nw, u64 r, u64 s) {
+    const int t = blockIdx.y;
+    u64 *out = Hs + (size_t)t * stride;
+    const u64 *cur = Sq + (size_t)t * stride, *prev = Sq + (size_t)(t - 1) * stride;
+    for (u64 w = (u64)blockIdx.x * blockDim.x + threadIdx.x; w < nw;
+         w += (u64)gridDim.x * blockDim.x) {
+        u64 v = (t < j - 1) ? cur[w] : 0;
+        if (t >= 1) v ^= mulx_word(prev, r, s, w);
+        if (t == 0 && w == 0) v ^= 2;
+        out[w] = v;
+    }
+}
+
+// C = x^m + sum_t h[t] x^(m-1-t), bits >= r dropped here (folded by
+// k_horner_fold); slot = blockIdx.y
+__global__ void k_horner(const u64 *__restrict__ H, size_t stride, int m, u64 *__restrict__ C,
+                         u64 nw, u64 r) {
+    const int y = blockIdx.y;
+    const u64 *h0 = H + (size_t)y * m * stride;
+    u64 *c = C + (size_t)y * stride;
+    const u64 topmask = (r & 63) ? ((1ull << (r & 63)) - 1) : ~0ull;
+    for (u64 w = (u64)blockIdx.x * blockDim.x + threadIdx.x; w < nw;
+         w += (u64)gridDim.x * blockDim.x) {
+        u64 acc = 0;
+        for (int t = 0; t < m; t++) {
+            const u64 *h = h0 + (size_t)t * stride;
+            const unsigned sh = (unsigned)(m - 1 - t);
+            const u64 a = h[w], b = w ? h[w - 1] : 0;
+            acc ^= sh ? ((a << sh) | (b >> (64 - sh))) : a;
+        }
+        if (w == nw - 1) acc &= topmask;
+        if (w == ((u64)m >> 6)) acc ^= 1ull << (m & 63);
+        c[w] = acc;
+    }
+}
+
+// the bits of sum_t h[t] x^(m-1-t) at x^(r+e), e <= m-2, folded as
+// x^(r+e) = x^(s+e) + x^e (one thread per slot)
+__global__ void k_horner_fold(const u64 *__restrict__ H, size_t stride, int m, u64 *C, u64 r,
+                              const u64 *__restrict__ s_dev) {
+    const int y = blockIdx.x;
+    if (threadIdx.x != 0) return;
+    const u64 *h0 = H + (size_t)y * m * stride;
+    u64 *c = C + (size_t)y * stride;
+    const u64 s = s_dev[y];
+    u64 O = 0;                                   // bit e = coefficient of x^(r+e)
+    for (int t = 0; t < m - 1; t++) {
+        const unsigned sh = (unsigned)(m - 1 - t);     // h[t] bits [r-sh, r) move to [r, r+sh)
+        const u64 p = r - sh, i = p >> 6;
+        const unsigned b = (unsigned)(p & 63);
+        u64 win = h0[(size_t)t * stride + i] >> b;
+        if (b && ((r - 1) >> 6) > i) win |= h0[(size_t)t * stride + i + 1] << (64 - b);
+        O ^= win & ((1ull << sh) - 1);
+    }
+    if (!O) return;
+    c[0] ^= O;
+    const u64 sw = s >> 6;
+    const unsigned sb = (unsigned)(s & 63);
+    c[sw] ^= O << sb;
+    if (sb) c[sw + 1] ^= O >> (64 - sb);
 }
 
 int load_slot(gf2e_scanner &S, int j, const gf2e_scanner::Job &job, cudaStream_t st) {
@@ -113,8 +211,37 @@ int load_slot(gf2e_scanner &S, int j, const gf2e_scanner::Job &job, cudaStream_t
         e = cudaMemcpyAsync(S.sdev + j, &S.shost[j], 8, cudaMemcpyHostToDevice, st);
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);      // host staging reused
     if (e != cudaSuccess) return gf2e::cuda_status(e, "scanner slot load");
-    GF2E_TRY(gf2e::trin_set_const(S.F + S.stride * j, S.stride, 1, S.r, 2, st));
     GF2E_TRY(gf2e::trin_set_const(S.ACC + S.stride * j, S.stride, 1, S.r, 1, st));
+    if (S.m > 1) {
+        // h for the block at degree 0, then k0 + 1 Frobenius steps
+        const int m = S.m;
+        u64 *Hj = S.H + (size_t)j * m * S.stride, *HSj = S.HS + (size_t)j * m * S.stride;
+        const u64 *sHj = S.sH + (size_t)j * m;
+        for (int t = 0; t < m; t++) S.shH[(size_t)j * m + t] = job.s;
+        e = cudaMemcpyAsync(S.sH + (size_t)j * m, S.shH.data() + (size_t)j * m, (size_t)m * 8,
+                            cudaMemcpyHostToDevice, st);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+        if (e != cudaSuccess) return gf2e::cuda_status(e, "scanner block slot load");
+        const int gx = std::max(1, gf2e::grid_for(S.nw, 256) / m);
+        for (int jj = 1; jj <= m; jj++) {
+            if (jj > 1)
+                GF2E_TRY(gf2e::trin_square_states(Hj, HSj, S.stride, jj - 1, S.r, sHj, st));
+            k_esym_step<<<dim3(gx, jj), 256, 0, st>>>(Hj, HSj, S.stride, jj, S.nw, S.r, job.s);
+            GF2E_CHECK_LAUNCH("k_esym_step");
+        }
+        for (u64 k = 0; k <= job.k0; k++) {
+            const bool even = (k & 1) == 0;
+            GF2E_TRY(gf2e::trin_square_states(even ? Hj : HSj, even ? HSj : Hj, S.stride, m, S.r,
+                                              sHj, st));
+        }
+        if ((job.k0 + 1) & 1) {
+            e = cudaMemcpyAsync(Hj, HSj, (size_t)m * S.stride * 8, cudaMemcpyDeviceToDevice, st);
+            if (e != cudaSuccess) return gf2e::cuda_status(e, "scanner block ramp");
+        }
+        S.slot[j] = gf2e_scanner::Slot{job, job.k0, job.k0, job.L0};
+        return GF2E_OK;
+    }
+    GF2E_TRY(gf2e::trin_set_const(S.F + S.stride * j, S.stride, 1, S.r, 2, st));
     for (u64 k = 0; k < job.k0; k++) {
         GF2E_TRY(gf2e::trin_square_states(S.F + S.stride * j, S.Fs + S.stride * j, S.stride, 1,
                                           S.r, S.sdev + j, st));
@@ -138,6 +265,14 @@ int move_slot(gf2e_scanner &S, int to, int from, cudaStream_t st) {
     S.shost[to] = S.shost[from];
     if (e == cudaSuccess)
         e = cudaMemcpyAsync(S.sdev + to, &S.shost[to], 8, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess && S.m > 1) {
+        const size_t mw = (size_t)S.m * S.stride;
+        e = cudaMemcpyAsync(S.H + to * mw, S.H + from * mw, mw * 8, cudaMemcpyDeviceToDevice, st);
+        for (int t = 0; t < S.m; t++) S.shH[(size_t)to * S.m + t] = S.shost[to];
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(S.sH + (size_t)to * S.m, S.shH.data() + (size_t)to * S.m,
+                                (size_t)S.m * 8, cudaMemcpyHostToDevice, st);
+    }
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);
     S.slot[to] = S.slot[from];
     return gf2e::cuda_status(e, "scanner compaction");
@@ -169,16 +304,44 @@ int degree_kernels(gf2e_scanner &S, int na, u64 *F, u64 *Fs, cudaStream_t st) {
     return GF2E_OK;
 }
 
+// the launches of one block of m degrees for `na` resident s: C by Horner,
+// ACC *= C mod T, then every h squared m times (m even: back in H)
+int block_kernels(gf2e_scanner &S, int na, cudaStream_t st) {
+    const int m = S.m;
+    const int gx = std::max(1, gf2e::grid_for(S.nw, 256) / na);
+    k_horner<<<dim3(gx, na), 256, 0, st>>>(S.H, S.stride, m, S.C, S.nw, S.r);
+    GF2E_CHECK_LAUNCH("k_horner");
+    k_horner_fold<<<na, 32, 0, st>>>(S.H, S.stride, m, S.C, S.r, S.sdev);
+    GF2E_CHECK_LAUNCH("k_horner_fold");
+    GF2E_TRY(gf2e::fft_fwd_packed_batch(S.plan, S.FA, S.n, reinterpret_cast<const u32 *>(S.ACC),
+                                        2 * S.stride, S.nchunks, 0, na, st));
+    GF2E_TRY(gf2e::fft_fwd_packed_batch(S.plan, S.FB, S.n, reinterpret_cast<const u32 *>(S.C),
+                                        2 * S.stride, S.nchunks, 0, na, st));
+    GF2E_TRY(gf2e::pointwise(S.FA, S.FB, S.n * na, st));
+    GF2E_TRY(gf2e::fft_run_batch(S.plan, false, S.FA, S.n, na, st));
+    GF2E_TRY(gf2e::overlap_add_batch(S.FA, S.n, 2 * S.nchunks - 1, S.P, S.pstride, S.ow, na, st));
+    GF2E_TRY(gf2e::trin_reduce_batch(S.P, S.pstride, S.ow, 2 * S.r - 1, S.ACC, S.stride, S.r,
+                                     S.sdev, na, st));
+    for (int t = 0; t < m; t++)
+        GF2E_TRY(gf2e::trin_square_states((t & 1) ? S.HS : S.H, (t & 1) ? S.H : S.HS, S.stride,
+                                          na * m, S.r, S.sH, st));
+    return GF2E_OK;
+}
+
+int step_kernels(gf2e_scanner &S, int na, cudaStream_t st) {
+    return S.m > 1 ? block_kernels(S, na, st) : degree_kernels(S, na, S.F, S.Fs, st);
+}
+
 int launch_degree(gf2e_scanner &S, cudaStream_t st) {
     const int na = S.nact;
-    if (!S.use_graphs || st != S.own) return degree_kernels(S, na, S.F, S.Fs, st);
+    if (!S.use_graphs || st != S.own) return step_kernels(S, na, st);
     for (auto &g : S.graphs)
         if (g.first.nact == na && g.first.F == S.F)
             return gf2e::cuda_status(cudaGraphLaunch(g.second, st), "degree graph launch");
     cudaGraph_t graph = nullptr;
     cudaError_t e = cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal);
     if (e != cudaSuccess) return gf2e::cuda_status(e, "degree graph capture");
-    int status = degree_kernels(S, na, S.F, S.Fs, st);
+    int status = step_kernels(S, na, st);
     e = cudaStreamEndCapture(st, &graph);
     if (status != GF2E_OK) { if (graph) cudaGraphDestroy(graph); return status; }
     if (e != cudaSuccess) return gf2e::cuda_status(e, "degree graph end capture");
@@ -198,14 +361,15 @@ int launch_degree(gf2e_scanner &S, cudaStream_t st) {
 int degree_step(gf2e_scanner &S, cudaStream_t st) {
     const int na = S.nact;
     GF2E_TRY(launch_degree(S, st));
-    std::swap(S.F, S.Fs);
-    S.degree_steps++;
-    S.sd_pairs += (u64)na;
+    const u64 adv = (u64)S.m;                    // degrees per step
+    if (S.m == 1) std::swap(S.F, S.Fs);
+    S.degree_steps += adv;
+    S.sd_pairs += (u64)na * adv;
     std::vector<int> due;
     for (int j = 0; j < na; j++) {
         gf2e_scanner::Slot &sl = S.slot[j];
-        sl.k++;
-        if (sl.k - sl.iv >= sl.L || sl.k == sl.job.maxd) due.push_back(j);
+        sl.k += adv;
+        if (sl.k - sl.iv >= sl.L || sl.k >= sl.job.maxd) due.push_back(j);
     }
     if (due.empty()) return GF2E_OK;
     for (size_t q = 0; q < due.size(); q++) {
@@ -224,10 +388,10 @@ int degree_step(gf2e_scanner &S, cudaStream_t st) {
     for (size_t q = 0; q < due.size(); q++) {
         int j = due[q];
         gf2e_scanner::Slot &sl = S.slot[j];
-        if (S.degs[q] > 0 || sl.k == sl.job.maxd) {
+        if (S.degs[q] > 0 || sl.k >= sl.job.maxd) {
             gf2e_scanner::Done D;
             D.tag = sl.job.tag;
-            D.res = gf2e_scan_result{sl.job.s, 2, 0, 0, sl.iv + 1, sl.k};
+            D.res = gf2e_scan_result{sl.job.s, 2, 0, 0, sl.iv + 1, std::min(sl.k, sl.job.maxd)};
             if (S.degs[q] > 0) {
                 D.res.status = 3;
                 if ((size_t)(S.degs[q] / 64 + 1) <= S.gcap) {
@@ -241,6 +405,10 @@ int degree_step(gf2e_scanner &S, cudaStream_t st) {
                         D.res.status = 1;
                         D.res.d = d;
                         D.res.mask_words = D.mask.size();
+                        if (d > sl.job.maxd) {       // a block ran past maxd
+                            D.res = gf2e_scan_result{sl.job.s, 2, 0, 0, sl.iv + 1, sl.job.maxd};
+                            D.mask.clear();
+                        }
                     }
                 }
             }
@@ -271,10 +439,12 @@ int degree_step(gf2e_scanner &S, cudaStream_t st) {
 
 extern "C" {
 
-int gf2e_scanner_footprint(uint64_t r, int slots, size_t *bytes) {
+int gf2e_scanner_footprint_blocked(uint64_t r, int slots, int block, size_t *bytes) {
     if (!bytes || slots < 1 || r < 5) return gf2e::invalid("bad footprint query");
+    if (!(block == 1 || (block >= 2 && block <= 62 && !(block & 1))))
+        return gf2e::invalid("scanner: block size must be 1 or even in 2..62");
     Geometry g = geometry(r);
-    size_t words = device_words(g, slots);
+    size_t words = device_words(g, slots, block);
     // gcd workspace: job table + 4 buffers per job (quadratic gcd), or the
     // pools of the concurrent half-gcds
     size_t gw = ((size_t)slots * 96 + 255) + (size_t)slots * 4 * (g.tw + 1) * 8;
@@ -287,18 +457,26 @@ int gf2e_scanner_footprint(uint64_t r, int slots, size_t *bytes) {
     return GF2E_OK;
 }
 
-int gf2e_scanner_create(uint64_t r, int slots, gf2e_scanner **out) {
+int gf2e_scanner_footprint(uint64_t r, int slots, size_t *bytes) {
+    return gf2e_scanner_footprint_blocked(r, slots, 1, bytes);
+}
+
+int gf2e_scanner_create_blocked(uint64_t r, int slots, int block, gf2e_scanner **out) {
     if (!out || slots < 1 || slots > 4096) return gf2e::invalid("scanner: 1 <= slots <= 4096");
     if (r < 5 || !(r & 1) || r >= (1ull << 31)) return gf2e::invalid("scanner: bad r");
+    if (!(block == 1 || (block >= 2 && block <= 62 && !(block & 1))))
+        return gf2e::invalid("scanner: block size must be 1 or even in 2..62");
+    if ((u64)block >= r) return gf2e::invalid("scanner: block size must be below r");
     Geometry g = geometry(r);
     gf2e_scanner *S = new gf2e_scanner;
     S->r = r;
     S->B = slots;
+    S->m = block;
     S->nw = g.nw; S->stride = g.stride; S->tw = g.tw; S->ow = g.ow; S->pstride = g.pstride;
     S->gcap = g.gcap; S->n = g.n; S->nchunks = g.nchunks;
     S->plan = gf2e::cached_plan(g.m);
     if (!S->plan) { delete S; return gf2e::invalid("FFT plan m=%d", g.m); }
-    S->dmem_bytes = device_words(g, slots) * 8;
+    S->dmem_bytes = device_words(g, slots, block) * 8;
     cudaError_t e = cudaMalloc(&S->dmem, S->dmem_bytes);
     if (e != cudaSuccess) { delete S; return gf2e::cuda_status(e, "scanner buffers"); }
     const int B = slots;
@@ -311,6 +489,13 @@ int gf2e_scanner_create(uint64_t r, int slots, gf2e_scanner **out) {
     S->T = S->P + g.pstride * B;
     S->sdev = S->T + g.tw * B;
     S->G = S->sdev + B;
+    if (block > 1) {
+        S->H = S->G + g.gcap * B;
+        S->HS = S->H + (size_t)block * g.stride * B;
+        S->C = S->HS + (size_t)block * g.stride * B;
+        S->sH = S->C + g.stride * B;
+        S->shH.assign((size_t)block * B, 0);
+    }
     std::vector<gf2e_gcd_job> tmp(B, gf2e_gcd_job{S->ACC, r, S->T, r + 1, S->G, g.gcap});
     int st = GF2E_OK;
     if (r < GCD_LARGE_BITS) st = gf2e_gcd_workspace_size(tmp.data(), B, &S->gws_bytes);
@@ -342,6 +527,10 @@ int gf2e_scanner_create(uint64_t r, int slots, gf2e_scanner **out) {
     return GF2E_OK;
 }
 
+int gf2e_scanner_create(uint64_t r, int slots, gf2e_scanner **out) {
+    return gf2e_scanner_create_blocked(r, slots, 1, out);
+}
+
 int gf2e_scanner_destroy(gf2e_scanner *S) {
     if (!S) return GF2E_OK;
     if (S->own) cudaStreamSynchronize(S->own);
@@ -366,6 +555,10 @@ int gf2e_scanner_submit(gf2e_scanner *S, const uint64_t *s_host, int ns, uint64_
     if (Lmax < 1) Lmax = 1;
     if (L0 < 1) L0 = 1;
     if (L0 > Lmax) L0 = Lmax;
+    // blocked mode: intervals are whole blocks
+    const u64 bm = (u64)S->m;
+    L0 = (L0 + bm - 1) / bm * bm;
+    Lmax = (Lmax + bm - 1) / bm * bm;
     for (int i = 0; i < ns; i++)
         S->queue.push_back(gf2e_scanner::Job{s_host[i], k0, maxd, L0, Lmax, tag0 + (u64)i});
     return GF2E_OK;
@@ -380,7 +573,8 @@ int gf2e_scanner_step(gf2e_scanner *S, int degrees, void *stream) {
     if (e == cudaSuccess) e = cudaStreamWaitEvent(S->own, S->ev_in, 0);
     if (e != cudaSuccess) return gf2e::cuda_status(e, "scanner stream order");
     int st = fill_slots(*S, S->own);
-    for (int i = 0; st == GF2E_OK && i < degrees && S->nact > 0; i++) st = degree_step(*S, S->own);
+    const int steps = (degrees + S->m - 1) / S->m;               // blocks in blocked mode
+    for (int i = 0; st == GF2E_OK && i < steps && S->nact > 0; i++) st = degree_step(*S, S->own);
     e = cudaEventRecord(S->ev_out, S->own);
     if (e == cudaSuccess) e = cudaStreamWaitEvent(caller, S->ev_out, 0);
     if (st != GF2E_OK) return st;
@@ -423,10 +617,17 @@ int gf2e_scanner_poll(gf2e_scanner *S, gf2e_scan_result *res, uint64_t *tags,
 int gf2e_scan(uint64_t r, const uint64_t *s_host, int ns, uint64_t k0, uint64_t maxd,
               uint64_t L0, uint64_t Lmax, int batch, gf2e_scan_result *res,
               uint64_t *masks_host, size_t mask_cap_words, void *stream) {
+    return gf2e_scan_blocked(r, s_host, ns, k0, maxd, L0, Lmax, batch, 1, res, masks_host,
+                             mask_cap_words, stream);
+}
+
+int gf2e_scan_blocked(uint64_t r, const uint64_t *s_host, int ns, uint64_t k0, uint64_t maxd,
+                      uint64_t L0, uint64_t Lmax, int batch, int block, gf2e_scan_result *res,
+                      uint64_t *masks_host, size_t mask_cap_words, void *stream) {
     if (!s_host || !res || ns < 1 || batch < 1)
         return gf2e::invalid("gf2e_scan: ns >= 1 and batch >= 1 required");
     gf2e_scanner *S = nullptr;
-    GF2E_TRY(gf2e_scanner_create(r, std::min(batch, ns), &S));
+    GF2E_TRY(gf2e_scanner_create_blocked(r, std::min(batch, ns), block, &S));
     int st = gf2e_scanner_submit(S, s_host, ns, k0, maxd, L0, Lmax, 0);
     std::vector<gf2e_scan_result> tmp(ns);
     std::vector<u64> tags(ns), masks((size_t)ns * mask_cap_words);

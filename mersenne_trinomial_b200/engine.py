@@ -350,16 +350,17 @@ def _hex(words) -> str:
 
 
 def scan(r: int, survivors, k0: int, maxd: int, L0: int = 64, Lmax: int = 4096,
-         batch: int = 64, mask_cap_words: int = 1024, stream=None) -> list:
+         batch: int = 64, mask_cap_words: int = 1024, stream=None, block: int = 1) -> list:
     """Deep scan (trinomial_scan.cu): one result line per s in the reference's
-    format, 's d p<hex>', 's u' or 's rA-B'."""
+    format, 's d p<hex>', 's u' or 's rA-B'.  block = m > 1 runs tsfactor's
+    blocked DDF (m degrees per step: one modmul and m*m squarings)."""
     from ._lib import ScanResult
     s = np.ascontiguousarray(np.asarray(survivors, dtype=np.uint64))
     n = s.size
     res = (ScanResult * n)()
     masks = np.zeros((n, mask_cap_words), dtype=np.uint64)
-    call("gf2e_scan", r, s.ctypes.data, n, k0, maxd, L0, Lmax, batch, res, masks.ctypes.data,
-         mask_cap_words, _sp(stream))
+    call("gf2e_scan_blocked", r, s.ctypes.data, n, k0, maxd, L0, Lmax, batch, block, res,
+         masks.ctypes.data, mask_cap_words, _sp(stream))
     out = []
     for i in range(n):
         R = res[i]

@@ -75,3 +75,29 @@ def test_scan_r136279841_known_answer(engine, oracle):
     got = engine.scan(136279841, [474], 24, 200, L0=64, Lmax=4096, batch=1)
     assert got == ["474 41 p3991ef16129"]
     assert oracle.factor_divides(136279841, 474, 41, "3991ef16129") == 1
+
+
+@pytest.mark.parametrize("block,L0,batch", [(2, 32, 128), (8, 8, 16), (16, 64, 7), (62, 64, 33)])
+def test_blocked_scan_matches_per_degree_scan(engine, block, L0, batch):
+    """tsfactor's blocked DDF (m degrees per step) gives the per-degree
+    scanner's result for every survivor of the reference selftest at r = 4423
+    (whose lines the per-degree scan reproduces exactly)."""
+    fx = load_json("scan.json")
+    r, k0, maxd = fx["r"], fx["k0"], fx["maxd"]
+    want = engine.scan(r, fx["survivors"], k0, maxd, L0=32, Lmax=4096, batch=128)
+    got = engine.scan(r, fx["survivors"], k0, maxd, L0=L0, Lmax=4096, batch=batch, block=block)
+    assert got == want
+
+
+def test_blocked_scan_rejects_bad_block(engine):
+    for m in (3, 0, 64, -2):
+        with pytest.raises(engine.Gf2eError):
+            engine.scan(4423, [3], 5, 200, block=m)
+
+
+@pytest.mark.timeout(900)
+def test_blocked_scan_r136279841_known_answer(engine):
+    """The blocked DDF at full size: `474 41 p3991ef16129` (blocks of 32
+    degrees from k0 = 24, one gcd after two blocks)."""
+    got = engine.scan(136279841, [474], 24, 200, L0=64, Lmax=4096, batch=1, block=32)
+    assert got == ["474 41 p3991ef16129"]
