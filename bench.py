@@ -306,7 +306,7 @@ def main():
 
     extras = {}
     if rank == 0 and not args.no_extras:
-        extras = run_extras(torch, M, W)
+        extras = run_extras(torch, M, W, sq_rate=value / world)
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         ksq = 12
@@ -358,7 +358,7 @@ def _ev_time(torch, fn, reps=3, flush=None):
     return statistics.median(ts)
 
 
-def run_extras(torch, M, W):
+def run_extras(torch, M, W, sq_rate=None):
     """The other hot-path legs named by the metric / configurations."""
     out = {}
     flush_buf = torch.empty(64 * 2**20, dtype=torch.int64, device="cuda")   # 512 MB > L2
@@ -439,12 +439,21 @@ def run_extras(torch, M, W):
                            "default": dflt_row[0]["ms"] if dflt_row else None}}
     del bufs, jobs, wsb
     out["deep_scan_r136279841"] = deep_scan_sample(torch, M)
-    out["deep_scan_r136279841_with_gcd"] = deep_scan_gcd_sample(M)
+    # blocked DDF: block size from the measured modmul (per-degree sample) and
+    # batched squaring costs
+    from mersenne_trinomial_b200 import autotune as A
+    t_mul = out["deep_scan_r136279841"]["ms_per_degree_per_s"] / 1e3
+    t_sq = 1.0 / sq_rate if sq_rate else 7.2e-6          # batched state-squaring
+    mblk = A.choose_block(t_mul, t_sq)
+    out["deep_scan_r136279841_blocked"] = deep_scan_sample(torch, M, nsurv=8, degrees=4 * mblk,
+                                                           block=mblk)
+    out["deep_scan_r136279841_blocked"]["block_from"] = {"t_mul_s": t_mul, "t_sq_s": t_sq}
+    out["deep_scan_r136279841_with_gcd"] = deep_scan_gcd_sample(M, block=32)
     out["serving"] = serving_sample()
     return out
 
 
-def deep_scan_sample(torch, M, nsurv=4, degrees=32):
+def deep_scan_sample(torch, M, nsurv=4, degrees=32, block=1):
     """Config 4's per-degree leg at full size: F <- F^2 and ACC <- ACC*(F+x)
     mod T for `nsurv` d<=24 survivors of r = 136279841, batched, degrees
     25..24+degrees; the interval-end half-gcds are measured by
@@ -455,11 +464,11 @@ def deep_scan_sample(torch, M, nsurv=4, degrees=32):
     best = M.run_sieve(R, 24, smax)
     surv = [s for s in range(3, smax + 1) if int(best[s]) == 0xFFFFFFFFFFFFFFFF][:nsurv]
     h = C.c_void_p()
-    call("gf2e_scanner_create", R, nsurv, C.byref(h))
+    call("gf2e_scanner_create_blocked", R, nsurv, block, C.byref(h))
     s_arr = np.asarray(surv, dtype=np.uint64)
     call("gf2e_scanner_submit", h.value, s_arr.ctypes.data, nsurv, 24, 24 + 1000000, 1 << 30,
          1 << 30, 0)
-    call("gf2e_scanner_step", h.value, 1, None)              # ramp + first degree (warm-up)
+    call("gf2e_scanner_step", h.value, block, None)          # ramp + first step (warm-up)
     torch.cuda.synchronize()
     a = torch.cuda.Event(enable_timing=True)
     b = torch.cuda.Event(enable_timing=True)
@@ -469,13 +478,15 @@ def deep_scan_sample(torch, M, nsurv=4, degrees=32):
     torch.cuda.synchronize()
     ms = a.elapsed_time(b)
     M.lib().gf2e_scanner_destroy(h.value)
-    return {"survivors": surv, "degrees": degrees, "ms": ms,
+    return {"survivors": surv, "degrees": degrees, "block": block, "ms": ms,
             "sd_pairs_per_s": nsurv * degrees / (ms / 1e3),
             "ms_per_degree_per_s": ms / degrees / nsurv,
-            "note": "square + running product per degree (no interval end in the sample)"}
+            "note": ("square + running product per degree" if block == 1 else
+                     f"blocked DDF, {block} degrees per step: Horner product, one modmul, "
+                     f"{block}x{block} squarings") + " (no interval end in the sample)"}
 
 
-def deep_scan_gcd_sample(M, nsurv=8, maxd=88):
+def deep_scan_gcd_sample(M, nsurv=8, maxd=88, block=1):
     """Config 4's full cycle at r = 136279841 on a bounded sample: `nsurv`
     d<=24 survivors (s = 474 first, the reference's known answer
     `474 41 p3991ef16129`), ramp to k0 = 24, running products for degrees
@@ -486,11 +497,11 @@ def deep_scan_gcd_sample(M, nsurv=8, maxd=88):
     surv = [474] + [s for s in range(3, smax + 1)
                     if int(best[s]) == 0xFFFFFFFFFFFFFFFF and s != 474][:nsurv - 1]
     t0 = time.perf_counter()
-    lines = M.scan(R, surv, 24, maxd, L0=maxd - 24, Lmax=4096, batch=nsurv)
+    lines = M.scan(R, surv, 24, maxd, L0=maxd - 24, Lmax=4096, batch=nsurv, block=block)
     wall = time.perf_counter() - t0
     return {"survivors": surv, "k0": 24, "maxd": maxd, "results": lines, "wall_s": wall,
             "sd_pairs_per_s": nsurv * (maxd - 24) / wall,
-            "known_answer_474": "474 41 p3991ef16129" in lines,
+            "known_answer_474": "474 41 p3991ef16129" in lines, "block": block,
             "note": "one interval of 64 degrees then one half-gcd per s (concurrent)"}
 
 

@@ -296,6 +296,9 @@ int gf2e_scanner_poll(gf2e_scanner *scanner, gf2e_scan_result *results_host,
  * ====================================================================== */
 typedef struct gf2e_server gf2e_server;
 int gf2e_server_create(size_t budget_bytes, int slots_per_r, gf2e_server **server);
+/* Server whose scanners run the blocked DDF with `block` degrees per step. */
+int gf2e_server_create_blocked(size_t budget_bytes, int slots_per_r, int block,
+                               gf2e_server **server);
 int gf2e_server_destroy(gf2e_server *server);
 int gf2e_server_submit(gf2e_server *server, uint64_t job_id, uint64_t r, const uint64_t *s_host,
                        int ns, uint64_t dmax, uint64_t L0, uint64_t Lmax);
@@ -420,6 +423,11 @@ int gf2e_sieve_autotune(uint64_t r, int dmax, uint64_t smax, int reps,
  * scanning one survivor of a k0-deep sieve up to maxd, under the model that
  * the least factor degree d exceeds D with probability k0 / D.  Pure host
  * arithmetic. */
+/* Block size of the blocked DDF (gf2e_scan_blocked): per scanned degree the
+ * cost is m squarings (t_sq each, per s) plus one modmul (t_mul) per m
+ * degrees, least at m = sqrt(t_mul / t_sq); rounded to even, 2..62. */
+int gf2e_scan_choose_block(double t_mul, double t_sq, int *block);
+
 int gf2e_scan_choose_interval(uint64_t k0, uint64_t maxd, double t_degree,
                               double t_gcd, uint64_t *L0, uint64_t *Lmax,
                               double *expected_cost);

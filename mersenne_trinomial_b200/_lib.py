@@ -111,6 +111,7 @@ SIGNATURES = {
                          _sz, _vp]),
     "gf2e_resolve_factor": (_i32, [_vp, _sz, _u64, _u64, _P(_u64), _vp, _sz, _P(_sz)]),
     "gf2e_server_create": (_i32, [_sz, _i32, _P(_vp)]),
+    "gf2e_server_create_blocked": (_i32, [_sz, _i32, _i32, _P(_vp)]),
     "gf2e_server_destroy": (_i32, [_vp]),
     "gf2e_server_submit": (_i32, [_vp, _u64, _u64, _vp, _i32, _u64, _u64, _u64]),
     "gf2e_server_step": (_i32, [_vp, _i32, _vp]),
@@ -146,6 +147,7 @@ SIGNATURES = {
     "gf2e_fft_autotune": (_i32, [_i32, _i32, _P(Tune), _P(C.c_double), C.c_char_p, _sz]),
     "gf2e_sieve_autotune": (_i32, [_u64, _i32, _u64, _i32, _P(Tune), _P(C.c_double),
                                    C.c_char_p, _sz]),
+    "gf2e_scan_choose_block": (_i32, [C.c_double, C.c_double, _P(_i32)]),
     "gf2e_scan_choose_interval": (_i32, [_u64, _u64, C.c_double, C.c_double, _P(_u64),
                                          _P(_u64), _P(C.c_double)]),
 }

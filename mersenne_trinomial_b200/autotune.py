@@ -88,6 +88,13 @@ def sieve_autotune(r: int, depth: int, smax: int, reps: int = 3) -> dict:
             "best_ms": ms.value, "candidates": rows}
 
 
+def choose_block(t_mul: float, t_sq: float) -> int:
+    """Block size of the blocked DDF from the modmul and squaring costs."""
+    m = C.c_int()
+    call("gf2e_scan_choose_block", float(t_mul), float(t_sq), C.byref(m))
+    return m.value
+
+
 def choose_interval(k0: int, maxd: int, t_degree: float, t_gcd: float) -> dict:
     """gcd interval schedule (L0 doubling to Lmax) minimising expected scan cost."""
     L0, Lmax, cost = C.c_uint64(), C.c_uint64(), C.c_double()

@@ -61,6 +61,7 @@ struct RClass {
 struct gf2e_server {
     size_t budget = 0, used = 0;
     int slots = 64;
+    int block = 1;                                   // blocked-DDF block size of the scanners
     uint64_t next_tag = 1;
     std::map<uint64_t, Job> jobs;                    // by id
     std::deque<uint64_t> waiting;                    // ids not yet admitted
@@ -123,8 +124,8 @@ int admit(gf2e_server &S, Job &J, cudaStream_t st) {
     if (!deep.empty()) {
         RClass &rc = S.rclass[J.r];
         if (!rc.sc) {
-            GF2E_TRY(gf2e_scanner_create(J.r, S.slots, &rc.sc));
-            gf2e_scanner_footprint(J.r, S.slots, &rc.bytes);
+            GF2E_TRY(gf2e_scanner_create_blocked(J.r, S.slots, S.block, &rc.sc));
+            gf2e_scanner_footprint_blocked(J.r, S.slots, S.block, &rc.bytes);
             S.used += rc.bytes;
         }
         rc.users++;
@@ -145,7 +146,7 @@ int try_admit(gf2e_server &S, cudaStream_t st) {
         Job &J = S.jobs[S.waiting.front()];
         size_t need = 0;
         if (J.dmax > (uint64_t)SIEVE_DMAX && !S.rclass[J.r].sc)
-            gf2e_scanner_footprint(J.r, S.slots, &need);
+            gf2e_scanner_footprint_blocked(J.r, S.slots, S.block, &need);
         if (S.used + need > S.budget && S.used > 0) break;      // wait for memory
         S.waiting.pop_front();
         GF2E_TRY(admit(S, J, st));
@@ -158,9 +159,17 @@ int try_admit(gf2e_server &S, cudaStream_t st) {
 extern "C" {
 
 int gf2e_server_create(size_t budget_bytes, int slots_per_r, gf2e_server **out) {
+    return gf2e_server_create_blocked(budget_bytes, slots_per_r, 1, out);
+}
+
+int gf2e_server_create_blocked(size_t budget_bytes, int slots_per_r, int block,
+                               gf2e_server **out) {
     if (!out || slots_per_r < 1) return gf2e::invalid("server: bad arguments");
+    if (!(block == 1 || (block >= 2 && block <= 62 && !(block & 1))))
+        return gf2e::invalid("server: block size must be 1 or even in 2..62");
     gf2e_server *S = new gf2e_server;
     S->slots = slots_per_r;
+    S->block = block;
     int st = gf2e_sieve_workspace_size(SIEVE_DMAX, &S->sieve_ws_bytes);
     if (st != GF2E_OK) { delete S; return st; }
     cudaError_t e = cudaMalloc(&S->sieve_ws, S->sieve_ws_bytes);

@@ -3,7 +3,7 @@
 // survivors, batched over the s values on the GPU with GPU gcds.
 //
 //   trinomial_scan <r> <survivors.txt> <k0> <maxd> <out_prefix>
-//                  [--interval Lmax] [--l0 L0] [--batch B] [--verbose 0..3]
+//                  [--interval Lmax] [--l0 L0] [--batch B] [--block m] [--verbose 0..3]
 //                  [--gcd-threads N] [--state FILE]      (accepted, unused)
 //   trinomial_scan --selftest
 //
@@ -90,12 +90,12 @@ static bool divides(u64 r, u64 s, const u64 *p, size_t pw, u64 d) {
 }
 
 static int run(u64 r, const std::vector<u64> &surv, u64 k0, u64 maxd, u64 L0, u64 Lmax,
-               int batch, FILE *fres, int verbose, u64 *nfound, u64 *nu, u64 *nbad) {
+               int batch, int block, FILE *fres, int verbose, u64 *nfound, u64 *nu, u64 *nbad) {
     const size_t cap = 4096;
     std::vector<gf2e_scan_result> res(surv.size());
     std::vector<u64> masks(surv.size() * cap);
-    int st = gf2e_scan(r, surv.data(), (int)surv.size(), k0, maxd, L0, Lmax, batch, res.data(),
-                       masks.data(), cap, nullptr);
+    int st = gf2e_scan_blocked(r, surv.data(), (int)surv.size(), k0, maxd, L0, Lmax, batch, block,
+                               res.data(), masks.data(), cap, nullptr);
     if (st != GF2E_OK) {
         fprintf(stderr, "scan failed: %s (%s)\n", gf2e_status_string(st), gf2e_last_error());
         return 1;
@@ -137,7 +137,7 @@ static int selftest() {
     const u64 pol[2][2] = {{32, 4096}, {8, 8}};
     for (auto &p : pol) {
         u64 nf = 0, nu = 0, nb = 0;
-        if (run(r, surv, k0, maxd, p[0], p[1], 64, nullptr, 0, &nf, &nu, &nb)) return 1;
+        if (run(r, surv, k0, maxd, p[0], p[1], 64, 1, nullptr, 0, &nf, &nu, &nb)) return 1;
         bool ok = surv.size() == 104 && nf == 102 && nu == 2 && nb == 0;
         printf("scan r=4423 k0=5 maxd=200 intervals %" PRIu64 "/%" PRIu64 ": %zu survivors, "
                "%" PRIu64 " found, %" PRIu64 " u, %" PRIu64 " not dividing  %s\n",
@@ -152,7 +152,7 @@ int main(int argc, char **argv) {
     if (argc >= 2 && !strcmp(argv[1], "--selftest")) return selftest();
     if (argc < 6) {
         fprintf(stderr, "usage: %s <r> <survivors.txt> <k0> <maxd> <out_prefix>\n"
-                        "          [--interval Lmax] [--l0 L0] [--batch B] [--verbose 0..3]\n"
+                        "          [--interval Lmax] [--l0 L0] [--batch B] [--block m] [--verbose 0..3]\n"
                         "       %s --selftest\n"
                         "k0 must be the depth the coarse sieve actually reached.\n",
                 argv[0], argv[0]);
@@ -161,11 +161,12 @@ int main(int argc, char **argv) {
     u64 r = strtoull(argv[1], 0, 10), k0 = strtoull(argv[3], 0, 10), maxd = strtoull(argv[4], 0, 10);
     std::string prefix = argv[5];
     u64 L0 = 64, Lmax = 4096;
-    int batch = 64, verbose = 1;
+    int batch = 64, verbose = 1, block = 1;
     for (int i = 6; i < argc; i++) {
         if (!strcmp(argv[i], "--interval") && i + 1 < argc) Lmax = strtoull(argv[++i], 0, 10);
         else if (!strcmp(argv[i], "--l0") && i + 1 < argc) L0 = strtoull(argv[++i], 0, 10);
         else if (!strcmp(argv[i], "--batch") && i + 1 < argc) batch = atoi(argv[++i]);
+        else if (!strcmp(argv[i], "--block") && i + 1 < argc) block = atoi(argv[++i]);
         else if (!strcmp(argv[i], "--verbose") && i + 1 < argc) verbose = atoi(argv[++i]);
         else if ((!strcmp(argv[i], "--gcd-threads") || !strcmp(argv[i], "--state")) && i + 1 < argc) {
             fprintf(stderr, "note: %s ignored (gcds run on the GPU; results file is the resume record)\n",
@@ -206,7 +207,7 @@ int main(int argc, char **argv) {
     if (!fres) { perror(rpath.c_str()); return 1; }
     double t0 = now_s();
     u64 nf = 0, nu = 0, nb = 0;
-    int rc = todo.empty() ? 0 : run(r, todo, k0, maxd, L0, Lmax, batch, fres, verbose, &nf, &nu, &nb);
+    int rc = todo.empty() ? 0 : run(r, todo, k0, maxd, L0, Lmax, batch, block, fres, verbose, &nf, &nu, &nb);
     fclose(fres);
     fprintf(stderr, "done: %" PRIu64 " found, %" PRIu64 " u, %.1fs total%s\n", nf, nu,
             now_s() - t0, nb ? " (WARNING: some factors failed verification)" : "");

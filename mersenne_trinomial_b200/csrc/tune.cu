@@ -11,7 +11,8 @@
 //         Taylor / butterfly levels fused per register stage;
 //   sieve the strip width of k_strip (entries of best[] per CTA);
 //   scan  the gcd interval schedule (L0 doubling to Lmax), from a cost
-//         model over measured per-degree and per-gcd costs.
+//         model over measured per-degree and per-gcd costs, and the block
+//         size of the blocked DDF from the measured modmul and squaring costs.
 #include "gf2e_internal.cuh"
 
 #include <cmath>
@@ -352,6 +353,18 @@ int gf2e_sieve_autotune(uint64_t r, int dmax, uint64_t smax, int reps, gf2e_tune
     GF2E_TRY(gf2e_tune_set(&win));
     if (best) *best = win;
     if (best_ms) *best_ms = win_ms;
+    return GF2E_OK;
+}
+
+int gf2e_scan_choose_block(double t_mul, double t_sq, int *block) {
+    if (!block || !(t_mul > 0) || !(t_sq > 0)) return gf2e::invalid("gf2e_scan_choose_block: bad arguments");
+    // per degree: m squarings of the m h's... m * t_sq + t_mul / m, least at
+    // m = sqrt(t_mul / t_sq) (tsfactor.cu:1979-1984 picks the same balance)
+    double m = std::sqrt(t_mul / t_sq);
+    int mi = 2 * (int)std::lround(m / 2.0);
+    if (mi < 2) mi = 2;
+    if (mi > 62) mi = 62;
+    *block = mi;
     return GF2E_OK;
 }
 

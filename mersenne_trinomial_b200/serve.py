@@ -25,9 +25,9 @@ from . import workloads as W
 class Server:
     """Owner of one gf2e_server (device memory budget, scanner slots per r)."""
 
-    def __init__(self, budget_bytes: int = 64 << 30, slots_per_r: int = 64):
+    def __init__(self, budget_bytes: int = 64 << 30, slots_per_r: int = 64, block: int = 1):
         h = C.c_void_p()
-        call("gf2e_server_create", budget_bytes, slots_per_r, C.byref(h))
+        call("gf2e_server_create_blocked", budget_bytes, slots_per_r, block, C.byref(h))
         self.h = h.value
 
     def submit(self, job_id: int, r: int, s_values, dmax: int, L0: int = 64, Lmax: int = 4096):
@@ -107,9 +107,9 @@ def job_stream(seed: int, n_jobs: int, rate: float, deep_max: int = 2000,
 
 
 def run_stream(jobs, slots: int = 64, budget: int = 64 << 30, degrees: int = 16,
-               realtime: bool = True):
+               realtime: bool = True, block: int = 1):
     """Serve `jobs` (arrival times in seconds); returns (latencies, wall, lines)."""
-    srv = Server(budget, slots)
+    srv = Server(budget, slots, block)
     t0 = time.perf_counter()
     pending = sorted(jobs, key=lambda j: j["t"])
     i = 0
@@ -135,12 +135,12 @@ def run_stream(jobs, slots: int = 64, budget: int = 64 << 30, degrees: int = 16,
     return lat, wall, lines
 
 
-def run_one_at_a_time(jobs, slots: int = 64, degrees: int = 256):
+def run_one_at_a_time(jobs, slots: int = 64, degrees: int = 256, block: int = 1):
     """The plain path: each job alone on a fresh server, back to back."""
     t0 = time.perf_counter()
     lines = {}
     for j in jobs:
-        srv = Server(64 << 30, slots)
+        srv = Server(64 << 30, slots, block)
         srv.submit(j["id"], j["r"], j["s"], j["dmax"])
         done = []
         while not done:
@@ -161,10 +161,11 @@ def main(argv=None):
     ap.add_argument("--rate", type=float, default=4.0)
     ap.add_argument("--seed", type=int, default=1)
     ap.add_argument("--deep-max", type=int, default=1000)
+    ap.add_argument("--block", type=int, default=1, help="blocked-DDF degrees per step")
     a = ap.parse_args(argv)
     jobs = job_stream(a.seed, a.jobs, a.rate, a.deep_max)
-    lat, wall, lines = run_stream(jobs)
-    plain_wall, plain_lines = run_one_at_a_time(jobs)
+    lat, wall, lines = run_stream(jobs, block=a.block)
+    plain_wall, plain_lines = run_one_at_a_time(jobs, block=a.block)
     v = sorted(lat.values())
     same = all(lines[k] == plain_lines[k] for k in lines)
     out = {"jobs": len(jobs), "p50_s": float(np.percentile(v, 50)),

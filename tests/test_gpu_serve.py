@@ -57,3 +57,13 @@ def test_sieve_only_job_matches_oracle(engine, oracle):
         want.append(f"{v} u" if k == 0xFFFFFFFFFFFFFFFF else f"{v} {k >> 48} p{k & 0xFFFFFFFFFFFF:x}")
     assert lines == want
     srv.close()
+
+
+def test_blocked_server_matches_per_degree_server(engine):
+    """Scanners in blocked-DDF mode give every job the same lines as the
+    per-degree scanners."""
+    from mersenne_trinomial_b200 import serve
+    jobs = serve.job_stream(seed=7, n_jobs=6, rate=1000.0, deep_max=300, s_lo=8, s_hi=24)
+    _, _, plain = serve.run_stream(jobs, slots=16, realtime=False)
+    _, _, blocked = serve.run_stream(jobs, slots=16, realtime=False, block=8)
+    assert plain == blocked

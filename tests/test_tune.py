@@ -88,3 +88,17 @@ def test_choose_interval_rejects_bad_arguments(engine):
                  (24, 100, 1.0, -1.0)):
         with pytest.raises(engine.Gf2eError):
             A.choose_interval(*args)
+
+
+def test_choose_block_balances_squarings_and_modmuls(engine):
+    from mersenne_trinomial_b200 import autotune as A
+    assert A.choose_block(15e-3, 7.2e-6) == 46          # sqrt(2083) = 45.6
+    assert A.choose_block(1.0, 1.0) == 2                 # floor
+    assert A.choose_block(1.0, 1e-9) == 62               # cap
+    for t_mul, t_sq in ((1e-2, 1e-5), (3e-3, 2e-5), (0.2, 1e-6)):
+        m = A.choose_block(t_mul, t_sq)
+        assert m % 2 == 0 and 2 <= m <= 62
+        cost = lambda k: k * t_sq + t_mul / k
+        assert cost(m) <= min(cost(k) for k in range(2, 63, 2)) * 1.05
+    with pytest.raises(engine.Gf2eError):
+        A.choose_block(0.0, 1.0)
