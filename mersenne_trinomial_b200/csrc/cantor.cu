@@ -26,8 +26,7 @@
 
 namespace {
 
-constexpr int TILE_LOG_MIN = 11;           // shared-memory tile sizes a plan may use:
-constexpr int TILE_LOG_MAX = 13;           // 2^11..2^13 elements (16..64 KB)
+// shared-memory tiles are 2^11..2^13 elements (16..64 KB), chosen per plan
 constexpr int MAXOPS = 96;
 constexpr int FFT_THREADS = 512;           // 2 CTAs x 64 registers per SM
 constexpr int NTWTAB = 4;                  // byte tables: t < 2^32

@@ -76,14 +76,6 @@ void pmod(Poly &a, const Poly &m) {
     }
     ptrim(a);
 }
-Poly pmul(const Poly &a, const Poly &b) {
-    Poly c(a.size() + b.size() + 1, 0);
-    for (size_t i = 0; i < a.size(); i++)
-        for (int bit = 0; bit < 64; bit++)
-            if ((a[i] >> bit) & 1) pxor_shift(c, b, (u64)i * 64 + bit);
-    ptrim(c);
-    return c;
-}
 Poly psqr(const Poly &a) {
     Poly c(2 * a.size() + 1, 0);
     for (size_t i = 0; i < a.size(); i++)

@@ -107,8 +107,8 @@ int admit(gf2e_server &S, Job &J, cudaStream_t st) {
         uint64_t k = best[J.s[i]];
         char buf[96];
         if (k != ~0ull) {
-            snprintf(buf, sizeof buf, "%" PRIu64 " %u p%" PRIx64, J.s[i], (unsigned)(k >> 48),
-                     k & 0xFFFFFFFFFFFFull);
+            snprintf(buf, sizeof buf, "%" PRIu64 " %u p%" PRIx64, (uint64_t)J.s[i],
+                     (unsigned)(k >> 48), (uint64_t)(k & 0xFFFFFFFFFFFFull));
             J.lines[i] = buf;
         } else if (J.dmax <= (uint64_t)SIEVE_DMAX) {
             snprintf(buf, sizeof buf, "%" PRIu64 " u", J.s[i]);
