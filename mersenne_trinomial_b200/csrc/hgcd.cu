@@ -113,9 +113,19 @@ __global__ void k_shr(const u64 *__restrict__ src, u64 ns, u64 k, u64 *__restric
 // out = x1*y1 + x2*y2 (schoolbook).  Thread = two adjacent output words,
 // blockIdx.y = a chunk of the x index; partial sums are XORed into out,
 // which must be zero on entry.
-__global__ void k_mul2(const u64 *__restrict__ x1, u64 nx1, const u64 *__restrict__ y1, u64 ny1,
-                       const u64 *__restrict__ x2, u64 nx2, const u64 *__restrict__ y2, u64 ny2,
-                       unsigned long long *__restrict__ out, u64 nout, u64 chunk) {
+struct Mul2Jobs {                       // up to four sums of two products, blockIdx.z = job
+    const u64 *x1[4], *y1[4], *x2[4], *y2[4];
+    u64 nx1[4], ny1[4], nx2[4], ny2[4];
+    unsigned long long *out[4];
+    u64 nout[4];
+};
+__global__ void k_mul2(const Mul2Jobs J, u64 chunk) {
+    const int z = blockIdx.z;
+    const u64 *__restrict__ x1 = J.x1[z], *__restrict__ y1 = J.y1[z];
+    const u64 *__restrict__ x2 = J.x2[z], *__restrict__ y2 = J.y2[z];
+    const u64 nx1 = J.nx1[z], ny1 = J.ny1[z], nx2 = J.nx2[z], ny2 = J.ny2[z];
+    unsigned long long *__restrict__ out = J.out[z];
+    const u64 nout = J.nout[z];
     const u64 w = 2 * ((u64)blockIdx.x * blockDim.x + threadIdx.x);
     if (w >= nout) return;
     const u64 i0 = (u64)blockIdx.y * chunk;
@@ -190,12 +200,6 @@ GF2E_DEV u64 clmul_masked(const Masked &a, const Masked &b) {
     u64 c3 = (a.p[0] * b.p[3]) ^ (a.p[1] * b.p[2]) ^ (a.p[2] * b.p[1]) ^ (a.p[3] * b.p[0]);
     return (c0 & M0) ^ (c1 & (M0 << 1)) ^ (c2 & (M0 << 2)) ^ (c3 & (M0 << 3));
 }
-// x (64 bits) times m (<= 32 bits): (lo 64, hi 32)
-GF2E_DEV void mul64x32(u64 x, const Masked &m, u64 &lo, u64 &hi) {
-    u64 p0 = clmul_masked(mask32((u32)x), m), p1 = clmul_masked(mask32((u32)(x >> 32)), m);
-    lo = p0 ^ (p1 << 32);
-    hi = p1 >> 32;
-}
 
 GF2E_DEV u64 win_at(const u64 *X, long long nw, long long pos) {   // bits pos..pos+63
     long long i = pos >> 6;
@@ -204,11 +208,11 @@ GF2E_DEV u64 win_at(const u64 *X, long long nw, long long pos) {   // bits pos..
     return funnel64(a, b, sh);
 }
 
-struct BaseOut {
-    long long deg_a, deg_b;     // degrees of the reduced pair
-    long long rounds;
-    long long cyc_serial, cyc_total;   // SM clock cycles: thread-0 window phase, whole kernel
-    int status;
+// totals over the base cases of one gcd, read once when the gcd is done
+struct BaseAcc {
+    unsigned long long rounds;
+    unsigned long long cyc_serial, cyc_total;   // SM clock cycles: thread-0 window phase, total
+    int worst;                                  // first non-OK status, else GF2E_OK
 };
 
 // warp-wide degree of X below word `top` (inclusive); all 32 lanes return it
@@ -227,30 +231,102 @@ GF2E_DEV long long warp_degree(const u64 *X, long long top) {
     return -1;
 }
 
+// one Lehmer round on exact 64-bit windows of A and B taken at bit `lo`
+// (deg A = da >= deg B): whole quotients while every bit they depend on is
+// exact (a row's window bits are exact above its matrix degree), the
+// half-gcd stop (deg B < m) is not reached and the 2x2 matrix stays within
+// degree 31; mode 1 (no quotient fits) is the single shift-XOR A ^= B << k.
+struct Lehmer {
+    u32 mt[4];
+    long long k;
+    int mode;
+};
+GF2E_DEV Lehmer lehmer_round(u64 wa, u64 wb, long long da, long long db, long long lo,
+                             long long m) {
+    Lehmer L;
+    u32 ma0 = 1, ma1 = 0, mb0 = 0, mb1 = 1;
+    int dga = (int)(da - lo), dgb = deg64(wb), dma = 0, dmb = 0, steps = 0;
+    const bool exact = (lo == 0);
+    const int dstop = (int)max(-1LL, m - lo);          // window degree of x^m
+    for (int it = 0; it < 64; it++) {
+        if (dgb < 0 || dgb < dstop) break;              // b = 0 / half-gcd stop
+        const int dq = dga - dgb;
+        const int ndm = max(dma, dmb + dq);
+        if (ndm > 31) break;                            // matrix degree bound
+        if (!exact && dgb < ndm) break;                 // quotient not exact
+#pragma unroll 1
+        do {                                            // a <- a mod b
+            const int k = dga - dgb;
+            wa ^= wb << k;
+            ma0 ^= mb0 << k;
+            ma1 ^= mb1 << k;
+            dga = deg64(wa);
+        } while (dga >= dgb);
+        dma = ndm;
+        u64 t = wa; wa = wb; wb = t;                    // (a, b) <- (b, a mod b)
+        u32 y = ma0; ma0 = mb0; mb0 = y;
+        y = ma1; ma1 = mb1; mb1 = y;
+        int z = dga; dga = dgb; dgb = z;
+        z = dma; dma = dmb; dmb = z;
+        steps++;
+    }
+    if (steps == 0) {
+        L.mode = 1;
+        L.k = da - db;
+        L.mt[0] = L.mt[1] = L.mt[2] = L.mt[3] = 0;
+    } else {
+        L.mode = 0;
+        L.k = 0;
+        L.mt[0] = ma0; L.mt[1] = ma1; L.mt[2] = mb0; L.mt[3] = mb1;
+    }
+    return L;
+}
+
+// lo and hi parts of x (64 bits) times a 32-bit polynomial
+GF2E_DEV u64 mul64x32_lo(u64 x, const Masked &m) {
+    return clmul_masked(mask32((u32)x), m) ^ (clmul_masked(mask32((u32)(x >> 32)), m) << 32);
+}
+GF2E_DEV u64 mul64x32_hi(u64 x, const Masked &m) {
+    return clmul_masked(mask32((u32)(x >> 32)), m) >> 32;
+}
+// word w of (X << k) for a vector X
+GF2E_DEV u64 shl_word(const u64 *X, long long w, long long k) {
+    const long long ks = k >> 6;
+    const unsigned kb = (unsigned)(k & 63);
+    u64 h = (w >= ks) ? X[w - ks] : 0, l = (w >= ks + 1) ? X[w - ks - 1] : 0;
+    return kb ? ((h << kb) | (l >> (64 - kb))) : h;
+}
+// word w of one new vector / row: mode 0: m0*X + m1*Y; mode 1 (row a): X ^ (Y << k)
+GF2E_DEV u64 new_word(int mode, const u64 *X, const u64 *Y, long long w, const Masked &m0,
+                      const Masked &m1, long long k, bool is_a) {
+    if (mode == 1) return is_a ? (X[w] ^ shl_word(Y, w, k)) : Y[w];
+    u64 v = mul64x32_lo(X[w], m0) ^ mul64x32_lo(Y[w], m1);
+    if (w >= 1) v ^= mul64x32_hi(X[w - 1], m0) ^ mul64x32_hi(Y[w - 1], m1);
+    return v;
+}
+
 // (a', b') = M (a, b) with deg a' >= m > deg b'; M written to four arrays of
 // mw words (row-major M00 M01 M10 M11).
 //
-// Each round, thread 0 runs Euclid on the 64-bit top windows of A and B
-// (Lehmer): whole quotients, each taken only when every bit it depends on is
-// exact (window bits of a row lie above that row's matrix degree) and the
-// half-gcd stop (deg B < m) is not reached, while the accumulated 2x2 matrix
-// stays within degree 31.  The CTA then applies the matrix to A, B and to the
-// accumulated rows, one output word per thread.  Leading bits that were exact
-// in the windows give the new degrees; otherwise warp 0 scans down from the
-// old top word.  A degree gap the matrix cannot hold is one shift-XOR round.
-// Shared memory: V[4][W] (two buffers of A, B), R[2][4][mw] (two buffers of
-// the rows), carries of 2W + 4mw words.
+// Lehmer rounds, pipelined: while warps 1..15 apply round r's matrix to the
+// vectors A, B and to the accumulated rows (one output word per item, the
+// carry from word w-1 recomputed, so no barrier inside the round), warp 0
+// computes the three top words of the new A and B itself, reads their
+// degrees and 64-bit windows off them and runs round r+1's Euclid steps on
+// thread 0.  One barrier per round; when the new windows are not within
+// those three words (a large drop in degree), warp 0 scans the new vectors
+// after the barrier instead.  Round state is double-buffered by parity.
+// Shared memory: V[4][W] (two buffers of A, B), R[2][4][mw].
 __global__ void __launch_bounds__(BASE_THREADS)
 k_hgcd_base(const u64 *__restrict__ a, long long da0, const u64 *__restrict__ b, long long db0,
-            long long m, u64 W, u64 mw, u64 *__restrict__ Mout, BaseOut *res) {
+            long long m, u64 W, u64 mw, u64 *__restrict__ Mout, BaseAcc *acc) {
     extern __shared__ u64 sh[];
     u64 *V = sh;
     u64 *R = sh + 4 * W;
-    u64 *hiv = R + 8 * mw;
-    u64 *hir = hiv + 2 * W;
-    __shared__ int s_va, s_vb, s_ra, s_buf, s_mode, s_done;
-    __shared__ long long s_md, s_k, s_top;
-    __shared__ u32 s_m[4];
+    __shared__ int s_va[2], s_vb[2], s_ra[2], s_mode[2], s_done[2], s_slow;
+    __shared__ long long s_k[2], s_top[2], s_md[2];
+    __shared__ u32 s_m[2][4];
+    __shared__ u64 s_tw[6];
     const int tid = threadIdx.x;
     for (u64 i = tid; i < 4 * W; i += BASE_THREADS) {
         u64 v = 0;
@@ -259,202 +335,159 @@ k_hgcd_base(const u64 *__restrict__ a, long long da0, const u64 *__restrict__ b,
         V[i] = v;
     }
     for (u64 i = tid; i < 8 * mw; i += BASE_THREADS) R[i] = (i == 0 || i == 3 * mw) ? 1 : 0;
-    if (tid == 0) {
-        s_va = 0; s_vb = 1; s_ra = 0; s_buf = 0;
-        s_md = 0; s_done = 0; s_top = 0;
-    }
     __syncthreads();
-    // warp-0 registers: degrees, buffer roles, round bookkeeping
-    long long da = da0, db = db0;
-    int va = 0, vb = 1, ra = 0, status = GF2E_ERR_INTERNAL;
-    bool known_a = true, known_b = true;
-    long long top = 0, rounds = 0;
     const long long max_rounds = 2 * (da0 + 2) + 16;
+    int status = GF2E_OK;
+    long long rounds = 0;
     const long long cyc0 = clock64();
     long long cyc_serial = 0;
-    for (long long round = 0;; round++) {
-        if (tid < 32) {
-            if (round > 0) {
-                // the spare buffers hold the new A, B; rows were written in (A, B) order
-                int spare[2], ns = 0;
-                for (int i = 0; i < 4 && ns < 2; i++)
-                    if (i != va && i != vb) spare[ns++] = i;
-                va = spare[0]; vb = spare[1]; ra = 0;
-                if (!known_a) da = warp_degree(V + (u64)va * W, top);
-                if (!known_b) db = warp_degree(V + (u64)vb * W, top);
-            }
-            if (tid == 0) {
-                const long long c0 = clock64();
-                if (da < db) {
-                    long long t = da; da = db; db = t;
-                    int x = va; va = vb; vb = x;
-                    ra ^= 1;
-                }
-                int mode = 0;
-                bool done = false;
-                if (db < m || round > max_rounds) {
-                    done = true;
-                    status = (round > max_rounds) ? GF2E_ERR_TIMEOUT : GF2E_OK;
-                    rounds = round;
-                } else {
-                    const u64 *A = V + (u64)va * W, *B = V + (u64)vb * W;
-                    const long long lo = da >= 63 ? da - 63 : 0;
-                    u64 wa = win_at(A, (long long)W, lo), wb = win_at(B, (long long)W, lo);
-                    u32 ma0 = 1, ma1 = 0, mb0 = 0, mb1 = 1;
-                    int dga = (int)(da - lo), dgb = deg64(wb), dma = 0, dmb = 0, steps = 0;
-                    const bool exact = (lo == 0);
-                    const int dstop = (int)max(-1LL, m - lo);      // window degree of x^m
-                    for (int it = 0; it < 64; it++) {
-                        if (dgb < 0 || dgb < dstop) break;          // b = 0 / half-gcd stop
-                        const int dq = dga - dgb;
-                        const int ndm = max(dma, dmb + dq);
-                        if (ndm > 31) break;                         // matrix degree bound
-                        if (!exact && dgb < max(dma, dmb + dq)) break;   // quotient not exact
-#pragma unroll 1
-                        do {                                         // a <- a mod b
-                            const int k = dga - dgb;
-                            wa ^= wb << k;
-                            ma0 ^= mb0 << k;
-                            ma1 ^= mb1 << k;
-                            dga = deg64(wa);
-                        } while (dga >= dgb);
-                        dma = ndm;
-                        u64 t = wa; wa = wb; wb = t;                 // (a, b) <- (b, a mod b)
-                        u32 y = ma0; ma0 = mb0; mb0 = y;
-                        y = ma1; ma1 = mb1; mb1 = y;
-                        int z = dga; dga = dgb; dgb = z;
-                        z = dma; dma = dmb; dmb = z;
-                        steps++;
-                    }
-                    top = da >> 6;
-                    if (steps == 0) {
-                        mode = 1;                                    // A ^= B << (da - db)
-                        s_k = da - db;
-                        known_a = false;
-                        known_b = true;
-                    } else {
-                        s_m[0] = ma0; s_m[1] = ma1; s_m[2] = mb0; s_m[3] = mb1;
-                        known_a = true;                              // the old b's exact lead
-                        da = dga + lo;
-                        known_b = exact || (dgb >= 0 && dgb >= dmb);
-                        if (known_b) db = dgb < 0 ? -1 : dgb + lo;
-                    }
-                }
-                s_mode = mode;
-                s_done = done;
-                s_va = va; s_vb = vb; s_ra = ra; s_top = top;
-                cyc_serial += clock64() - c0;
-            }
-            // share thread 0's decisions with the rest of warp 0
-            da = __shfl_sync(0xffffffffu, da, 0);
-            db = __shfl_sync(0xffffffffu, db, 0);
-            va = __shfl_sync(0xffffffffu, va, 0);
-            vb = __shfl_sync(0xffffffffu, vb, 0);
-            ra = __shfl_sync(0xffffffffu, ra, 0);
-            top = __shfl_sync(0xffffffffu, top, 0);
-            known_a = __shfl_sync(0xffffffffu, known_a, 0);
-            known_b = __shfl_sync(0xffffffffu, known_b, 0);
+
+    // thread 0: publish round q's state from degrees/roles and windows
+    auto publish = [&](int q, int va, int vb, int ra, long long da, long long db, u64 wa, u64 wb,
+                       long long md, long long round) {
+        if (da < db) {
+            int x = va; va = vb; vb = x;
+            ra ^= 1;
+            long long t = da; da = db; db = t;
+            u64 u = wa; wa = wb; wb = u;
         }
-        __syncthreads();
-        if (s_done) break;
-        const int cva = s_va, cvb = s_vb, buf = s_buf, nb = buf ^ 1, cra = s_ra, crb = s_ra ^ 1;
-        const long long nwv = s_top + 1;                       // live vector words
-        const long long nwm = min((long long)mw, s_md + 2);    // live matrix words
+        s_va[q] = va; s_vb[q] = vb; s_ra[q] = ra;
+        s_top[q] = da >> 6;
+        s_md[q] = md;
+        if (db < m || round > max_rounds) {
+            s_done[q] = 1;
+            if (round > max_rounds) status = GF2E_ERR_TIMEOUT;
+            rounds = round;
+            return;
+        }
+        s_done[q] = 0;
+        const long long lo = da >= 63 ? da - 63 : 0;
+        const long long c0 = clock64();
+        Lehmer L = lehmer_round(wa, wb, da, db, lo, m);
+        cyc_serial += clock64() - c0;
+        s_mode[q] = L.mode;
+        s_k[q] = L.k;
+        for (int i = 0; i < 4; i++) s_m[q][i] = L.mt[i];
+    };
+    // thread 0: degrees and windows of vectors va, vb read from shared memory
+    auto publish_from_vectors = [&](int q, int va, int vb, int ra, long long da, long long db,
+                                    long long md, long long round) {
+        const long long dhi = max(da, db);
+        const long long lo = dhi >= 63 ? dhi - 63 : 0;
+        publish(q, va, vb, ra, da, db, win_at(V + (u64)va * W, (long long)W, lo),
+                win_at(V + (u64)vb * W, (long long)W, lo), md, round);
+    };
+    if (tid == 0) publish_from_vectors(0, 0, 1, 0, da0, db0, 0, 0);
+    __syncthreads();
+
+    long long final_round = 0;
+    for (long long round = 0;; round++) {
+        const int p = (int)(round & 1), q = p ^ 1;
+        if (s_done[p]) { final_round = round; break; }
+        const int va = s_va[p], vb = s_vb[p], ra = s_ra[p], mode = s_mode[p];
+        const long long top = s_top[p], md = s_md[p], k = s_k[p];
+        // live words: vectors 0..top; rows 0..nwm (the growth of this round included)
+        const long long nwv = top + 1;
+        const long long nwm = min((long long)mw - 1, md + (mode == 1 ? (k >> 6) + 1 : 1));
         int spare[2], ns = 0;
         for (int i = 0; i < 4 && ns < 2; i++)
-            if (i != cva && i != cvb) spare[ns++] = i;
-        const u64 *VA = V + (u64)cva * W, *VB = V + (u64)cvb * W;
-        u64 *V2a = V + (u64)spare[0] * W, *V2b = V + (u64)spare[1] * W;
-        const u64 *RA = R + (u64)(buf * 4 + 2 * cra) * mw;     // row of A: col c at RA + c*mw
-        const u64 *RB = R + (u64)(buf * 4 + 2 * crb) * mw;
-        u64 *N = R + (u64)nb * 4 * mw;                          // new rows, entry e at N + e*mw
-        if (s_mode == 1) {
-            const long long k = s_k, ks = k >> 6;
-            const unsigned kb = (unsigned)(k & 63);
-            auto shl = [&](const u64 *X, long long w) -> u64 {
-                u64 h = (w >= ks) ? X[w - ks] : 0, l = (w >= ks + 1) ? X[w - ks - 1] : 0;
-                return kb ? ((h << kb) | (l >> (64 - kb))) : h;
-            };
-            for (long long w = tid; w < (long long)W; w += BASE_THREADS) {
-                V2a[w] = (w < nwv) ? (VA[w] ^ shl(VB, w)) : 0;
-                V2b[w] = (w < nwv) ? VB[w] : 0;
-            }
-            for (long long w = tid; w < (long long)mw; w += BASE_THREADS) {
-                N[0 * mw + w] = RA[w] ^ shl(RB, w);
-                N[1 * mw + w] = RA[mw + w] ^ shl(RB + mw, w);
-                N[2 * mw + w] = RB[w];
-                N[3 * mw + w] = RB[mw + w];
-            }
-            __syncthreads();
-            if (tid == 0) s_md = min((long long)mw - 2, s_md + ks + 1);
-        } else {
-            const Masked k0 = mask32(s_m[0]), k1 = mask32(s_m[1]), k2 = mask32(s_m[2]),
-                         k3 = mask32(s_m[3]);
-            // items: 2 vectors x nwv words, then 4 row entries x nwm words
-            const long long nvi = 2 * nwv, nitems = nvi + 4 * nwm;
-            for (long long it = tid; it < nitems; it += BASE_THREADS) {
-                u64 lo0, hi0, lo1, hi1;
+            if (i != va && i != vb) spare[ns++] = i;
+        const u64 *A = V + (u64)va * W, *B = V + (u64)vb * W;
+        u64 *A2 = V + (u64)spare[0] * W, *B2 = V + (u64)spare[1] * W;
+        const u64 *RA = R + (u64)(p * 4 + 2 * ra) * mw, *RB = R + (u64)(p * 4 + 2 * (ra ^ 1)) * mw;
+        u64 *N = R + (u64)q * 4 * mw;
+        const Masked m0 = mask32(s_m[p][0]), m1 = mask32(s_m[p][1]), m2 = mask32(s_m[p][2]),
+                     m3 = mask32(s_m[p][3]);
+        const long long md_next = min((long long)mw - 2, md + (mode == 1 ? (k >> 6) + 1 : 1));
+        const int warp = tid >> 5;
+        if (warp != 0 && (warp & 3) != 0) {
+            // the apply runs on the warps of the other three schedulers, so
+            // warp 0's serial chain keeps its scheduler (warp w is on w % 4).
+            // items: 2 vectors x W words (stale words beyond the live range
+            // cleared), then 4 row entries x (nwm + 1) words
+            constexpr int APPLY_THREADS = (BASE_THREADS / 32 / 4) * 3 * 32;
+            const int at = (warp - 1 - (warp >> 2)) * 32 + (tid & 31);
+            const long long nvi = 2 * (long long)W, nitems = nvi + 4 * (nwm + 1);
+            for (long long it = at; it < nitems; it += APPLY_THREADS) {
                 if (it < nvi) {
-                    const bool v = it >= nwv;
-                    const long long w = v ? it - nwv : it;
-                    mul64x32(VA[w], v ? k2 : k0, lo0, hi0);
-                    mul64x32(VB[w], v ? k3 : k1, lo1, hi1);
-                    (v ? V2b : V2a)[w] = lo0 ^ lo1;
-                    hiv[(v ? W : 0) + w] = hi0 ^ hi1;
+                    const bool v = it >= (long long)W;
+                    const long long w = v ? it - (long long)W : it;
+                    u64 val = 0;
+                    if (w < nwv)
+                        val = v ? new_word(mode, A, B, w, m2, m3, k, false)
+                                : new_word(mode, A, B, w, m0, m1, k, true);
+                    (v ? B2 : A2)[w] = val;
                 } else {
                     const long long j = it - nvi;
-                    const int e = (int)(j / nwm);
-                    const long long w = j - (long long)e * nwm;
+                    const int e = (int)(j / (nwm + 1));
+                    const long long w = j - (long long)e * (nwm + 1);
                     const bool row = e >> 1;
                     const u64 col = (u64)(e & 1) * mw;
-                    mul64x32(RA[col + w], row ? k2 : k0, lo0, hi0);
-                    mul64x32(RB[col + w], row ? k3 : k1, lo1, hi1);
-                    N[(u64)e * mw + w] = lo0 ^ lo1;
-                    hir[(u64)e * mw + w] = hi0 ^ hi1;
+                    N[(u64)e * mw + w] = row ? new_word(mode, RA + col, RB + col, w, m2, m3, k, false)
+                                             : new_word(mode, RA + col, RB + col, w, m0, m1, k, true);
                 }
             }
-            for (long long w = nwm + tid; w < (long long)mw; w += BASE_THREADS) {
-                N[0 * mw + w] = 0; N[1 * mw + w] = 0; N[2 * mw + w] = 0; N[3 * mw + w] = 0;
+        } else if (warp == 0) {
+            // warp 0: the three top words of the new A (lanes 0-2) and B (3-5)
+            const int lane = tid;
+            if (lane < 6) {
+                const bool v = lane >= 3;
+                const long long w = top - (lane % 3);
+                u64 val = 0;
+                if (w >= 0)
+                    val = v ? new_word(mode, A, B, w, m2, m3, k, false)
+                            : new_word(mode, A, B, w, m0, m1, k, true);
+                s_tw[lane] = val;
             }
-            for (long long w = nwv + tid; w < (long long)W; w += BASE_THREADS) {
-                V2a[w] = 0; V2b[w] = 0;
+            __syncwarp();
+            if (lane == 0) {
+                long long dn[2] = {-1, -1};
+                for (int v = 0; v < 2; v++)
+                    for (int i = 0; i < 3 && dn[v] < 0; i++)
+                        if (s_tw[3 * v + i]) dn[v] = (top - i) * 64 + 63 - __clzll(s_tw[3 * v + i]);
+                bool slow = dn[0] < 0 || dn[1] < 0;
+                if (!slow) {
+                    const long long dhi = max(dn[0], dn[1]);
+                    const long long lo = dhi >= 63 ? dhi - 63 : 0;
+                    const long long i0 = lo >> 6;
+                    slow = i0 < top - 2;
+                    if (!slow) {
+                        u64 wn[2];
+                        const unsigned sb = (unsigned)(lo & 63);
+                        for (int v = 0; v < 2; v++) {
+                            const u64 x0 = s_tw[3 * v + (int)(top - i0)];
+                            const u64 x1 = (i0 + 1 <= top) ? s_tw[3 * v + (int)(top - i0 - 1)] : 0;
+                            wn[v] = funnel64(x0, x1, sb);
+                        }
+                        publish(q, spare[0], spare[1], 0, dn[0], dn[1], wn[0], wn[1], md_next,
+                                round + 1);
+                    }
+                }
+                s_slow = slow;
+            }
+        }
+        __syncthreads();
+        if (s_slow) {                                  // degrees from the full new vectors
+            if (tid < 32) {
+                const long long d0 = warp_degree(A2, top), d1 = warp_degree(B2, top);
+                if (tid == 0) publish_from_vectors(q, spare[0], spare[1], 0, d0, d1, md_next, round + 1);
             }
             __syncthreads();
-            // carries out of word w-1 (the new vectors stay below the old top word)
-            for (long long it = tid; it < nitems; it += BASE_THREADS) {
-                if (it < nvi) {
-                    const bool v = it >= nwv;
-                    const long long w = v ? it - nwv : it;
-                    if (w >= 1) (v ? V2b : V2a)[w] ^= hiv[(v ? W : 0) + w - 1];
-                } else {
-                    const long long j = it - nvi;
-                    const int e = (int)(j / nwm);
-                    const long long w = j - (long long)e * nwm;
-                    if (w >= 1) N[(u64)e * mw + w] ^= hir[(u64)e * mw + w - 1];
-                }
-            }
-            // the growth word of the rows takes the carry out of the last live word
-            if (nwm < (long long)mw)
-                for (int e = tid; e < 4; e += BASE_THREADS)
-                    N[(u64)e * mw + nwm] ^= hir[(u64)e * mw + nwm - 1];
-            if (tid == 0) s_md = min((long long)mw - 2, s_md + 1);
         }
-        if (tid == 0) s_buf = nb;
-        __syncthreads();
     }
-    // matrix out, rows in (A, B) order
-    const int buf = s_buf, fra = s_ra;
+    // matrix out, rows in (A, B) order; the final round's parity holds them
+    const int pf = (int)(final_round & 1);
+    __syncthreads();
+    const int fra = s_ra[pf];
     for (u64 w = tid; w < 2 * mw; w += BASE_THREADS) {
-        Mout[w] = R[(u64)(buf * 4 + 2 * fra) * mw + w];
-        Mout[2 * mw + w] = R[(u64)(buf * 4 + 2 * (fra ^ 1)) * mw + w];
+        Mout[w] = R[(u64)(pf * 4 + 2 * fra) * mw + w];
+        Mout[2 * mw + w] = R[(u64)(pf * 4 + 2 * (fra ^ 1)) * mw + w];
     }
     if (tid == 0) {
-        res->deg_a = da;
-        res->deg_b = db;
-        res->rounds = rounds;
-        res->cyc_serial = cyc_serial;
-        res->cyc_total = clock64() - cyc0;
-        res->status = status;
+        atomicAdd(&acc->rounds, (unsigned long long)rounds);
+        atomicAdd(&acc->cyc_serial, (unsigned long long)cyc_serial);
+        atomicAdd(&acc->cyc_total, (unsigned long long)(clock64() - cyc0));
+        if (status != GF2E_OK) atomicCAS(&acc->worst, GF2E_OK, status);
     }
 }
 
@@ -489,6 +522,8 @@ typedef std::shared_ptr<DBuf> Buf;
 struct Poly {
     Buf b;
     long long deg = -1;
+    u64 win = 0;          // top 64 bits aligned at deg, valid when has_win
+    bool has_win = false;
     u64 *p() const { return b ? b->p : nullptr; }
     u64 words() const { return deg < 0 ? 0 : (u64)(deg >> 6) + 1; }
 };
@@ -536,6 +571,21 @@ public:
         ckc(cudaMallocHost(&h_probe_, 16 * sizeof(long long)), "hgcd probe host buffer");
         d_probe_ = alloc(16);
         d_res_ = alloc(8);
+        ckc(cudaMemsetAsync(d_res_->p, 0, sizeof(BaseAcc), st_), "hgcd base accumulator");
+    }
+
+    // read the base-case totals; a failed base case fails the gcd
+    void finish_bases() {
+        BaseAcc acc;
+        ckc(cudaMemcpyAsync(&acc, d_res_->p, sizeof acc, cudaMemcpyDeviceToHost, st_), "base totals");
+        ckc(cudaStreamSynchronize(st_), "base totals sync");
+        stats.base_rounds = (long long)acc.rounds;
+        stats.cyc_serial = (long long)acc.cyc_serial;
+        stats.cyc_total = (long long)acc.cyc_total;
+        if (acc.worst != GF2E_OK) {
+            gf2e::set_error("hgcd base case status %d", acc.worst);
+            throw Fail{acc.worst};
+        }
     }
     ~Hgcd() {
         if (h_probe_) cudaFreeHost(h_probe_);
@@ -594,7 +644,9 @@ public:
         int i = 0;
         for (Poly *p : ps) {
             p->deg = h_probe_[2 * i];
-            if (wins) wins[i] = (u64)h_probe_[2 * i + 1];
+            p->win = (u64)h_probe_[2 * i + 1];
+            p->has_win = true;
+            if (wins) wins[i] = p->win;
             i++;
         }
     }
@@ -610,66 +662,42 @@ public:
         return r;
     }
 
-    // x1*y1 + x2*y2 (x2/y2 may be empty); deg of the result is a bound
-    Poly mul2(const Poly &x1, const Poly &y1, const Poly &x2, const Poly &y2) {
-        const bool t1 = x1.deg >= 0 && y1.deg >= 0, t2 = x2.deg >= 0 && y2.deg >= 0;
-        long long dmax = -1;
-        if (t1) dmax = std::max(dmax, x1.deg + y1.deg);
-        if (t2) dmax = std::max(dmax, x2.deg + y2.deg);
-        Poly r;
-        if (dmax < 0) { r.b = alloc(1); r.deg = -1; return r; }
-        const u64 nout = (u64)(dmax >> 6) + 2;
-        if (dmax + 1 > tn_.fft_bits) {
-            r = fft_mul2(t1 ? &x1 : nullptr, t1 ? &y1 : nullptr, t2 ? &x2 : nullptr,
-                         t2 ? &y2 : nullptr, nout);
-        } else {
-            r = zeros(nout);
-            const u64 nxm = std::max(t1 ? x1.words() : 0, t2 ? x2.words() : 0);
-            const u64 chunk = 32;
-            dim3 grid((unsigned)((nout / 2 + 1 + 127) / 128), (unsigned)((nxm + chunk - 1) / chunk));
-            k_mul2<<<grid, 128, 0, st_>>>(t1 ? x1.p() : nullptr, t1 ? x1.words() : 0,
-                                          t1 ? y1.p() : nullptr, t1 ? y1.words() : 0,
-                                          t2 ? x2.p() : nullptr, t2 ? x2.words() : 0,
-                                          t2 ? y2.p() : nullptr, t2 ? y2.words() : 0,
-                                          (unsigned long long *)r.p(), nout, chunk);
-            ckc(cudaGetLastError(), "k_mul2");
-            stats.school_mul2++;
+    // up to four sums x1*y1 + x2*y2 in one schoolbook launch (one zeroed
+    // buffer for all outputs); degrees of the results are bounds
+    struct Pair { const Poly *x1, *y1, *x2, *y2; };
+    void mul2_school(const Pair *jobs, int nj, Poly *outs) {
+        Mul2Jobs J;
+        memset(&J, 0, sizeof J);
+        u64 off[4], total = 0, nmax = 0, xmax = 0;
+        long long dm[4];
+        for (int z = 0; z < nj; z++) {
+            const Pair &P = jobs[z];
+            const bool t1 = P.x1->deg >= 0 && P.y1->deg >= 0;
+            const bool t2 = P.x2 && P.x2->deg >= 0 && P.y2->deg >= 0;
+            dm[z] = -1;
+            if (t1) dm[z] = std::max(dm[z], P.x1->deg + P.y1->deg);
+            if (t2) dm[z] = std::max(dm[z], P.x2->deg + P.y2->deg);
+            J.nout[z] = dm[z] < 0 ? 1 : (u64)(dm[z] >> 6) + 2;
+            off[z] = total;
+            total += J.nout[z];
+            if (t1) { J.x1[z] = P.x1->p(); J.nx1[z] = P.x1->words(); J.y1[z] = P.y1->p(); J.ny1[z] = P.y1->words(); }
+            if (t2) { J.x2[z] = P.x2->p(); J.nx2[z] = P.x2->words(); J.y2[z] = P.y2->p(); J.ny2[z] = P.y2->words(); }
+            nmax = std::max(nmax, J.nout[z]);
+            xmax = std::max(xmax, std::max(J.nx1[z], J.nx2[z]));
         }
-        r.deg = dmax;
-        return r;
-    }
-
-    // FFT form of mul2: transforms of the four operands, one pointwise
-    // multiply-add, one inverse transform, overlap-add
-    Poly fft_mul2(const Poly *x1, const Poly *y1, const Poly *x2, const Poly *y2, u64 nout) {
-        u64 need = 0;
-        auto chunks = [](const Poly *p) { return p ? ((u64)p->deg + 1 + 31) / 32 : 0; };
-        if (x1) need = std::max(need, chunks(x1) + chunks(y1) - 1);
-        if (x2) need = std::max(need, chunks(x2) + chunks(y2) - 1);
-        int m = 1;
-        while (((u64)1 << m) < need) m++;
-        gf2e_fft_plan *plan = gf2e::cached_plan(m);
-        if (!plan) throw Fail{GF2E_ERR_CUDA};
-        const u64 n = (u64)1 << m;
-        Buf F[4];
-        const Poly *ops[4] = {x1, y1, x2, y2};
-        for (int i = 0; i < 4; i++) {
-            if (!ops[i]) continue;
-            F[i] = alloc(n);
-            ck(gf2e::fft_fwd_packed(plan, F[i]->p, reinterpret_cast<const u32 *>(ops[i]->p()),
-                                    chunks(ops[i]), st_));
+        Poly all = zeros(total);
+        for (int z = 0; z < nj; z++) {
+            J.out[z] = (unsigned long long *)(all.p() + off[z]);
+            outs[z] = Poly();
+            outs[z].b = alias(all.b, off[z], J.nout[z]);
+            outs[z].deg = dm[z];
         }
-        u64 *f0 = F[0] ? F[0]->p : F[2]->p;
-        u64 *g0 = F[0] ? F[1]->p : F[3]->p;
-        k_pw_muladd<<<gf2e::grid_for(n, 256), 256, 0, st_>>>(
-            f0, f0, g0, (F[0] && F[2]) ? F[2]->p : nullptr, (F[0] && F[2]) ? F[3]->p : nullptr, n);
-        ckc(cudaGetLastError(), "k_pw_muladd");
-        ck(gf2e::fft_run(plan, false, f0, st_));
-        Poly r;
-        r.b = alloc(nout);
-        ck(gf2e::overlap_add(f0, need, r.p(), nout, st_));
-        stats.fft_mul2++;
-        return r;
+        const u64 chunk = 32;
+        dim3 grid((unsigned)((nmax / 2 + 1 + 127) / 128), (unsigned)std::max<u64>(1, (xmax + chunk - 1) / chunk),
+                  (unsigned)nj);
+        k_mul2<<<grid, 128, 0, st_>>>(J, chunk);
+        ckc(cudaGetLastError(), "k_mul2");
+        stats.school_mul2 += nj;
     }
 
     // (c, d) = M (a, b); exact degrees
@@ -683,8 +711,11 @@ public:
         if (std::max(M.e[0].deg + a.deg, M.e[1].deg + b.deg) + 1 > tn_.fft_bits) {
             fft_mat_vec(M, a, b, c, d);
         } else {
-            c = mul2(M.e[0], a, M.e[1], b);
-            d = mul2(M.e[2], a, M.e[3], b);
+            Pair P[2] = {{&M.e[0], &a, &M.e[1], &b}, {&M.e[2], &a, &M.e[3], &b}};
+            Poly o[2];
+            mul2_school(P, 2, o);
+            c = o[0];
+            d = o[1];
         }
         probe({&c, &d});
     }
@@ -737,9 +768,62 @@ public:
         if (M2.ident) return M1;
         if (M1.ident) return M2;
         Mat r;
+        long long dmax = 0;
         for (int i = 0; i < 2; i++)
             for (int j = 0; j < 2; j++)
-                r.e[2 * i + j] = mul2(M2.e[2 * i], M1.e[j], M2.e[2 * i + 1], M1.e[2 + j]);
+                dmax = std::max(dmax, std::max(M2.e[2 * i].deg + M1.e[j].deg,
+                                               M2.e[2 * i + 1].deg + M1.e[2 + j].deg));
+        if (dmax + 1 > tn_.fft_bits) return fft_mat_mul(M2, M1);
+        Pair P[4];
+        for (int i = 0; i < 2; i++)
+            for (int j = 0; j < 2; j++)
+                P[2 * i + j] = Pair{&M2.e[2 * i], &M1.e[j], &M2.e[2 * i + 1], &M1.e[2 + j]};
+        mul2_school(P, 4, r.e);
+        return r;
+    }
+
+    // FFT matrix x matrix: eight forward transforms, four inverse
+    Mat fft_mat_mul(const Mat &M2, const Mat &M1) {
+        auto chunks = [](const Poly &p) { return p.deg < 0 ? 0 : ((u64)p.deg + 1 + 31) / 32; };
+        u64 need = 1;
+        for (int i = 0; i < 2; i++)
+            for (int j = 0; j < 2; j++)
+                for (int k = 0; k < 2; k++) {
+                    const Poly &x = M2.e[2 * i + k], &y = M1.e[2 * k + j];
+                    if (x.deg >= 0 && y.deg >= 0) need = std::max(need, chunks(x) + chunks(y) - 1);
+                }
+        int m = 1;
+        while (((u64)1 << m) < need) m++;
+        gf2e_fft_plan *plan = gf2e::cached_plan(m);
+        if (!plan) throw Fail{GF2E_ERR_CUDA};
+        const u64 n = (u64)1 << m;
+        Buf F2[4], F1[4];
+        auto fwd = [&](const Poly &p, Buf &f) {
+            f = alloc(n);
+            if (p.deg < 0) ckc(cudaMemsetAsync(f->p, 0, n * 8, st_), "fft zero operand");
+            else ck(gf2e::fft_fwd_packed(plan, f->p, reinterpret_cast<const u32 *>(p.p()), chunks(p), st_));
+        };
+        for (int i = 0; i < 4; i++) { fwd(M2.e[i], F2[i]); fwd(M1.e[i], F1[i]); }
+        Mat r;
+        Buf O[4];
+        for (int i = 0; i < 2; i++)
+            for (int j = 0; j < 2; j++) {
+                Buf &o = O[2 * i + j];
+                o = alloc(n);
+                k_pw_muladd<<<gf2e::grid_for(n, 256), 256, 0, st_>>>(
+                    o->p, F2[2 * i]->p, F1[j]->p, F2[2 * i + 1]->p, F1[2 + j]->p, n);
+                ckc(cudaGetLastError(), "k_pw_muladd");
+                ck(gf2e::fft_run(plan, false, o->p, st_));
+                long long dm = std::max(M2.e[2 * i].deg + M1.e[j].deg,
+                                        M2.e[2 * i + 1].deg + M1.e[2 + j].deg);
+                Poly &out = r.e[2 * i + j];
+                if (dm < 0) { out.b = alloc(1); out.deg = -1; continue; }
+                const u64 nout = (u64)(dm >> 6) + 2;
+                out.b = alloc(nout);
+                ck(gf2e::overlap_add(o->p, need, out.p(), nout, st_));
+                out.deg = dm;
+            }
+        stats.fft_mul2 += 4;
         return r;
     }
 
@@ -785,9 +869,9 @@ public:
         if (d.deg < 0) throw Fail{gf2e::invalid("hgcd: division by zero")};
         u64 win[2];
         Poly cc = c;
-        probe({&cc, &d}, win);
-        u64 wc = win[0];
-        const u64 wd = win[1];
+        if (!c.has_win || !d.has_win) probe({&cc, &d}, win);
+        u64 wc = cc.win;
+        const u64 wd = d.win;
         Poly r0a, r0b;
         if (M) { r0a = M->e[0]; r0b = M->e[1]; }
         bool first = true;
@@ -833,7 +917,7 @@ public:
         const u64 W = (u64)(a.deg >> 6) + 2;
         const u64 mw = (u64)((a.deg - m) >> 6) + 3;
         Buf out = alloc(4 * mw);
-        const size_t smem = (4 * W + 8 * mw + 2 * W + 4 * mw) * 8;
+        const size_t smem = (4 * W + 8 * mw) * 8;
         {
             static std::mutex mu;
             static bool attr[64] = {false};
@@ -846,19 +930,11 @@ public:
                 attr[dev] = true;
             }
         }
+        // no round trip: statuses and counters accumulate on the device and
+        // are read once when the gcd is done (finish_bases)
         k_hgcd_base<<<1, BASE_THREADS, smem, st_>>>(a.p(), a.deg, b.p(), b.deg, m, W, mw, out->p,
-                                                    (BaseOut *)d_res_->p);
+                                                    (BaseAcc *)d_res_->p);
         ckc(cudaGetLastError(), "k_hgcd_base");
-        BaseOut res;
-        ckc(cudaMemcpyAsync(&res, d_res_->p, sizeof res, cudaMemcpyDeviceToHost, st_), "base read");
-        ckc(cudaStreamSynchronize(st_), "base sync");
-        if (res.status != GF2E_OK) {
-            gf2e::set_error("hgcd base case status %d", res.status);
-            throw Fail{res.status};
-        }
-        stats.base_rounds += res.rounds;
-        stats.cyc_serial += res.cyc_serial;
-        stats.cyc_total += res.cyc_total;
         Mat M;
         const long long dm = a.deg - m;       // entries have degree <= n - m
         for (int i = 0; i < 4; i++) {         // four views into the output buffer
@@ -982,6 +1058,7 @@ int run_one(const gf2e_gcd_job &j, int64_t *deg_out, gf2e_hgcd_stats *stats, cud
         Hgcd H(st, pool);
         Poly a = H.from_device(j.a_dev, j.abits), b = H.from_device(j.b_dev, j.bbits);
         Poly g = H.gcd(a, b);
+        H.finish_bases();
         *deg_out = g.deg < 0 ? 0 : g.deg;
         if (j.g_dev && j.g_cap_words) {
             const u64 gw = g.deg < 0 ? 0 : g.words();
