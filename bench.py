@@ -234,18 +234,15 @@ def main():
             dist.barrier()
         torch.cuda.synchronize()
 
+    from mersenne_trinomial_b200 import multi
+
     def max_over_ranks(x):
-        if not dist:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        return multi.max_over_ranks(x, dist, device="cuda")
 
     r, n, k = R, args.nstates, args.k
     nw = (r + 63) // 64
     stride = nw + (nw & 1)
-    rng = np.random.default_rng(1000 + rank)
-    s_host = rng.integers(3, r // 2, size=n).astype(np.uint64)
+    s_host = multi.rank_s_values(r, n, rank)             # disjoint seeded s per rank
     states = torch.empty(stride * n, dtype=torch.int64, device="cuda")
     scratch = torch.empty_like(states)
     s_dev = torch.from_numpy(s_host.view(np.int64)).cuda()
