@@ -446,6 +446,13 @@ def run_extras(torch, M, W, sq_rate=None):
                                                            block=mblk)
     out["deep_scan_r136279841_blocked"]["block_from"] = {"t_mul_s": t_mul, "t_sq_s": t_sq}
     out["deep_scan_r136279841_with_gcd"] = deep_scan_gcd_sample(M, block=32)
+    # gcd interval schedule for config 4 (k0 = 24, d <= 20000) from this run's
+    # per-degree cost (blocked) and amortised per-s gcd cost
+    g = out["deep_scan_r136279841_with_gcd"]
+    t_deg = out["deep_scan_r136279841_blocked"]["ms_per_degree_per_s"] / 1e3
+    ns = len(g["survivors"])
+    t_gcd = max(1e-3, g["wall_s"] - ns * (g["maxd"] - g["k0"]) * t_deg) / ns
+    out["config4_interval_choice"] = A.choose_interval(24, 20000, t_deg, t_gcd)
     out["serving"] = serving_sample()
     return out
 
