@@ -418,7 +418,7 @@ def run_extras(torch, M, W, sq_rate=None):
     # autotune the transform at the largest config-3 size (2^23 points), then
     # the same 64 products under the chosen settings
     from mersenne_trinomial_b200 import autotune as A
-    dflt = A.tune_default()
+    dflt = A.resolve_by_size(A.tune_default(), 23)
     t0 = time.perf_counter()
     tuned = A.fft_autotune(23, reps=2)
     tune_s = time.perf_counter() - t0

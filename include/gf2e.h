@@ -392,8 +392,8 @@ int gf2e_gcd_large(const gf2e_gcd_job *jobs, int njobs, int64_t *deg_host,
  * GF2E_FFT_BFLY_LV, GF2E_SIEVE_STRIP_LOG.
  * ====================================================================== */
 typedef struct gf2e_tune {
-    int fft_tile_log;    /* log2 elements per shared-memory tile, 11..13 */
-    int fft_cmin;        /* least contiguous columns per tile row: 1, 2, 4, 8, 16 */
+    int fft_tile_log;    /* log2 elements per shared-memory tile, 11..13; 0 = by size */
+    int fft_cmin;        /* least contiguous columns per tile row: 1, 2, 4, 8, 16; 0 = by size */
     int fft_taylor_lv;   /* Taylor levels fused per register stage, 1..3 */
     int fft_bfly_lv;     /* butterfly levels fused per register stage, 1..2 */
     int sieve_strip_log; /* log2 best[] entries per strip CTA, 10..14 */

@@ -42,6 +42,17 @@ def tune_get() -> dict:
     return t.as_dict()
 
 
+def resolve_by_size(tune: dict, m: int) -> dict:
+    """The FFT knobs a plan of size 2^m uses when they are 0 ("by size"),
+    the same rule as the library's plan creation."""
+    t = dict(tune)
+    if t["fft_tile_log"] == 0:
+        t["fft_tile_log"] = 11 if m <= 17 else (12 if m <= 21 else 13)
+    if t["fft_cmin"] == 0:
+        t["fft_cmin"] = 2 if m <= 17 else (4 if m <= 23 else 8)
+    return t
+
+
 def tune_set(**kw) -> dict:
     """Set some knobs (others keep their current value); returns the new tuning."""
     cur = tune_get()

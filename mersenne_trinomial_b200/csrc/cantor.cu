@@ -28,7 +28,7 @@ namespace {
 
 // shared-memory tiles are 2^11..2^13 elements (16..64 KB), chosen per plan
 constexpr int MAXOPS = 96;
-constexpr int FFT_THREADS = 512;           // 2 CTAs x 64 registers per SM
+constexpr int FFT_THREADS = 512;           // one CTA per SM, double-buffered tiles
 constexpr int NTWTAB = 4;                  // byte tables: t < 2^32
 
 enum OpType : u32 { TAY_F = 0, TAY_I = 1, BF_F = 2, BF_I = 3 };
@@ -170,11 +170,29 @@ struct Batch {
 // One pass over all tiles.  src32/nchunks: when non-null the tile is loaded
 // from 32-bit chunks of an operand (packing fused into the first pass),
 // zero beyond nchunks.
-template <int TL>
-__global__ void __launch_bounds__(FFT_THREADS, 2)
+// asynchronous 8-byte global -> shared copies (completion by group)
+GF2E_DEV void cp_async8(u64 *smem_dst, const u64 *gsrc) {
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(smem_dst);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(sa), "l"(gsrc) : "memory");
+}
+GF2E_DEV void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+GF2E_DEV void cp_async_wait_prev() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
+
+// One pass over all tiles.  src32/nchunks: when non-null the tile is loaded
+// from 32-bit chunks of an operand (packing fused into the first pass),
+// zero beyond nchunks.
+//
+// DB (large passes): each CTA runs over its tiles with two tile buffers in
+// shared memory, the next tile fetched with asynchronous copies while the
+// current one is transformed and stored, so HBM traffic overlaps the stage
+// work (the packing pass, which converts 32-bit chunks, loads
+// synchronously).  Without DB (passes with few tiles per CTA) one buffer,
+// synchronous loads and two CTAs per SM.
+template <int TL, bool DB>
+__global__ void __launch_bounds__(FFT_THREADS, DB ? 1 : 2)
 k_fft_pass(u64 *__restrict__ f, const u64 *__restrict__ tab, const Pass P, u64 ntiles,
            const u32 *__restrict__ src32, u64 nchunks, const Batch bt) {
-    extern __shared__ u64 sm[];
+    extern __shared__ u64 smbuf[];                   // one or two tiles of 2^TL elements
     __shared__ u32 s_off[MAXOPS * 16];               // per stage: srow(j << lg) << c_log
     __shared__ u32 s_loff[16];                       // load/store rows: srow(j << rs) << c_log
     f += (u64)blockIdx.y * bt.fstride;
@@ -200,45 +218,74 @@ k_fft_pass(u64 *__restrict__ f, const u64 *__restrict__ tab, const Pass P, u64 n
     if (threadIdx.x < 16) s_loff[threadIdx.x] = srow(threadIdx.x << rs) << P.c_log;
     __syncthreads();
     constexpr int EPT = (1 << TL) / FFT_THREADS;
-    constexpr int BATCH = EPT < 8 ? EPT : 8;
+    const u64 g_step = P.CH << rs;
 
-    for (u64 tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
-        u64 base;
-        if (P.wpt_log) {                             // several whole windows, C == CH
-            base = tile * ((u64)tile_elems);
-        } else {
-            u64 win = tile / cgroups, cg = tile - win * cgroups;
-            base = win * ((u64)NS * P.CH) + cg * C;
-        }
-        const u64 g_t = base + (u64)row_t * P.CH + col_t;       // fast path: element j = 0
-        const u64 g_step = P.CH << rs;
-        // load: every thread issues a batch of loads before the first use
+    auto tile_base = [&](u64 tile) -> u64 {
+        if (P.wpt_log) return tile * ((u64)tile_elems);       // several whole windows, C == CH
+        const u64 win = tile / cgroups, cg = tile - win * cgroups;
+        return win * ((u64)NS * P.CH) + cg * C;
+    };
+    // issue the loads of `tile` into buffer `sm` (asynchronous unless packing)
+    auto load_tile = [&](u64 tile, u64 *sm) {
+        const u64 base = tile_base(tile);
+        const u64 g_t = base + (u64)row_t * P.CH + col_t;
+        if (src32 || !DB) {
 #pragma unroll
-        for (int j0 = 0; j0 < EPT; j0 += BATCH) {
-            u64 v[BATCH];
+            for (int j0 = 0; j0 < EPT; j0 += 8) {
+                u64 v[8];
 #pragma unroll
-            for (int j = 0; j < BATCH; j++) {
-                const u32 e = threadIdx.x + (j0 + j) * FFT_THREADS;
-                v[j] = 0;
-                if (e < tile_elems) {
-                    const u64 g = fast ? g_t + (u64)(j0 + j) * g_step
-                                       : base + (u64)(e >> P.c_log) * P.CH + (e & (C - 1));
-                    if (src32) {
-                        v[j] = (g < nchunks) ? (u64)__ldg(src32 + g) : 0ull;
-                        if (g == 0) v[j] ^= bt.xor0;
-                    } else {
-                        v[j] = f[g];
+                for (int j = 0; j < 8; j++) {
+                    const u32 e = threadIdx.x + (j0 + j) * FFT_THREADS;
+                    v[j] = 0;
+                    if (j0 + j < EPT && e < tile_elems) {
+                        const u64 g = fast ? g_t + (u64)(j0 + j) * g_step
+                                           : base + (u64)(e >> P.c_log) * P.CH + (e & (C - 1));
+                        if (src32) {
+                            v[j] = (g < nchunks) ? (u64)__ldg(src32 + g) : 0ull;
+                            if (g == 0) v[j] ^= bt.xor0;
+                        } else {
+                            v[j] = f[g];
+                        }
                     }
                 }
-            }
 #pragma unroll
-            for (int j = 0; j < BATCH; j++) {
-                const u32 e = threadIdx.x + (j0 + j) * FFT_THREADS;
-                if (e < tile_elems)
-                    sm[fast ? (sb_t ^ s_loff[j0 + j]) : sidx(e >> P.c_log, e & (C - 1), P.c_log)] = v[j];
+                for (int j = 0; j < 8; j++) {
+                    const u32 e = threadIdx.x + (j0 + j) * FFT_THREADS;
+                    if (j0 + j < EPT && e < tile_elems)
+                        sm[fast ? (sb_t ^ s_loff[j0 + j]) : sidx(e >> P.c_log, e & (C - 1), P.c_log)] = v[j];
+                }
+            }
+        } else {
+#pragma unroll
+            for (int j = 0; j < EPT; j++) {
+                const u32 e = threadIdx.x + j * FFT_THREADS;
+                if (e < tile_elems) {
+                    if (fast) cp_async8(sm + (sb_t ^ s_loff[j]), f + g_t + (u64)j * g_step);
+                    else cp_async8(sm + sidx(e >> P.c_log, e & (C - 1), P.c_log),
+                                   f + base + (u64)(e >> P.c_log) * P.CH + (e & (C - 1)));
+                }
             }
         }
+        if (DB) cp_async_commit();
+    };
+
+    u64 tile = blockIdx.x;
+    if (DB) {
+        if (tile < ntiles) load_tile(tile, smbuf);
+        else cp_async_commit();
+    }
+    for (int it = 0; tile < ntiles; tile += gridDim.x, it++) {
+        u64 *sm = DB ? smbuf + ((it & 1) << TL) : smbuf;
+        if (DB) {
+            const u64 next = tile + gridDim.x;
+            if (next < ntiles) load_tile(next, smbuf + (((it + 1) & 1) << TL));
+            else cp_async_commit();                    // keep one group per iteration
+            cp_async_wait_prev();                      // this tile's copies are done
+        } else {
+            load_tile(tile, sm);
+        }
         __syncthreads();
+        const u64 base = tile_base(tile);
         for (u32 k = 0; k < P.nops; k++) {
             const u32 op = P.ops[k];
             const u32 type = op & 3, lg = (op >> 2) & 63, L = (op >> 8) & 127;
@@ -260,6 +307,7 @@ k_fft_pass(u64 *__restrict__ f, const u64 *__restrict__ tab, const Pass P, u64 n
             __syncthreads();
         }
         if (fast) {
+            const u64 g_t = base + (u64)row_t * P.CH + col_t;
 #pragma unroll
             for (int j = 0; j < EPT; j++) {
                 const u32 e = threadIdx.x + j * FFT_THREADS;
@@ -271,8 +319,9 @@ k_fft_pass(u64 *__restrict__ f, const u64 *__restrict__ tab, const Pass P, u64 n
                 f[base + (u64)row * P.CH + col] = sm[sidx(row, col, P.c_log)];
             }
         }
-        __syncthreads();
+        __syncthreads();                               // buffer free for the load after next
     }
+    if (DB) asm volatile("cp.async.wait_all;\n" ::: "memory");
 }
 
 __global__ void k_pack(const u32 *__restrict__ a32, u64 nchunks, u64 *__restrict__ F, u64 n) {
@@ -529,16 +578,26 @@ int run_passes(const PlanImpl &P, bool forward, u64 *f, const u32 *src32, u64 nc
     const auto &ps = forward ? P.fwd : P.inv;
     const auto &nt = forward ? P.ntiles_fwd : P.ntiles_inv;
     for (size_t i = 0; i < ps.size(); i++) {
-        u64 elems = (u64)1 << (ps[i].ns_log + ps[i].c_log + ps[i].wpt_log);
-        size_t smem = elems * sizeof(u64);
-        u64 per = std::max<u64>(1, (u64)gf2e::sm_count() * 8 / (u64)batch);
+        // many tiles per CTA: two tile buffers, one resident CTA per SM looping
+        // over its tiles; otherwise one buffer and up to eight CTAs per SM
+        const u64 sms = (u64)gf2e::sm_count();
+        const bool db = nt[i] * (u64)batch >= 4 * sms;
+        const size_t tile_bytes = ((size_t)1 << P.cfg.fft_tile_log) * sizeof(u64);
+        const size_t smem = db ? 2 * tile_bytes : tile_bytes;
+        const u64 per = std::max<u64>(1, (db ? sms : 8 * sms) / (u64)batch);
         dim3 grid((unsigned)std::min<u64>(nt[i], per), (unsigned)batch);
         const u32 *s32 = (i == 0) ? src32 : nullptr;
-        switch (P.cfg.fft_tile_log) {
-        case 11: k_fft_pass<11><<<grid, FFT_THREADS, smem, st>>>(f, P.tab, ps[i], nt[i], s32, nchunks, bt); break;
-        case 12: k_fft_pass<12><<<grid, FFT_THREADS, smem, st>>>(f, P.tab, ps[i], nt[i], s32, nchunks, bt); break;
-        default: k_fft_pass<13><<<grid, FFT_THREADS, smem, st>>>(f, P.tab, ps[i], nt[i], s32, nchunks, bt); break;
+#define GF2E_FFT_LAUNCH(T, D) \
+    k_fft_pass<T, D><<<grid, FFT_THREADS, smem, st>>>(f, P.tab, ps[i], nt[i], s32, nchunks, bt)
+        switch (P.cfg.fft_tile_log * 2 + (db ? 1 : 0)) {
+        case 22: GF2E_FFT_LAUNCH(11, false); break;
+        case 23: GF2E_FFT_LAUNCH(11, true); break;
+        case 24: GF2E_FFT_LAUNCH(12, false); break;
+        case 25: GF2E_FFT_LAUNCH(12, true); break;
+        case 26: GF2E_FFT_LAUNCH(13, false); break;
+        default: GF2E_FFT_LAUNCH(13, true); break;
         }
+#undef GF2E_FFT_LAUNCH
         GF2E_CHECK_LAUNCH("k_fft_pass");
     }
     return GF2E_OK;
@@ -571,18 +630,28 @@ static int allow_tile_smem() {
     int dev = 0;
     cudaGetDevice(&dev);
     if (dev >= 0 && dev < 64 && !done[dev]) {
-        cudaError_t e = cudaFuncSetAttribute(k_fft_pass<11>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             (1 << 11) * (int)sizeof(u64));
-        if (e == cudaSuccess)
-            e = cudaFuncSetAttribute(k_fft_pass<12>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (1 << 12) * (int)sizeof(u64));
-        if (e == cudaSuccess)
-            e = cudaFuncSetAttribute(k_fft_pass<13>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (1 << 13) * (int)sizeof(u64));
+        cudaError_t e = cudaSuccess;
+#define GF2E_FFT_ATTR(T, D, N)                                                              \
+    if (e == cudaSuccess)                                                                   \
+        e = cudaFuncSetAttribute(k_fft_pass<T, D>, cudaFuncAttributeMaxDynamicSharedMemorySize, \
+                                 (N) * (1 << T) * (int)sizeof(u64));
+        GF2E_FFT_ATTR(11, false, 1) GF2E_FFT_ATTR(11, true, 2)
+        GF2E_FFT_ATTR(12, false, 1) GF2E_FFT_ATTR(12, true, 2)
+        GF2E_FFT_ATTR(13, false, 1) GF2E_FFT_ATTR(13, true, 2)
+#undef GF2E_FFT_ATTR
         if (e != cudaSuccess) return cuda_status(e, "k_fft_pass smem attribute");
         done[dev] = true;
     }
     return GF2E_OK;
+}
+
+// knobs left at 0 take the size-dependent choice the autotuner makes on B200
+// (tiles of 2^11 / 2^12 / 2^13 elements up to m = 17 / 21 / above, at least
+// 2 / 4 / 8 contiguous columns up to m = 17 / 23 / above)
+gf2e_tune resolve_by_size(gf2e_tune c, int m) {
+    if (c.fft_tile_log == 0) c.fft_tile_log = m <= 17 ? 11 : (m <= 21 ? 12 : 13);
+    if (c.fft_cmin == 0) c.fft_cmin = m <= 17 ? 2 : (m <= 23 ? 4 : 8);
+    return c;
 }
 
 // plan whose passes read the caller's twiddle tables; no device allocation
@@ -595,7 +664,7 @@ int fft_plan_create_tables_cfg(int m, const u64 *tab_dev, const gf2e_tune &cfg,
     p->impl.m = m;
     p->impl.n = (u64)1 << m;
     p->impl.tab = tab_dev;
-    p->impl.cfg = cfg;
+    p->impl.cfg = resolve_by_size(cfg, m);
     build_passes(p->impl);
     *out = p;
     return GF2E_OK;

@@ -35,8 +35,8 @@ gf2e_tune g_tune;
 
 gf2e_tune builtin_default() {
     gf2e_tune t;
-    t.fft_tile_log = 13;             // autotuned on B200: best or within 2 % at m = 20..24
-    t.fft_cmin = 8;
+    t.fft_tile_log = 0;              // 0: by transform size (the autotuned B200 choices)
+    t.fft_cmin = 0;
     t.fft_taylor_lv = 3;
     t.fft_bfly_lv = 2;
     t.sieve_strip_log = 12;
@@ -46,8 +46,10 @@ gf2e_tune builtin_default() {
 bool pow2(int v) { return v > 0 && (v & (v - 1)) == 0; }
 
 const char *tune_problem(const gf2e_tune &t) {
-    if (t.fft_tile_log < 11 || t.fft_tile_log > 13) return "fft_tile_log outside 11..13";
-    if (!pow2(t.fft_cmin) || t.fft_cmin > 16) return "fft_cmin not one of 1, 2, 4, 8, 16";
+    if (t.fft_tile_log != 0 && (t.fft_tile_log < 11 || t.fft_tile_log > 13))
+        return "fft_tile_log not 0 (by size) or 11..13";
+    if (t.fft_cmin != 0 && (!pow2(t.fft_cmin) || t.fft_cmin > 16))
+        return "fft_cmin not 0 (by size) or one of 1, 2, 4, 8, 16";
     if (t.fft_taylor_lv < 1 || t.fft_taylor_lv > 3) return "fft_taylor_lv outside 1..3";
     if (t.fft_bfly_lv < 1 || t.fft_bfly_lv > 2) return "fft_bfly_lv outside 1..2";
     if (t.sieve_strip_log < 10 || t.sieve_strip_log > 14) return "sieve_strip_log outside 10..14";

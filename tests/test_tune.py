@@ -22,11 +22,12 @@ def model_cost(k0, maxd, t_deg, t_gcd, L0, Lmax):
 def test_tune_defaults_and_validation(engine):
     from mersenne_trinomial_b200 import autotune as A
     d = A.tune_default()
-    assert d == {"fft_tile_log": 13, "fft_cmin": 8, "fft_taylor_lv": 3, "fft_bfly_lv": 2,
+    assert d == {"fft_tile_log": 0, "fft_cmin": 0, "fft_taylor_lv": 3, "fft_bfly_lv": 2,
                  "sieve_strip_log": 12}
     saved = A.tune_get()
     try:
-        for bad in ({"fft_tile_log": 10}, {"fft_tile_log": 14}, {"fft_cmin": 3},
+        for bad in ({"fft_tile_log": 10}, {"fft_tile_log": 14}, {"fft_tile_log": -1},
+                    {"fft_cmin": 3}, {"fft_cmin": -2},
                     {"fft_cmin": 32}, {"fft_taylor_lv": 0}, {"fft_taylor_lv": 4},
                     {"fft_bfly_lv": 3}, {"sieve_strip_log": 9}, {"sieve_strip_log": 15}):
             with pytest.raises(engine.Gf2eError):
@@ -55,7 +56,7 @@ def test_tune_environment_overrides(engine):
                              "GF2E_SIEVE_STRIP_LOG": "13"})
     assert got["fft_tile_log"] == 11 and got["fft_bfly_lv"] == 1 and got["sieve_strip_log"] == 13
     got, err = _tune_in_child({"GF2E_FFT_TILE_LOG": "99"})
-    assert got["fft_tile_log"] == 13 and "ignoring" in err
+    assert got["fft_tile_log"] == 0 and "ignoring" in err
 
 
 @pytest.mark.parametrize("k0,maxd,t_deg,t_gcd", [
@@ -102,3 +103,13 @@ def test_choose_block_balances_squarings_and_modmuls(engine):
         assert cost(m) <= min(cost(k) for k in range(2, 63, 2)) * 1.05
     with pytest.raises(engine.Gf2eError):
         A.choose_block(0.0, 1.0)
+
+
+def test_resolve_by_size_rule():
+    from mersenne_trinomial_b200 import autotune as A
+    d = {"fft_tile_log": 0, "fft_cmin": 0, "fft_taylor_lv": 3, "fft_bfly_lv": 2,
+         "sieve_strip_log": 12}
+    assert A.resolve_by_size(d, 16)["fft_tile_log"] == 11
+    assert A.resolve_by_size(d, 20)["fft_tile_log"] == 12
+    assert A.resolve_by_size(d, 24) == dict(d, fft_tile_log=13, fft_cmin=8)
+    assert A.resolve_by_size(dict(d, fft_tile_log=12), 24)["fft_tile_log"] == 12
