@@ -437,6 +437,12 @@ int degree_step(gf2e_scanner &S, cudaStream_t st) {
 
 }  // namespace
 
+namespace gf2e {
+// the scanner's own stream: the serving loop runs independent scanners
+// concurrently by stepping each on its own stream
+cudaStream_t scanner_stream(gf2e_scanner *S) { return S ? S->own : nullptr; }
+}  // namespace gf2e
+
 extern "C" {
 
 int gf2e_scanner_footprint_blocked(uint64_t r, int slots, int block, size_t *bytes) {

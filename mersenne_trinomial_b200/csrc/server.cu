@@ -58,8 +58,18 @@ struct RClass {
 
 }  // namespace
 
+namespace gf2e {
+cudaStream_t scanner_stream(gf2e_scanner *S);
+}  // namespace gf2e
+
+namespace {
+
+}  // namespace
+
 struct gf2e_server {
     size_t budget = 0, used = 0;
+    cudaEvent_t ev_caller = nullptr;                 // caller's stream at the start of a step
+    std::vector<cudaEvent_t> ev_join;                // each scanner's stream at its end
     int slots = 64;
     int block = 1;                                   // blocked-DDF block size of the scanners
     uint64_t next_tag = 1;
@@ -184,6 +194,8 @@ int gf2e_server_create_blocked(size_t budget_bytes, int slots_per_r, int block,
 
 int gf2e_server_destroy(gf2e_server *S) {
     if (!S) return GF2E_OK;
+    if (S->ev_caller) cudaEventDestroy(S->ev_caller);
+    for (cudaEvent_t ev : S->ev_join) cudaEventDestroy(ev);
     for (auto &kv : S->rclass)
         if (kv.second.sc) gf2e_scanner_destroy(kv.second.sc);
     cudaFree(S->sieve_ws);
@@ -217,10 +229,32 @@ int gf2e_server_step(gf2e_server *S, int degrees, void *stream) {
     if (!S) return gf2e::invalid("null server");
     cudaStream_t st = (cudaStream_t)stream;
     GF2E_TRY(try_admit(*S, st));
+    // scanners of different r are independent: each steps on its own stream,
+    // after the caller's prior work, and the caller waits for all of them
+    if (!S->ev_caller) {
+        cudaError_t e = cudaEventCreateWithFlags(&S->ev_caller, cudaEventDisableTiming);
+        if (e != cudaSuccess) return gf2e::cuda_status(e, "server event");
+    }
+    cudaError_t e = cudaEventRecord(S->ev_caller, st);
+    if (e != cudaSuccess) return gf2e::cuda_status(e, "server stream order");
+    size_t nj = 0;
     for (auto it = S->rclass.begin(); it != S->rclass.end(); ++it) {
         RClass &rc = it->second;
         if (!rc.sc) continue;
-        GF2E_TRY(gf2e_scanner_step(rc.sc, degrees, st));
+        cudaStream_t own = gf2e::scanner_stream(rc.sc);
+        e = cudaStreamWaitEvent(own, S->ev_caller, 0);
+        if (e != cudaSuccess) return gf2e::cuda_status(e, "server stream order");
+        GF2E_TRY(gf2e_scanner_step(rc.sc, degrees, own));
+        if (nj == S->ev_join.size()) {
+            cudaEvent_t ev;
+            e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming);
+            if (e != cudaSuccess) return gf2e::cuda_status(e, "server event");
+            S->ev_join.push_back(ev);
+        }
+        e = cudaEventRecord(S->ev_join[nj], own);
+        if (e == cudaSuccess) e = cudaStreamWaitEvent(st, S->ev_join[nj], 0);
+        if (e != cudaSuccess) return gf2e::cuda_status(e, "server stream join");
+        nj++;
         for (;;) {
             int n = 0;
             GF2E_TRY(gf2e_scanner_poll(rc.sc, S->res.data(), S->tags.data(), S->masks.data(),

@@ -78,25 +78,23 @@ BAD_R = {127, 151, 241, 257, 337, 8191, 131071, 178481, 524287}
 
 def job_stream(seed: int, n_jobs: int, rate: float, deep_max: int = 2000,
                s_lo: int = 16, s_hi: int = 256):
-    """Seeded Poisson arrivals.  r from {~1e5, ~1e6, ~1e7, 136279841} (seeded
-    primes = +-1 mod 8 that the sieve supports, apart from the last); s-sets of
-    s_lo..s_hi values; d-range 2..24 (sieve only) or, for r ~1e5 / ~1e6, up to
-    2..deep_max (squaring + gcd)."""
+    """Seeded Poisson arrivals.  r from the set {~1e5, ~1e6, ~1e7, 136279841}
+    (one seeded prime = +-1 mod 8 that the sieve supports near each of the
+    first three); s-sets of s_lo..s_hi values; d-range 2..24 (sieve only) or,
+    for r ~1e5 / ~1e6, up to 2..deep_max (squaring + gcd).  Jobs with the same
+    r share that r's resident scanner."""
     rng = np.random.default_rng(seed)
-    pools = {}
+    rset = {}
     for name, near in R_CLASSES.items():
         cands = [p for p in W.primes_pm1_mod8(near - 3000, near + 3000)
                  if p not in BAD_R and W.sieve_compatible(p, 24)]
-        pools[name] = cands
+        rset[name] = int(cands[int(rng.integers(len(cands)))])
     t = 0.0
     jobs = []
     for i in range(n_jobs):
         t += rng.exponential(1.0 / rate)
         cls = rng.choice(["1e5", "1e6", "1e7", "deep"])
-        if cls == "deep":
-            r = W.R_DEEP
-        else:
-            r = int(pools[cls][int(rng.integers(len(pools[cls])))])
+        r = W.R_DEEP if cls == "deep" else rset[cls]
         ns = int(rng.integers(s_lo, s_hi + 1))
         s = np.unique(rng.integers(3, r // 2, size=ns)).astype(np.uint64)
         deep_ok = r < 2_000_000
