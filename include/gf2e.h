@@ -69,7 +69,10 @@ int gf2e_sieve_workspace_size(int dmax, size_t *bytes);
 /* best_dev[0..smax] = UINT64_MAX (coarse_sieve.cu k_fill 301-305). */
 int gf2e_sieve_fill(uint64_t *best_dev, uint64_t smax, void *stream);
 
-/* Sieve degrees dmin..dmax (2 <= dmin <= dmax <= 24) into best_dev.
+/* Sieve degrees dmin..dmax (2 <= dmin <= dmax <= 31) into best_dev.  The
+ * workspace holds dense antilog/log tables of 2^dmax entries (2 x 8 GB at
+ * d = 31); the reference switches to bucketed tables beyond its GPU memory
+ * (coarse_sieve.cu:920-1117).
  * Host-side per-degree setup (primitive polynomial search) is cached.
  * Returns GF2E_ERR_UNSUPPORTED_R when gcd(r mod (2^d-1), 2^d-1) != 1 for
  * some d in range, before launching anything.  All degrees are enqueued on
@@ -80,7 +83,7 @@ int gf2e_sieve_run(uint64_t r, int dmin, int dmax, uint64_t smax,
                    size_t workspace_bytes, void *stream);
 
 /* Read back per-degree statistics of the last gf2e_sieve_run on this
- * workspace (sized for `dmax`): coset classes and marks, arrays of 25
+ * workspace (sized for `dmax`): coset classes and marks, arrays of dmax + 1
  * entries indexed by d (sieve_ref.cpp:128-132 prints the same counts).
  * Synchronizes `stream`. */
 int gf2e_sieve_stats(const void *workspace_dev, int dmax, uint64_t *classes_host,

@@ -1,5 +1,11 @@
 // sieve.cu -- Zech-log sieve for the smallest irreducible factor of degree
-// d <= 24 of x^r + x^s + 1, for every s in [1, smax] at once.
+// d <= 31 of x^r + x^s + 1, for every s in [1, smax] at once.
+//
+// Degrees up to 31 keep every field element and modulus in 32 bits.  The
+// reference needs bucketed low-memory tables beyond d = 29 on its 8 GB GPU
+// (coarse_sieve.cu:920-1117, gf2_wide_field.h); on a B200 the dense antilog
+// and log tables of d = 31 (2 x 8 GB) fit in HBM, so every degree uses the
+// same dense path.
 //
 // Number theory (the reference's, sieve_ref.cpp:8-26): in GF(2^d) built on
 // the smallest primitive q_d (x generates the group of order M = 2^d - 1), an
@@ -12,7 +18,7 @@
 // B200 mapping:
 //   k_tables    antilog A[i] = x^i (a multiply-by-x chain per 32 entries) and
 //               the log scatter L[A[i]] = i in the same pass (tables are
-//               L2-resident up to d = 23: 2 x 32 MB).
+//               L2-resident up to d = 23: 2 x 32 MB, 2 x 8 GB at d = 31).
 //   k_classes   one thread per j: coset/subfield filters, Zech lookup,
 //               progression; the minimal polynomial only for classes that
 //               mark some s <= smax, by GF(2) elimination on the powers
@@ -35,7 +41,7 @@
 
 namespace {
 
-constexpr int DMAX = 24;
+constexpr int DMAX = 31;
 constexpr int STRIP_LOG_MAX = 14;         // strip CTAs own 2^10..2^14 entries of best[]
                                           // (8..128 KB of shared memory), tunable
 constexpr u64 INLINE = 32;                // marks done inline by the class thread
@@ -67,7 +73,7 @@ Layout layout_for(int dmax) {
     return l;
 }
 
-// ---- small field GF(2^d), d <= 24, modulus q (bit d set)
+// ---- small field GF(2^d), d <= 31, modulus q (bit d set)
 GF2E_DEV u32 sf_mul(u32 a, u32 b, u32 q, int d) {
     u64 t = clmul32(a, b);
     for (int bit = 2 * d - 2; bit >= d; bit--)
@@ -431,7 +437,7 @@ int gf2e_sieve_stats(const void *workspace, int dmax, uint64_t *classes_host,
                                     cudaMemcpyDeviceToHost, st);
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);
     if (e != cudaSuccess) return gf2e::cuda_status(e, "sieve stats");
-    for (int d = 0; d <= DMAX; d++) {
+    for (int d = 0; d <= dmax; d++) {
         if (classes_host) classes_host[d] = c.classes[d];
         if (marks_host) marks_host[d] = c.marks[d];
     }

@@ -11,10 +11,11 @@
 //   <prefix>.survivors.txt  s with no factor of degree <= depth, one per line
 //   <prefix>.found.cert     "s d p<hex>" ascending s (default on)
 //   <prefix>.found.bin      LE u64 key per s = 1..smax, UINT64_MAX = none (--found)
-// Checkpoint flags (--checkpoint, --checkpoint-mins, --checkpoint-keep,
-// --resume) are accepted and ignored with a note: degrees <= 24 finish in
-// milliseconds, so there is nothing to resume.  Degrees above 24 (the
-// reference's bucketed low-memory and wide-field modes) are refused.
+// Degrees up to 31 run on dense tables in HBM (the reference needs its
+// bucketed low-memory mode beyond d = 29 on an 8 GB GPU).  Checkpoint flags
+// (--checkpoint, --checkpoint-mins, --checkpoint-keep, --resume) are
+// accepted and ignored with a note: the whole run finishes in seconds.
+// Degrees above 31 (the reference's wide-field mode) are refused.
 #include <cinttypes>
 #include <cstdio>
 #include <cstdlib>
@@ -55,7 +56,7 @@ static void run_gpu(u64 r, int depth, u64 smax, int min_depth, std::vector<u64> 
     die_on(gf2e_sieve_run(r, min_depth, depth, smax, (u64 *)dbest, ws, ws_bytes, nullptr),
            "sieve");
     double t1 = now_s();
-    u64 classes[25], marks[25];
+    u64 classes[32], marks[32];
     die_on(gf2e_sieve_stats(ws, depth, classes, marks, nullptr), "stats");
     for (int d = min_depth; d <= depth; d++)
         fprintf(stderr, "d=%2d done: %" PRIu64 " classes, %" PRIu64 " marks\n", d, classes[d],
@@ -109,7 +110,7 @@ static int selftest() {
     for (u64 s = 1; s <= smax; s++)
         if (a[s] != b[s] && ++bad <= 10)
             fprintf(stderr, "MISMATCH s=%" PRIu64 "\n", s);
-    // divisibility: x^r + x^s + 1 == 0 mod p for the reported p (d <= 24)
+    // divisibility: x^r + x^s + 1 == 0 mod p for the reported p (d <= 20 here)
     for (u64 s = 1; s <= smax; s++) {
         if (a[s] == ~0ULL) continue;
         nf++;
@@ -140,7 +141,7 @@ static int selftest() {
 int main(int argc, char **argv) {
     if (argc >= 2 && !strcmp(argv[1], "--selftest")) return selftest();
     if (argc >= 2 && !strcmp(argv[1], "--selftest-lowmem")) {
-        fprintf(stderr, "note: the bucketed low-memory mode is not needed for d <= 24; "
+        fprintf(stderr, "note: the bucketed low-memory mode is not needed for d <= 31; "
                         "running the standard selftest\n");
         return selftest();
     }
@@ -182,14 +183,14 @@ int main(int argc, char **argv) {
         else if ((!strcmp(argv[a], "--checkpoint") || !strcmp(argv[a], "--checkpoint-mins") ||
                   !strcmp(argv[a], "--checkpoint-keep") || !strcmp(argv[a], "--resume") ||
                   !strcmp(argv[a], "--gpus")) && a + 1 < argc) {
-            fprintf(stderr, "note: %s %s ignored (one GPU; degrees <= 24 need no checkpoint)\n",
+            fprintf(stderr, "note: %s %s ignored (one GPU; degrees <= 31 need no checkpoint)\n",
                     argv[a], argv[a + 1]);
             a++;
         } else fprintf(stderr, "warning: ignoring unknown argument '%s'\n", argv[a]);
     }
     if (min_depth < 2) min_depth = 2;
-    if (depth > 24) {
-        fprintf(stderr, "depth %d > 24 is not supported by this engine (dense tables only)\n",
+    if (depth > 31) {
+        fprintf(stderr, "depth %d > 31 is not supported by this engine (dense tables only)\n",
                 depth);
         return 1;
     }

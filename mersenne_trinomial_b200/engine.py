@@ -121,8 +121,8 @@ class SieveWorkspace:
         self.buf = DeviceBuffer(n.value)
 
     def stats(self, stream=None):
-        cls = np.zeros(25, dtype=np.uint64)
-        mk = np.zeros(25, dtype=np.uint64)
+        cls = np.zeros(self.dmax + 1, dtype=np.uint64)
+        mk = np.zeros(self.dmax + 1, dtype=np.uint64)
         call("gf2e_sieve_stats", self.buf.ptr, self.dmax, cls.ctypes.data, mk.ctypes.data,
              _sp(stream))
         return cls, mk

@@ -51,8 +51,9 @@ def gen_sieve():
         out["cases"].append({"r": c["r"], "depth": c["dmax"], "smax": c["smax"], "file": name,
                              "lines": txt.count("\n"), "sha256": sha(txt.encode())})
     # the reference GPU selftest configuration and the reference CPU selftests
+    # (d <= 27 at r = 136279841: about 3 minutes of the reference CPU sieve)
     for r, depth, smax in [(136279841, 20, 999999), (136279841, 11, 30000),
-                           (74207281, 10, 20000), (101, 9, 100)]:
+                           (74207281, 10, 20000), (101, 9, 100), (136279841, 27, 999999)]:
         txt = run([os.path.join(REF, "sieve_ref"), "run", str(r), str(depth), str(smax)]).stdout
         out["cases"].append({"r": r, "depth": depth, "smax": smax, "file": None,
                              "lines": txt.count("\n"), "sha256": sha(txt.encode()),
