@@ -372,6 +372,21 @@ def run_extras(torch, M, W, sq_rate=None):
     ms = _ev_time(torch, run, 3, flush)
     out["sieve_r136279841_d24"] = {"pairs_per_s": smax * 23 / (ms / 1e3), "ms": ms,
                                    "pairs": smax * 23}
+    # the reference's published full-range run: d <= 29 (7.52 s on its GPU,
+    # coarse_sieve.log:9-40) and the dense-table limit d <= 31
+    for dmax in (29, 31):
+        wsd = M.engine.SieveWorkspace(dmax)
+        rund = lambda: M.sieve_device(R, dmax, smax, best, workspace=wsd)
+        rund()
+        ms = _ev_time(torch, rund, 3)
+        out[f"sieve_r136279841_d{dmax}"] = {"pairs_per_s": smax * (dmax - 1) / (ms / 1e3),
+                                            "ms": ms, "pairs": smax * (dmax - 1)}
+        if dmax == 29:
+            h = best[1:].cpu().numpy().view(np.uint64)
+            surv = int(np.count_nonzero(h == np.uint64(0xFFFFFFFFFFFFFFFF)))
+            out["sieve_r136279841_d29"].update({"survivors": surv, "factors": smax - surv,
+                                                "reference_published_s": 7.52})
+        del wsd
     # config 1: r in [40000, 50000], d <= 20
     c1 = W.sieve_config(1)
     best1 = torch.empty(c1["smax"] + 1, dtype=torch.int64, device="cuda")
