@@ -13,6 +13,8 @@
 #   oracle/_ref/libref_cantor.so      gf2x_fft_mul & friends behind a C ABI
 #   oracle/_ref/trinomial_stage2_emul trinomial_stage2.cu kernels run on CPU
 #   oracle/_ref/trinomial_scan_emul   trinomial_scan.cu (naive gcd) on CPU
+#   oracle/_ref/cert2bin, bin2cert,   certificate <-> found.bin converters and
+#   oracle/_ref/check_ref             the sieve-vs-reference cross-check
 #
 # Flags: the reference uses -O2 -march=native; we use -O2 with PCLMUL/SSE4
 # enabled but no host-specific ISA so the binaries also run on the GPU
@@ -32,6 +34,9 @@ FLAGS="-O2 -mpclmul -msse4.1 -w"
 "$CXX" $FLAGS -I"$REF" -o "$OUT/sieve_ref" "$REF/sieve_ref.cpp"
 "$CXX" $FLAGS -I"$REF" -o "$OUT/cantor_ref" "$REF/cantor_ref.cpp"
 "$CXX" $FLAGS -fPIC -shared -I"$REF" -o "$OUT/libref_cantor.so" "$HERE/ref_cantor_driver.cpp"
+"${CC:-gcc}" -O2 -w -o "$OUT/cert2bin" "$REF/cert2bin.c"
+"${CC:-gcc}" -O2 -w -o "$OUT/bin2cert" "$REF/bin2cert.c"
+"$CXX" $FLAGS -o "$OUT/check_ref" "$REF/check_ref.cpp"
 
 TMP="$(mktemp -d /tmp/gf2e_refemul.XXXXXX)"
 trap 'rm -rf "$TMP"' EXIT

@@ -1,0 +1,114 @@
+"""Certificate formats: cert2bin / bin2cert / check_ref (the reference's
+cert2bin.c, bin2cert.c, check_ref.cpp) against the reference's own tools
+built from its sources, on a sieve certificate from the oracle.  Host-only
+tools: no GPU."""
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+from conftest import ROOT
+
+BIN = os.path.join(ROOT, "mersenne_trinomial_b200", "bin")
+REF = os.path.join(ROOT, "oracle", "_ref")
+
+
+def _need(*paths):
+    for p in paths:
+        if not os.path.exists(p):
+            pytest.skip(f"{p} not built")
+
+
+@pytest.fixture(scope="module")
+def image(oracle, tmp_path_factory):
+    """found.bin of the oracle sieve at r = 44687, d <= 20 (s = 1..22343)."""
+    best = oracle.sieve(44687, 20, 22343)
+    d = tmp_path_factory.mktemp("certs")
+    path = d / "f.found.bin"
+    np.ascontiguousarray(best[1:], dtype="<u8").tofile(path)
+    return d, path, best
+
+
+def _run(cmd, **kw):
+    return subprocess.run([str(c) for c in cmd], capture_output=True, text=kw.pop("text", True),
+                          timeout=120, **kw)
+
+
+def test_bin2cert_matches_reference(image):
+    _need(os.path.join(BIN, "bin2cert"), os.path.join(REF, "bin2cert"))
+    _, path, best = image
+    ours = _run([os.path.join(BIN, "bin2cert"), path])
+    ref = _run([os.path.join(REF, "bin2cert"), path])
+    assert ours.returncode == ref.returncode == 0
+    assert ours.stdout == ref.stdout
+    assert ours.stdout.count("\n") == best.size - 1
+
+
+@pytest.mark.parametrize("limit", [20, 12, 47, 0])
+def test_cert2bin_matches_reference(image, limit):
+    _need(os.path.join(BIN, "cert2bin"), os.path.join(REF, "cert2bin"))
+    d, path, best = image
+    cert = d / "f.cert"
+    cert.write_text(_run([os.path.join(REF, "bin2cert"), path]).stdout)
+    a, b = d / f"ours{limit}.bin", d / f"ref{limit}.bin"
+    ro = _run([os.path.join(BIN, "cert2bin"), cert, a, limit])
+    rr = _run([os.path.join(REF, "cert2bin"), cert, b, limit])
+    assert ro.returncode == rr.returncode == 0
+    assert a.read_bytes() == b.read_bytes()
+    if limit >= 20:                             # round trip to the image
+        assert a.read_bytes() == path.read_bytes()
+
+
+@pytest.mark.parametrize("corrupt", ["order", "bits", "hex"])
+def test_cert2bin_rejects_what_the_reference_rejects(image, corrupt):
+    _need(os.path.join(BIN, "cert2bin"), os.path.join(REF, "cert2bin"))
+    d, path, _ = image
+    lines = _run([os.path.join(REF, "bin2cert"), path]).stdout.splitlines()
+    i = next(k for k, l in enumerate(lines) if " p" in l and k > 10)
+    s, deg, mask = lines[i].split()
+    if corrupt == "order":
+        lines[i] = f"{int(s) + 1} {deg} {mask}"
+    elif corrupt == "bits":
+        lines[i] = f"{s} {int(deg) + 1} {mask}"
+    else:
+        lines[i] = f"{s} {deg} {mask}z"
+    cert = d / f"bad_{corrupt}.cert"
+    cert.write_text("\n".join(lines) + "\n")
+    ro = _run([os.path.join(BIN, "cert2bin"), cert, d / "o.bin", 40])
+    rr = _run([os.path.join(REF, "cert2bin"), cert, d / "r.bin", 40])
+    assert ro.returncode != 0 and rr.returncode != 0
+
+
+def _summary(out):
+    return [l for l in out.splitlines() if l.startswith(("  ", "reference lines", "sieve input",
+                                                          "ALL CHECKS", "*** DISCREP"))]
+
+
+@pytest.mark.parametrize("plant", [None, "mask", "survivor", "extra"])
+def test_check_ref_matches_reference(image, plant):
+    _need(os.path.join(BIN, "check_ref"), os.path.join(REF, "check_ref"))
+    d, path, best = image
+    cert = _run([os.path.join(REF, "bin2cert"), path]).stdout.splitlines()
+    facts = [l for l in cert if " p" in l]
+    surv = [l.split()[0] for l in cert if l.endswith(" u")]
+    ref_lines = [l for l in facts if 14 <= int(l.split()[1]) <= 20]
+    sieve = list(facts)
+    if plant == "mask":                          # a wrong polynomial
+        k = next(i for i, l in enumerate(sieve) if int(l.split()[1]) == 17)
+        s_, d_, m_ = sieve[k].split()
+        sieve[k] = f"{s_} {d_} p{int(m_[1:], 16) ^ 2:x}"
+    elif plant == "survivor":                    # a factor lost
+        k = next(i for i, l in enumerate(sieve) if int(l.split()[1]) == 19)
+        surv.append(sieve.pop(k).split()[0])
+    elif plant == "extra":                       # a factor the reference lacks
+        ref_lines = [l for l in ref_lines if int(l.split()[1]) != 15]
+    (d / "ref.txt").write_text("\n".join(ref_lines) + "\n")
+    (d / "sieve.cert").write_text("\n".join(sieve) + "\n")
+    (d / "surv.txt").write_text("\n".join(surv) + "\n")
+    args = ["--ref", d / "ref.txt", "--dmin", 14, "--dmax", 20, "--cert", d / "sieve.cert",
+            "--survivors", d / "surv.txt", "--smax", best.size - 1]
+    ro = _run([os.path.join(BIN, "check_ref")] + args)
+    rr = _run([os.path.join(REF, "check_ref")] + args)
+    assert ro.returncode == rr.returncode == (0 if plant is None else 1)
+    assert _summary(ro.stdout) == _summary(rr.stdout)
