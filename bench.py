@@ -426,9 +426,26 @@ def run_extras(torch, M, W, sq_rate=None):
     tot_bits = sum(ab + bb for ab, bb in c3["sizes"])
     bytes3 = sum(48 * (1 << M.engine.fft_m_for(ab, bb)) + (ab + bb) // 4 for ab, bb in c3["sizes"])
     peak = measured_peaks()[0]
+
+    def pass_bytes():
+        # bytes the tile passes must move: each forward/inverse pass reads and
+        # writes the n points once (two forwards and one inverse per product),
+        # plus the 48 n of packing, pointwise product and overlap-add
+        tot = 0
+        for ab, bb in c3["sizes"]:
+            m = M.engine.fft_m_for(ab, bb)
+            F = M.CudaFFT()
+            F.init(m)
+            f, i = F.passes()
+            F.fini()
+            tot += 16 * (1 << m) * (2 * f + i) + 48 * (1 << m) + (ab + bb) // 4
+        return tot
+    pb3 = pass_bytes()
     out["mul_config3"] = {"products_per_s": 64 / (ms / 1e3), "ms": ms,
                           "algorithmic_GBps": bytes3 / (ms / 1e3) / 1e9,
                           "frac_of_measured_hbm": bytes3 / (ms / 1e3) / 1e9 / peak,
+                          "pass_GBps": pb3 / (ms / 1e3) / 1e9,
+                          "pass_frac_of_measured_hbm": pb3 / (ms / 1e3) / 1e9 / peak,
                           "operand_bits": tot_bits, "tuning": "built-in default"}
     # autotune the transform at the largest config-3 size (2^23 points), then
     # the same 64 products under the chosen settings
@@ -441,10 +458,13 @@ def run_extras(torch, M, W, sq_rate=None):
     dflt_row = [c for c in tuned["candidates"]
                 if all(c[k] == dflt[k] for k in ("fft_tile_log", "fft_cmin", "fft_taylor_lv",
                                                   "fft_bfly_lv"))]
+    pb3t = pass_bytes()
     out["mul_config3_tuned"] = {
         "products_per_s": 64 / (ms_t / 1e3), "ms": ms_t,
         "algorithmic_GBps": bytes3 / (ms_t / 1e3) / 1e9,
         "frac_of_measured_hbm": bytes3 / (ms_t / 1e3) / 1e9 / peak,
+        "pass_GBps": pb3t / (ms_t / 1e3) / 1e9,
+        "pass_frac_of_measured_hbm": pb3t / (ms_t / 1e3) / 1e9 / peak,
         "tuning": {k: v for k, v in tuned["best"].items() if k.startswith("fft_")},
         "autotune_s": tune_s, "candidates_verified": len(tuned["candidates"]),
         "fwd_inv_ms_m23": {"tuned": tuned["best_fwd_inv_ms"],

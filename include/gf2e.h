@@ -149,6 +149,9 @@ int gf2e_cantor_basis(uint64_t *basis64, int *len);
 int gf2e_fft_plan_create(int m, gf2e_fft_plan **plan);
 int gf2e_fft_plan_destroy(gf2e_fft_plan *plan);
 int gf2e_fft_plan_m(const gf2e_fft_plan *plan);
+/* Tile passes of the forward and inverse transform (each reads and writes
+ * the n points once): the memory traffic a transform of this plan needs. */
+int gf2e_fft_plan_passes(const gf2e_fft_plan *plan, int *fwd, int *inv);
 
 /* In-place forward / inverse transform of n device words (CudaFFT::fwd/inv). */
 int gf2e_fft_fwd(const gf2e_fft_plan *plan, uint64_t *f_dev, void *stream);

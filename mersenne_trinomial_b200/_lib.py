@@ -141,6 +141,7 @@ SIGNATURES = {
     "gf2e_trin_reduce_T0": (_i32, [_vp, _vp, _u64, _vp]),
     "gf2e_trin_accumulate": (_i32, [_vp, _vp]),
     "gf2e_gcd_large": (_i32, [_vp, _i32, _vp, _i32, _P(HgcdStats), _vp]),
+    "gf2e_fft_plan_passes": (_i32, [_vp, _P(_i32), _P(_i32)]),
     "gf2e_tune_default": (_i32, [_P(Tune)]),
     "gf2e_tune_get": (_i32, [_P(Tune)]),
     "gf2e_tune_set": (_i32, [_P(Tune)]),

@@ -821,6 +821,13 @@ int gf2e_fft_plan_destroy(gf2e_fft_plan *plan) {
 
 int gf2e_fft_plan_m(const gf2e_fft_plan *plan) { return plan ? plan->impl.m : -1; }
 
+int gf2e_fft_plan_passes(const gf2e_fft_plan *plan, int *fwd, int *inv) {
+    if (!plan) return gf2e::invalid("null plan");
+    if (fwd) *fwd = (int)plan->impl.fwd.size();
+    if (inv) *inv = (int)plan->impl.inv.size();
+    return GF2E_OK;
+}
+
 int gf2e_fft_fwd(const gf2e_fft_plan *plan, uint64_t *f_dev, void *stream) {
     if (!plan || !f_dev) return gf2e::invalid("gf2e_fft_fwd: null argument");
     return gf2e::fft_run(plan, true, f_dev, (cudaStream_t)stream);

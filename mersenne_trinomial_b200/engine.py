@@ -218,6 +218,12 @@ class CudaFFT:
     def inv(self, buf, stream=None) -> None:
         call("gf2e_fft_inv", self.plan, _ptr(buf), _sp(stream))
 
+    def passes(self) -> tuple:
+        """(forward, inverse) tile passes of this plan."""
+        f, i = C.c_int(), C.c_int()
+        call("gf2e_fft_plan_passes", self.plan, C.byref(f), C.byref(i))
+        return f.value, i.value
+
     def twiddles(self) -> np.ndarray:
         W = np.zeros(max(1, self.n >> 1), dtype=np.uint64)
         call("gf2e_fft_twiddles", self.plan, W.ctypes.data)
