@@ -53,6 +53,13 @@ def build_lib(verbose: bool = False) -> str:
                 print("nvcc", os.path.basename(cu), flush=True)
             _run([NVCC] + NVFLAGS + ["-dc", "-o", obj, cu])
         objs.append(obj)
+    for cpp in sorted(glob.glob(os.path.join(CSRC, "*.cpp"))):
+        obj = os.path.join(BUILD, os.path.basename(cpp) + ".o")
+        if _newer([cpp] + headers + glob.glob(os.path.join(CSRC, "*.h")), obj):
+            if verbose:
+                print("g++", os.path.basename(cpp), flush=True)
+            _run(["g++", "-O2", "-std=c++17", "-fPIC", "-c", "-o", obj, cpp])
+        objs.append(obj)
     if _newer(objs, LIB):
         _run([NVCC] + ARCH + ["-shared", "-o", LIB] + objs + ["-lcudart"])
     return LIB

@@ -27,6 +27,7 @@
 // (squarings and multiplications by x only); it is then advanced by k0 + 1
 // Frobenius steps.
 #include "gf2e_internal.cuh"
+#include "polyhost.h"
 
 #include <algorithm>
 #include <deque>
@@ -48,8 +49,6 @@ int pointwise(u64 *fa, const u64 *fb, u64 n, cudaStream_t st);
 int mul_fft_m(u64 abits, u64 bbits);
 gf2e_fft_plan *cached_plan(int m);
 u64 fft_plan_n(const gf2e_fft_plan *plan);
-bool resolve_factor(const std::vector<u64> &g, u64 kmin, u64 kmax, u64 &d_out,
-                    std::vector<u64> &mask);
 }  // namespace gf2e
 
 struct gf2e_scanner {
@@ -401,7 +400,11 @@ int degree_step(gf2e_scanner &S, cudaStream_t st) {
                     if (e != cudaSuccess) return gf2e::cuda_status(e, "gcd readback");
                     std::vector<u64> g(S.ghost.begin(), S.ghost.end());
                     u64 d = 0;
-                    if (gf2e::resolve_factor(g, sl.iv + 1, sl.k, d, D.mask)) {
+                    // the clear intervals (k0, iv] exclude every factor degree
+                    // up to iv once iv >= 2 k0: each d <= k0 has a multiple in
+                    // (k0, 2 k0], so a factor of degree d would have hit there
+                    const u64 clean = sl.iv >= 2 * sl.job.k0 ? sl.iv : 0;
+                    if (gf2e::hostpoly::least_factor(g, clean, sl.k, d, D.mask)) {
                         D.res.status = 1;
                         D.res.d = d;
                         D.res.mask_words = D.mask.size();
