@@ -267,6 +267,39 @@ int gf2e_scan_blocked(uint64_t r, const uint64_t *s_host, int ns, uint64_t k0, u
                       gf2e_scan_result *results_host, uint64_t *masks_host,
                       size_t mask_cap_words, void *stream);
 
+/* Interval schedules: the cadence of interval gcds (results do not depend
+ * on it, only the cost does).
+ *   GF2E_SCHED_DOUBLING  L0, 2 L0, 4 L0, ... capped at Lmax degrees
+ *                        (trinomial_scan --l0/--interval; the default)
+ *   GF2E_SCHED_LINEAR    q0, 2 q0, 3 q0, ... blocks (tsfactor's QSched,
+ *                        tsfactor.cu:831-858, --q0)
+ *   GF2E_SCHED_OPT       tsfactor's Euler-optimal widths for a gcd that
+ *                        costs G degrees of scanning, geometric floor rho
+ *                        (tsfactor.cu:837-891, --sched opt --sched-G
+ *                        --sched-rho; the reference's defaults are G = 4000,
+ *                        rho = 1.25)
+ * qcap > 0 caps LINEAR and OPT intervals at qcap blocks (tsfactor --Zq). */
+enum { GF2E_SCHED_DOUBLING = 0, GF2E_SCHED_LINEAR = 1, GF2E_SCHED_OPT = 2 };
+typedef struct gf2e_sched {
+    int mode;
+    uint64_t q0;
+    uint64_t G;
+    double rho;
+    uint64_t qcap;
+} gf2e_sched;
+
+/* The first n interval widths (degrees) of a scan whose first interval
+ * starts at degree k_start >= 2 with `block` degrees per block. */
+int gf2e_sched_widths(const gf2e_sched *sched, int block, uint64_t k_start, uint64_t L0,
+                      uint64_t Lmax, int n, uint64_t *widths_host);
+
+/* gf2e_scan_blocked under an interval schedule (L0 and Lmax are read by
+ * GF2E_SCHED_DOUBLING only). */
+int gf2e_scan_sched(uint64_t r, const uint64_t *s_host, int ns, uint64_t k0, uint64_t maxd,
+                    const gf2e_sched *sched, uint64_t L0, uint64_t Lmax, int batch, int block,
+                    gf2e_scan_result *results_host, uint64_t *masks_host,
+                    size_t mask_cap_words, void *stream);
+
 /* The steppable engine behind gf2e_scan, for callers that interleave work
  * (the serving loop): one scanner per r keeps `slots` s values resident on
  * the device; submitted s wait in a queue and enter freed slots; each step
@@ -282,6 +315,9 @@ int gf2e_scanner_create(uint64_t r, int slots, gf2e_scanner **scanner);
 int gf2e_scanner_footprint_blocked(uint64_t r, int slots, int block, size_t *device_bytes);
 int gf2e_scanner_create_blocked(uint64_t r, int slots, int block, gf2e_scanner **scanner);
 int gf2e_scanner_destroy(gf2e_scanner *scanner);
+/* Interval schedule for the jobs submitted after this call (default
+ * GF2E_SCHED_DOUBLING). */
+int gf2e_scanner_set_schedule(gf2e_scanner *scanner, const gf2e_sched *sched);
 int gf2e_scanner_submit(gf2e_scanner *scanner, const uint64_t *s_host, int ns, uint64_t k0,
                         uint64_t maxd, uint64_t L0, uint64_t Lmax, uint64_t tag0);
 int gf2e_scanner_step(gf2e_scanner *scanner, int degrees, void *stream);

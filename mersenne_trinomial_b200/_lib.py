@@ -65,6 +65,13 @@ class Tune(C.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_}
 
 
+class Sched(C.Structure):
+    _fields_ = [("mode", C.c_int), ("q0", C.c_uint64), ("G", C.c_uint64), ("rho", C.c_double),
+                ("qcap", C.c_uint64)]
+
+
+SCHED_MODES = {"doubling": 0, "linear": 1, "opt": 2}
+
 _lib = None
 _lock = threading.Lock()
 
@@ -126,6 +133,10 @@ SIGNATURES = {
     "gf2e_scan_blocked": (_i32, [_u64, _vp, _i32, _u64, _u64, _u64, _u64, _i32, _i32,
                                  _P(ScanResult), _vp, _sz, _vp]),
     "gf2e_scanner_destroy": (_i32, [_vp]),
+    "gf2e_scanner_set_schedule": (_i32, [_vp, _P(Sched)]),
+    "gf2e_sched_widths": (_i32, [_P(Sched), _i32, _u64, _u64, _u64, _i32, _vp]),
+    "gf2e_scan_sched": (_i32, [_u64, _vp, _i32, _u64, _u64, _P(Sched), _u64, _u64, _i32, _i32,
+                               _P(ScanResult), _vp, _sz, _vp]),
     "gf2e_scanner_submit": (_i32, [_vp, _vp, _i32, _u64, _u64, _u64, _u64, _u64]),
     "gf2e_scanner_step": (_i32, [_vp, _i32, _vp]),
     "gf2e_scanner_status": (_i32, [_vp, _P(_i32), _P(_i32), _P(_i32), _P(_u64)]),

@@ -30,6 +30,7 @@
 #include "polyhost.h"
 
 #include <algorithm>
+#include <cmath>
 #include <deque>
 #include <vector>
 
@@ -52,7 +53,7 @@ u64 fft_plan_n(const gf2e_fft_plan *plan);
 }  // namespace gf2e
 
 struct gf2e_scanner {
-    struct Job { u64 s, k0, maxd, L0, Lmax, tag; };
+    struct Job { u64 s, k0, maxd, L0, Lmax, tag; gf2e_sched sched; };
     struct Slot { Job job; u64 k, iv, L; };
     struct Done { gf2e_scan_result res; u64 tag; std::vector<u64> mask; };
 
@@ -86,6 +87,7 @@ struct gf2e_scanner {
     int m = 1;
     u64 *H = nullptr, *HS = nullptr, *C = nullptr, *sH = nullptr;
     std::vector<u64> shH;
+    gf2e_sched sched{GF2E_SCHED_DOUBLING, 0, 0, 0.0, 0};   // for jobs submitted next
 };
 
 // operands of at least this many bits take the half-gcd (hgcd.cu) at
@@ -93,6 +95,85 @@ struct gf2e_scanner {
 constexpr u64 GCD_LARGE_BITS = 1ull << 19;
 // device words a concurrent half-gcd job draws from its pool, per operand word
 constexpr size_t HGCD_WORDS_PER_WORD = 48;
+
+namespace gf2e {
+
+// Interval schedules (the gcd cadence of the deep scan), in degrees.
+//   DOUBLING: L0, 2 L0, 4 L0, ... capped at Lmax (trinomial_scan.cu:379-381)
+//   LINEAR:   q0, 2 q0, 3 q0, ... blocks of m degrees (tsfactor.cu:858)
+//   OPT:      tsfactor's Euler-optimal widths (tsfactor.cu:837-891): with the
+//             survival law S(k) = (16/9)/k and gcd cost G degrees of scanning,
+//             stationarity of sum S(k_{j-1}) (w_j + G) gives
+//             w' = w k / (k - w) - G, kept non-decreasing and at least
+//             (rho - 1) k; the first width minimises that cost over 96
+//             candidate first ends.
+// qcap > 0 caps an interval at qcap blocks (tsfactor --Zq) in LINEAR and OPT.
+u64 sched_first(const gf2e_sched &q, u64 m, u64 k_start, u64 L0) {
+    if (q.mode == GF2E_SCHED_DOUBLING) return L0;
+    u64 blocks = 0;
+    if (q.mode == GF2E_SCHED_LINEAR) {
+        blocks = q.q0;
+    } else {
+        const double G = (double)q.G, C = 16.0 / 9.0, grow = q.rho - 1.0;
+        const u64 k0 = k_start;
+        u64 lo = (u64)(1.02 * std::sqrt((double)k0 * G)) + 1;
+        if (lo <= k0) lo = k0 + m;
+        double best = 1e300;
+        u64 best_k1 = 0;
+        for (int i = 0; i < 96; i++) {
+            const u64 k1 = lo + (u64)((double)lo * 0.06 * i);
+            double cost = 0, kp = (double)k0, kc = (double)k1;
+            for (int j = 0; j < 200 && kp < 4e18; j++) {
+                cost += (C / kp) * ((kc - kp) + G);
+                double w = kc * kc / kp - G - kc;
+                w = std::max(w, kc - kp);
+                w = std::max(w, grow * kc);
+                kp = kc;
+                kc += w;
+                if (kp > 1e14) break;
+            }
+            if (cost < best) {
+                best = cost;
+                best_k1 = k1;
+            }
+        }
+        const u64 w = best_k1 > k0 ? best_k1 - k0 : m;
+        blocks = (w + m - 1) / m;
+    }
+    blocks = std::max<u64>(blocks, 1);
+    if (q.qcap) blocks = std::min(blocks, q.qcap);
+    return blocks * m;
+}
+
+// width after an interval of `cur` degrees that ended at degree k_end
+u64 sched_next(const gf2e_sched &q, u64 m, u64 cur, u64 k_end, u64 Lmax) {
+    if (q.mode == GF2E_SCHED_DOUBLING) return std::min(2 * cur, Lmax);
+    u64 blocks;
+    if (q.mode == GF2E_SCHED_LINEAR) {
+        blocks = cur / m + q.q0;
+    } else {
+        const double k = (double)k_end, w = (double)cur;
+        double wn = k > w ? w * k / (k - w) - (double)q.G : w;
+        wn = std::max(wn, w);
+        wn = std::max(wn, (q.rho - 1.0) * k);
+        wn = std::min(wn, 4e18);
+        blocks = ((u64)wn + m - 1) / m;
+    }
+    blocks = std::max<u64>(blocks, 1);
+    if (q.qcap) blocks = std::min(blocks, q.qcap);
+    return blocks * m;
+}
+
+int sched_check(const gf2e_sched *q) {
+    if (!q) return invalid("null schedule");
+    if (q->mode == GF2E_SCHED_DOUBLING) return GF2E_OK;
+    if (q->mode == GF2E_SCHED_LINEAR) return q->q0 >= 1 ? GF2E_OK : invalid("linear schedule: q0 >= 1");
+    if (q->mode == GF2E_SCHED_OPT)
+        return (q->G >= 1 && q->rho > 1.0) ? GF2E_OK : invalid("opt schedule: G >= 1 and rho > 1");
+    return invalid("schedule mode %d", q->mode);
+}
+
+}  // namespace gf2e
 
 namespace {
 
@@ -237,7 +318,8 @@ int load_slot(gf2e_scanner &S, int j, const gf2e_scanner::Job &job, cudaStream_t
             e = cudaMemcpyAsync(Hj, HSj, (size_t)m * S.stride * 8, cudaMemcpyDeviceToDevice, st);
             if (e != cudaSuccess) return gf2e::cuda_status(e, "scanner block ramp");
         }
-        S.slot[j] = gf2e_scanner::Slot{job, job.k0, job.k0, job.L0};
+        S.slot[j] = gf2e_scanner::Slot{
+            job, job.k0, job.k0, gf2e::sched_first(job.sched, (u64)m, job.k0 + 1, job.L0)};
         return GF2E_OK;
     }
     GF2E_TRY(gf2e::trin_set_const(S.F + S.stride * j, S.stride, 1, S.r, 2, st));
@@ -248,7 +330,8 @@ int load_slot(gf2e_scanner &S, int j, const gf2e_scanner::Job &job, cudaStream_t
                             cudaMemcpyDeviceToDevice, st);
         if (e != cudaSuccess) return gf2e::cuda_status(e, "scanner ramp");
     }
-    S.slot[j] = gf2e_scanner::Slot{job, job.k0, job.k0, job.L0};
+    S.slot[j] = gf2e_scanner::Slot{job, job.k0, job.k0,
+                                   gf2e::sched_first(job.sched, 1, job.k0 + 1, job.L0)};
     return GF2E_OK;
 }
 
@@ -419,7 +502,7 @@ int degree_step(gf2e_scanner &S, cudaStream_t st) {
             retire.push_back(j);
         } else {
             sl.iv = sl.k;
-            sl.L = std::min(2 * sl.L, sl.job.Lmax);
+            sl.L = gf2e::sched_next(sl.job.sched, (u64)S.m, sl.L, sl.k, sl.job.Lmax);
             GF2E_TRY(gf2e::trin_set_const(S.ACC + S.stride * j, S.stride, 1, S.r, 1, st));
         }
     }
@@ -569,7 +652,8 @@ int gf2e_scanner_submit(gf2e_scanner *S, const uint64_t *s_host, int ns, uint64_
     L0 = (L0 + bm - 1) / bm * bm;
     Lmax = (Lmax + bm - 1) / bm * bm;
     for (int i = 0; i < ns; i++)
-        S->queue.push_back(gf2e_scanner::Job{s_host[i], k0, maxd, L0, Lmax, tag0 + (u64)i});
+        S->queue.push_back(
+            gf2e_scanner::Job{s_host[i], k0, maxd, L0, Lmax, tag0 + (u64)i, S->sched});
     return GF2E_OK;
 }
 
@@ -623,6 +707,32 @@ int gf2e_scanner_poll(gf2e_scanner *S, gf2e_scan_result *res, uint64_t *tags,
     return GF2E_OK;
 }
 
+int gf2e_scanner_set_schedule(gf2e_scanner *S, const gf2e_sched *sched) {
+    if (!S) return gf2e::invalid("null scanner");
+    GF2E_TRY(gf2e::sched_check(sched));
+    S->sched = *sched;
+    return GF2E_OK;
+}
+
+int gf2e_sched_widths(const gf2e_sched *sched, int block, uint64_t k_start, uint64_t L0,
+                      uint64_t Lmax, int n, uint64_t *widths) {
+    GF2E_TRY(gf2e::sched_check(sched));
+    if (block < 1 || k_start < 2 || n < 0 || (n && !widths))
+        return gf2e::invalid("schedule widths: bad arguments");
+    const u64 m = (u64)block;
+    if (Lmax < 1) Lmax = 1;
+    if (L0 < 1) L0 = 1;
+    L0 = (std::min(L0, Lmax) + m - 1) / m * m;
+    Lmax = (Lmax + m - 1) / m * m;
+    u64 w = gf2e::sched_first(*sched, m, k_start, L0), k_end = k_start - 1;
+    for (int i = 0; i < n; i++) {
+        widths[i] = w;
+        k_end += w;
+        w = gf2e::sched_next(*sched, m, w, k_end, Lmax);
+    }
+    return GF2E_OK;
+}
+
 int gf2e_scan(uint64_t r, const uint64_t *s_host, int ns, uint64_t k0, uint64_t maxd,
               uint64_t L0, uint64_t Lmax, int batch, gf2e_scan_result *res,
               uint64_t *masks_host, size_t mask_cap_words, void *stream) {
@@ -633,11 +743,22 @@ int gf2e_scan(uint64_t r, const uint64_t *s_host, int ns, uint64_t k0, uint64_t 
 int gf2e_scan_blocked(uint64_t r, const uint64_t *s_host, int ns, uint64_t k0, uint64_t maxd,
                       uint64_t L0, uint64_t Lmax, int batch, int block, gf2e_scan_result *res,
                       uint64_t *masks_host, size_t mask_cap_words, void *stream) {
+    const gf2e_sched dbl{GF2E_SCHED_DOUBLING, 0, 0, 0.0, 0};
+    return gf2e_scan_sched(r, s_host, ns, k0, maxd, &dbl, L0, Lmax, batch, block, res,
+                           masks_host, mask_cap_words, stream);
+}
+
+int gf2e_scan_sched(uint64_t r, const uint64_t *s_host, int ns, uint64_t k0, uint64_t maxd,
+                    const gf2e_sched *sched, uint64_t L0, uint64_t Lmax, int batch, int block,
+                    gf2e_scan_result *res, uint64_t *masks_host, size_t mask_cap_words,
+                    void *stream) {
     if (!s_host || !res || ns < 1 || batch < 1)
         return gf2e::invalid("gf2e_scan: ns >= 1 and batch >= 1 required");
+    GF2E_TRY(gf2e::sched_check(sched));
     gf2e_scanner *S = nullptr;
     GF2E_TRY(gf2e_scanner_create_blocked(r, std::min(batch, ns), block, &S));
-    int st = gf2e_scanner_submit(S, s_host, ns, k0, maxd, L0, Lmax, 0);
+    int st = gf2e_scanner_set_schedule(S, sched);
+    if (st == GF2E_OK) st = gf2e_scanner_submit(S, s_host, ns, k0, maxd, L0, Lmax, 0);
     std::vector<gf2e_scan_result> tmp(ns);
     std::vector<u64> tags(ns), masks((size_t)ns * mask_cap_words);
     int got = 0;

@@ -4,6 +4,8 @@
 //
 //   trinomial_scan <r> <survivors.txt> <k0> <maxd> <out_prefix>
 //                  [--interval Lmax] [--l0 L0] [--batch B] [--block m] [--verbose 0..3]
+//                  [--sched doubling|linear|opt] [--q0 N] [--sched-G N] [--sched-rho R]
+//                  [--Zq N]                              (tsfactor's interval schedules)
 //                  [--gcd-threads N] [--state FILE]      (accepted, unused)
 //   trinomial_scan --selftest
 //
@@ -90,12 +92,13 @@ static bool divides(u64 r, u64 s, const u64 *p, size_t pw, u64 d) {
 }
 
 static int run(u64 r, const std::vector<u64> &surv, u64 k0, u64 maxd, u64 L0, u64 Lmax,
-               int batch, int block, FILE *fres, int verbose, u64 *nfound, u64 *nu, u64 *nbad) {
+               int batch, int block, const gf2e_sched &sched, FILE *fres, int verbose,
+               u64 *nfound, u64 *nu, u64 *nbad) {
     const size_t cap = 4096;
     std::vector<gf2e_scan_result> res(surv.size());
     std::vector<u64> masks(surv.size() * cap);
-    int st = gf2e_scan_blocked(r, surv.data(), (int)surv.size(), k0, maxd, L0, Lmax, batch, block,
-                               res.data(), masks.data(), cap, nullptr);
+    int st = gf2e_scan_sched(r, surv.data(), (int)surv.size(), k0, maxd, &sched, L0, Lmax, batch,
+                             block, res.data(), masks.data(), cap, nullptr);
     if (st != GF2E_OK) {
         fprintf(stderr, "scan failed: %s (%s)\n", gf2e_status_string(st), gf2e_last_error());
         return 1;
@@ -134,14 +137,22 @@ static int selftest() {
     for (u64 s = 2; s <= smax; s++)
         if (best[s] == ~0ULL) surv.push_back(s);
     int bad = 0;
-    const u64 pol[2][2] = {{32, 4096}, {8, 8}};
-    for (auto &p : pol) {
+    // interval policies: trinomial_scan's doubling, then tsfactor's blocked
+    // DDF under its linear (m=4 q0=3) and Euler-optimal (m=6 G=60) schedules
+    struct Pol { u64 L0, Lmax; int block; gf2e_sched sched; const char *name; };
+    const Pol pol[] = {
+        {32, 4096, 1, {GF2E_SCHED_DOUBLING, 0, 0, 0.0, 0}, "intervals 32/4096"},
+        {8, 8, 1, {GF2E_SCHED_DOUBLING, 0, 0, 0.0, 0}, "intervals 8/8"},
+        {64, 4096, 4, {GF2E_SCHED_LINEAR, 3, 0, 0.0, 0}, "block m=4 q0=3"},
+        {64, 4096, 6, {GF2E_SCHED_OPT, 0, 60, 1.25, 0}, "block m=6 sched-opt G=60"}};
+    for (const Pol &p : pol) {
         u64 nf = 0, nu = 0, nb = 0;
-        if (run(r, surv, k0, maxd, p[0], p[1], 64, 1, nullptr, 0, &nf, &nu, &nb)) return 1;
+        if (run(r, surv, k0, maxd, p.L0, p.Lmax, 64, p.block, p.sched, nullptr, 0, &nf, &nu, &nb))
+            return 1;
         bool ok = surv.size() == 104 && nf == 102 && nu == 2 && nb == 0;
-        printf("scan r=4423 k0=5 maxd=200 intervals %" PRIu64 "/%" PRIu64 ": %zu survivors, "
+        printf("scan r=4423 k0=5 maxd=200 %s: %zu survivors, "
                "%" PRIu64 " found, %" PRIu64 " u, %" PRIu64 " not dividing  %s\n",
-               p[0], p[1], surv.size(), nf, nu, nb, ok ? "PASS" : "FAIL");
+               p.name, surv.size(), nf, nu, nb, ok ? "PASS" : "FAIL");
         bad += !ok;
     }
     printf(bad ? "\nSCAN SELFTEST: %d FAILURES\n" : "\nSCAN SELFTEST: ALL PASS\n", bad);
@@ -153,6 +164,7 @@ int main(int argc, char **argv) {
     if (argc < 6) {
         fprintf(stderr, "usage: %s <r> <survivors.txt> <k0> <maxd> <out_prefix>\n"
                         "          [--interval Lmax] [--l0 L0] [--batch B] [--block m] [--verbose 0..3]\n"
+                        "          [--sched doubling|linear|opt] [--q0 N] [--sched-G N] [--sched-rho R] [--Zq N]\n"
                         "       %s --selftest\n"
                         "k0 must be the depth the coarse sieve actually reached.\n",
                 argv[0], argv[0]);
@@ -162,7 +174,24 @@ int main(int argc, char **argv) {
     std::string prefix = argv[5];
     u64 L0 = 64, Lmax = 4096;
     int batch = 64, verbose = 1, block = 1;
+    gf2e_sched sched{GF2E_SCHED_DOUBLING, 0, 4000, 1.25, 0};
     for (int i = 6; i < argc; i++) {
+        if (!strcmp(argv[i], "--sched") && i + 1 < argc) {
+            const char *v = argv[++i];
+            if (!strcmp(v, "opt")) sched.mode = GF2E_SCHED_OPT;
+            else if (!strcmp(v, "linear")) sched.mode = GF2E_SCHED_LINEAR;
+            else if (!strcmp(v, "doubling")) sched.mode = GF2E_SCHED_DOUBLING;
+            else { fprintf(stderr, "bad --sched %s (doubling|linear|opt)\n", v); return 1; }
+            continue;
+        }
+        if (!strcmp(argv[i], "--q0") && i + 1 < argc) {
+            sched.q0 = strtoull(argv[++i], 0, 10);
+            if (sched.mode == GF2E_SCHED_DOUBLING) sched.mode = GF2E_SCHED_LINEAR;
+            continue;
+        }
+        if (!strcmp(argv[i], "--sched-G") && i + 1 < argc) { sched.G = strtoull(argv[++i], 0, 10); continue; }
+        if (!strcmp(argv[i], "--sched-rho") && i + 1 < argc) { sched.rho = atof(argv[++i]); continue; }
+        if (!strcmp(argv[i], "--Zq") && i + 1 < argc) { sched.qcap = strtoull(argv[++i], 0, 10); continue; }
         if (!strcmp(argv[i], "--interval") && i + 1 < argc) Lmax = strtoull(argv[++i], 0, 10);
         else if (!strcmp(argv[i], "--l0") && i + 1 < argc) L0 = strtoull(argv[++i], 0, 10);
         else if (!strcmp(argv[i], "--batch") && i + 1 < argc) batch = atoi(argv[++i]);
@@ -179,6 +208,9 @@ int main(int argc, char **argv) {
     }
     if (Lmax < 1) Lmax = 1;
     if (L0 > Lmax) L0 = Lmax;
+    // tsfactor's default first interval: ceil(600 / m) blocks
+    if (sched.mode != GF2E_SCHED_DOUBLING && sched.q0 == 0)
+        sched.q0 = (600 + (u64)block - 1) / (u64)block;
     if (!(k0 >= 1 && maxd > k0)) { fprintf(stderr, "need 1 <= k0 < maxd\n"); return 1; }
     std::vector<u64> surv;
     FILE *f = fopen(argv[2], "r");
@@ -207,7 +239,9 @@ int main(int argc, char **argv) {
     if (!fres) { perror(rpath.c_str()); return 1; }
     double t0 = now_s();
     u64 nf = 0, nu = 0, nb = 0;
-    int rc = todo.empty() ? 0 : run(r, todo, k0, maxd, L0, Lmax, batch, block, fres, verbose, &nf, &nu, &nb);
+    int rc = todo.empty() ? 0
+                          : run(r, todo, k0, maxd, L0, Lmax, batch, block, sched, fres, verbose,
+                                &nf, &nu, &nb);
     fclose(fres);
     fprintf(stderr, "done: %" PRIu64 " found, %" PRIu64 " u, %.1fs total%s\n", nf, nu,
             now_s() - t0, nb ? " (WARNING: some factors failed verification)" : "");

@@ -355,18 +355,42 @@ def _hex(words) -> str:
     return format(x, "x")
 
 
+def make_sched(sched: str = "doubling", q0: int = 0, G: int = 4000, rho: float = 1.25,
+               qcap: int = 0):
+    """Interval schedule (include/gf2e.h gf2e_sched): 'doubling' (trinomial_scan
+    L0, 2 L0, ... Lmax), 'linear' (tsfactor q0, 2 q0, ... blocks) or 'opt'
+    (tsfactor's Euler-optimal widths, gcd cost G degrees, floor rho)."""
+    from ._lib import SCHED_MODES, Sched
+    if sched not in SCHED_MODES:
+        raise ValueError(f"schedule {sched!r}: one of {sorted(SCHED_MODES)}")
+    return Sched(SCHED_MODES[sched], q0, G, rho, qcap)
+
+
+def sched_widths(sched: str, block: int, k_start: int, n: int, L0: int = 64, Lmax: int = 4096,
+                 **kw) -> list:
+    """The first n interval widths (degrees) of a scan starting at k_start."""
+    q = make_sched(sched, **kw)
+    out = np.zeros(max(1, n), dtype=np.uint64)
+    call("gf2e_sched_widths", C.byref(q), block, k_start, L0, Lmax, n, out.ctypes.data)
+    return [int(x) for x in out[:n]]
+
+
 def scan(r: int, survivors, k0: int, maxd: int, L0: int = 64, Lmax: int = 4096,
-         batch: int = 64, mask_cap_words: int = 1024, stream=None, block: int = 1) -> list:
+         batch: int = 64, mask_cap_words: int = 1024, stream=None, block: int = 1,
+         sched: str = "doubling", q0: int = 0, G: int = 4000, rho: float = 1.25,
+         qcap: int = 0) -> list:
     """Deep scan (trinomial_scan.cu): one result line per s in the reference's
     format, 's d p<hex>', 's u' or 's rA-B'.  block = m > 1 runs tsfactor's
-    blocked DDF (m degrees per step: one modmul and m*m squarings)."""
+    blocked DDF (m degrees per step: one modmul and m*m squarings); `sched`
+    picks the interval schedule (make_sched)."""
     from ._lib import ScanResult
+    q = make_sched(sched, q0=q0, G=G, rho=rho, qcap=qcap)
     s = np.ascontiguousarray(np.asarray(survivors, dtype=np.uint64))
     n = s.size
     res = (ScanResult * n)()
     masks = np.zeros((n, mask_cap_words), dtype=np.uint64)
-    call("gf2e_scan_blocked", r, s.ctypes.data, n, k0, maxd, L0, Lmax, batch, block, res,
-         masks.ctypes.data, mask_cap_words, _sp(stream))
+    call("gf2e_scan_sched", r, s.ctypes.data, n, k0, maxd, C.byref(q), L0, Lmax, batch, block,
+         res, masks.ctypes.data, mask_cap_words, _sp(stream))
     out = []
     for i in range(n):
         R = res[i]

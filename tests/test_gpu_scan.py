@@ -101,3 +101,38 @@ def test_blocked_scan_r136279841_known_answer(engine):
     degrees from k0 = 24, one gcd after two blocks)."""
     got = engine.scan(136279841, [474], 24, 200, L0=64, Lmax=4096, batch=1, block=32)
     assert got == ["474 41 p3991ef16129"]
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("block,sched,kw", [(1, "linear", {"q0": 40}), (4, "linear", {"q0": 3}),
+                                            (6, "opt", {"G": 60}), (2, "opt", {"G": 100, "rho": 1.1}),
+                                            (8, "linear", {"q0": 2, "qcap": 5})])
+def test_scheduled_scan_matches_doubling(engine, block, sched, kw):
+    """tsfactor's interval schedules (QSched linear / Euler-optimal, --Zq)
+    change only the gcd cadence: every result line of the r = 4423 selftest
+    survivors equals the doubling schedule's."""
+    fx = load_json("scan.json")
+    r, k0, maxd = fx["r"], fx["k0"], fx["maxd"]
+    want = engine.scan(r, fx["survivors"], k0, maxd, L0=32, Lmax=4096, batch=128)
+    got = engine.scan(r, fx["survivors"], k0, maxd, batch=64, block=block, sched=sched, **kw)
+    assert got == want
+
+
+@pytest.mark.gpu
+def test_late_hit_resolves_without_testing_cleared_degrees(engine, oracle):
+    """A hit in an interval that starts past 2 k0 is resolved from the gcd
+    alone (every factor degree below the interval is excluded by the clear
+    intervals): same lines as the oracle's scan for survivors whose least
+    factor lies deep."""
+    fx = load_json("scan.json")
+    r, k0, maxd = fx["r"], fx["k0"], fx["maxd"]
+    got = engine.scan(r, fx["survivors"], k0, maxd, L0=8, Lmax=8, batch=128)
+    deep = []
+    for line, s in zip(got, fx["survivors"]):
+        parts = line.split()
+        if parts[1] != "u" and int(parts[1]) > 2 * k0 + 8:
+            deep.append((s, line))
+    assert len(deep) >= 10
+    for s, line in deep[:10]:
+        st, d, gdeg, g_hex, mask_hex = oracle.scan_one(r, s, k0, maxd)
+        assert st == 1 and line == f"{s} {d} p{mask_hex}"
