@@ -63,16 +63,21 @@ int gf2e_copy_to_device(void *dst_dev, const void *src_host, size_t bytes, void 
  * extended exactly.
  * ====================================================================== */
 
-/* Device workspace bytes needed by gf2e_sieve_run for degrees <= dmax. */
+/* Device workspace bytes for gf2e_sieve_run up to degree dmax (<= 40). */
 int gf2e_sieve_workspace_size(int dmax, size_t *bytes);
 
 /* best_dev[0..smax] = UINT64_MAX (coarse_sieve.cu k_fill 301-305). */
 int gf2e_sieve_fill(uint64_t *best_dev, uint64_t smax, void *stream);
 
-/* Sieve degrees dmin..dmax (2 <= dmin <= dmax <= 31) into best_dev.  The
- * workspace holds dense antilog/log tables of 2^dmax entries (2 x 8 GB at
- * d = 31); the reference switches to bucketed tables beyond its GPU memory
- * (coarse_sieve.cu:920-1117).
+/* Sieve degrees dmin..dmax (2 <= dmin <= dmax <= 40) into best_dev.
+ * Degrees <= 31 use dense antilog/log tables of 2^d entries (2 x 8 GB at
+ * d = 31).  Degrees 32..40 keep 64-bit field elements and store only the log
+ * table, in value slices as large as the workspace allows (the reference's
+ * wide-field low-memory mode, coarse_sieve.cu:920-1117): each slice costs
+ * one walk over the 2^d - 1 exponents and one pass over the coset leaders.
+ * Any workspace of at least the dense tables (when dmin <= 31) and 256 MB
+ * (when dmax >= 32) works; gf2e_sieve_workspace_size gives one slice up to
+ * 64 GB (GF2E_SIEVE_WIDE_GB overrides).
  * Host-side per-degree setup (primitive polynomial search) is cached.
  * Returns GF2E_ERR_UNSUPPORTED_R when gcd(r mod (2^d-1), 2^d-1) != 1 for
  * some d in range, before launching anything.  All degrees are enqueued on
@@ -89,8 +94,8 @@ int gf2e_sieve_run(uint64_t r, int dmin, int dmax, uint64_t smax,
 int gf2e_sieve_stats(const void *workspace_dev, int dmax, uint64_t *classes_host,
                      uint64_t *marks_host, void *stream);
 
-/* Smallest primitive polynomial of degree d, 2 <= d <= 32
- * (gf2_field_setup.h:49-58).  Host only. */
+/* Smallest primitive polynomial of degree d, 2 <= d <= 40
+ * (gf2_field_setup.h:49-58, gf2_wide_setup.h:44-53).  Host only. */
 uint64_t gf2e_primitive_poly(int d);
 
 /* ======================================================================

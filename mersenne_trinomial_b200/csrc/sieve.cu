@@ -1,11 +1,20 @@
 // sieve.cu -- Zech-log sieve for the smallest irreducible factor of degree
-// d <= 31 of x^r + x^s + 1, for every s in [1, smax] at once.
+// d <= 40 of x^r + x^s + 1, for every s in [1, smax] at once.
 //
-// Degrees up to 31 keep every field element and modulus in 32 bits.  The
-// reference needs bucketed low-memory tables beyond d = 29 on its 8 GB GPU
-// (coarse_sieve.cu:920-1117, gf2_wide_field.h); on a B200 the dense antilog
-// and log tables of d = 31 (2 x 8 GB) fit in HBM, so every degree uses the
-// same dense path.
+// Degrees up to 31 keep every field element and modulus in 32 bits and use
+// dense antilog and log tables (2 x 8 GB at d = 31, resident in HBM).  The
+// reference switches to bucketed low-memory tables beyond its GPU memory
+// (coarse_sieve.cu:920-1117, 64-bit fields of gf2_wide_field.h for d >= 33).
+// Degrees 32..40 here ("wide") keep elements in 64 bits and store only the
+// log table, as slices of the value range [lo, hi) sized to the workspace
+// (one slice of 2^d entries when it fits: d = 32 takes 16 GB, d = 33 64 GB):
+//   k_wide_slice    walks the exponents with a multiply-by-x chain and
+//                   writes L[v - lo] = i for the values x^i in the slice
+//   k_wide_classes  per coset leader j: x^(j r) by square-and-multiply-by-x
+//                   (no antilog table), the Zech lookup when x^(j r) + 1 lies
+//                   in the slice, then the same progression and minimal
+//                   polynomial as the dense path
+// so a degree costs one exponent walk and one pass over j per slice.
 //
 // Number theory (the reference's, sieve_ref.cpp:8-26): in GF(2^d) built on
 // the smallest primitive q_d (x generates the group of order M = 2^d - 1), an
@@ -36,12 +45,15 @@
 // synchronisation is the final overflow/status read.
 #include "gf2e_internal.cuh"
 
+#include <algorithm>
+#include <cstdlib>
 #include <mutex>
 #include <vector>
 
 namespace {
 
-constexpr int DMAX = 31;
+constexpr int DMAX = 31;                  // dense tables (32-bit elements)
+constexpr int DMAX_WIDE = 40;             // 64-bit elements, sliced log table
 constexpr int STRIP_LOG_MAX = 14;         // strip CTAs own 2^10..2^14 entries of best[]
                                           // (8..128 KB of shared memory), tunable
 constexpr u64 INLINE = 32;                // marks done inline by the class thread
@@ -52,25 +64,58 @@ struct Prog { u64 s0, n, key; };          // first s, period, packed key
 
 struct Counters {
     unsigned long long nstrip, nheavy, overflow, bad;
-    unsigned long long classes[DMAX + 1];
-    unsigned long long marks[DMAX + 1];
+    unsigned long long classes[DMAX_WIDE + 1];
+    unsigned long long marks[DMAX_WIDE + 1];
 };
 
+// workspace: progression lists and counters first, then the table region
+// (dense A and L tables, or the wide log-table slice), whose size may be
+// anything the caller provides above the minimum
 struct Layout {
-    size_t off_A, off_L, off_strip, off_heavy, off_cnt, total;
+    size_t off_strip, off_heavy, off_cnt, off_region;
 };
 
-Layout layout_for(int dmax) {
-    Layout l;
-    size_t tab = ((size_t)1 << dmax) * sizeof(u32);
-    tab = (tab + 255) & ~(size_t)255;
-    l.off_A = 0;
-    l.off_L = tab;
-    l.off_strip = 2 * tab;
-    l.off_heavy = l.off_strip + SCAP * sizeof(Prog);
-    l.off_cnt = l.off_heavy + HCAP * sizeof(Prog);
-    l.total = l.off_cnt + ((sizeof(Counters) + 255) & ~(size_t)255);
-    return l;
+constexpr Layout layout() {
+    return Layout{0, SCAP * sizeof(Prog), SCAP * sizeof(Prog) + HCAP * sizeof(Prog),
+                  ((SCAP + HCAP) * sizeof(Prog) + sizeof(Counters) + 255) & ~(size_t)255};
+}
+
+size_t dense_table_bytes(int d) {
+    size_t tab = ((size_t)1 << d) * sizeof(u32);
+    return (tab + 255) & ~(size_t)255;
+}
+
+// log-table entry bytes of a wide degree (exponents below 2^d)
+size_t wide_entry_bytes(int d) { return d <= 32 ? 4 : 8; }
+
+// default wide slice budget (GF2E_SIEVE_WIDE_GB overrides)
+size_t wide_budget() {
+    const char *e = getenv("GF2E_SIEVE_WIDE_GB");
+    double gb = e ? atof(e) : 64.0;
+    if (!(gb >= 0.25)) gb = 0.25;
+    return (size_t)(gb * (double)(1ull << 30)) & ~(size_t)255;
+}
+
+// first degree sieved on the wide path (DMAX + 1; GF2E_SIEVE_WIDE_FROM
+// lowers it, down to 8, so the two paths can be compared on the same degrees)
+int wide_from() {
+    const char *e = getenv("GF2E_SIEVE_WIDE_FROM");
+    int v = e ? atoi(e) : DMAX + 1;
+    return std::min(std::max(v, 8), DMAX + 1);
+}
+
+// table region a run of dmin..dmax needs at least / would like
+size_t region_min(int dmin, int dmax) {
+    const int w = wide_from();
+    size_t need = dmin < w ? 2 * dense_table_bytes(std::min(dmax, w - 1)) : 0;
+    if (dmax >= w) need = std::max<size_t>(need, (size_t)1 << 28);
+    return need;
+}
+size_t region_want(int dmin, int dmax) {
+    size_t want = region_min(dmin, dmax);
+    if (dmax >= wide_from())
+        want = std::max(want, std::min(((size_t)1 << dmax) * wide_entry_bytes(dmax), wide_budget()));
+    return want;
 }
 
 // ---- small field GF(2^d), d <= 31, modulus q (bit d set)
@@ -269,6 +314,163 @@ __global__ void k_fill(unsigned long long *p, u64 n, unsigned long long v) {
         p[i] = v;
 }
 
+// ---- wide field GF(2^d), 32 <= d <= 40: elements in 64 bits, modulus
+// x^d + qlow with qlow of low degree e (2 e <= d), given by its terms
+struct WideField {
+    int d;
+    int nt;                   // terms of qlow (bit positions, < d)
+    int t[12];
+    u64 M, qlow;
+};
+
+// t (hi:lo, below 2^(2d-1)) mod the modulus: two folds of the bits >= d by qlow
+GF2E_DEV u64 wf_reduce(u64 lo, u64 hi, const WideField &F) {
+    const int d = F.d;
+    const u64 mask = F.M;                                // 2^d - 1
+    u64 h = (lo >> d) | (hi << (64 - d));                // bits >= d, below 2^(d-1)
+    u64 t = lo & mask;
+    u64 f = 0;
+#pragma unroll 4
+    for (int i = 0; i < F.nt; i++) f ^= h << F.t[i];     // < 2^(d-1+e)
+    t ^= f & mask;
+    h = f >> d;                                          // below 2^(e-1)
+    f = 0;
+#pragma unroll 4
+    for (int i = 0; i < F.nt; i++) f ^= h << F.t[i];     // < 2^(2e-1) <= 2^d
+    return t ^ f;
+}
+GF2E_DEV u64 wf_mulx(u64 a, const WideField &F) {
+    const u64 top = (a >> (F.d - 1)) & 1;
+    return ((a << 1) & F.M) ^ (F.qlow & (0ull - top));
+}
+GF2E_DEV u64 wf_sqr(u64 a, const WideField &F) {
+    return wf_reduce(spread32((u32)a), spread32((u32)(a >> 32)), F);
+}
+GF2E_DEV u64 wf_mul(u64 a, u64 b, const WideField &F) {
+    const u32 a0 = (u32)a, a1 = (u32)(a >> 32), b0 = (u32)b, b1 = (u32)(b >> 32);
+    const u64 lo = clmul32(a0, b0), hi = clmul32(a1, b1);
+    const u64 mid = clmul32(a0 ^ a1, b0 ^ b1) ^ lo ^ hi;
+    return wf_reduce(lo ^ (mid << 32), hi ^ (mid >> 32), F);
+}
+// x^e, e < 2^d: left to right, squaring then multiplying by x
+GF2E_DEV u64 wf_powx(u64 e, const WideField &F) {
+    if (!e) return 1;
+    u64 r = 1;
+    for (int bit = 63 - __clzll(e); bit >= 0; bit--) {
+        r = wf_sqr(r, F);
+        if ((e >> bit) & 1) r = wf_mulx(r, F);
+    }
+    return r;
+}
+// a * b mod M = 2^d - 1
+GF2E_DEV u64 mulmod_mersenne(u64 a, u64 b, int d, u64 M) {
+    unsigned __int128 p = (unsigned __int128)a * b;
+    while (p > M) p = (p & M) + (p >> d);
+    return p == M ? 0 : (u64)p;
+}
+GF2E_DEV u64 mulmod_u64(u64 a, u64 b, u64 n) {
+    return (u64)(((unsigned __int128)a * b) % n);
+}
+
+// log-table slice: L[v - lo] = i for the values v = x^i in [lo, lo + len)
+template <typename E>
+__global__ void k_wide_slice(E *__restrict__ L, const WideField F, u64 lo, u64 len) {
+    const u64 nchunk = (F.M + 63) >> 6;
+    for (u64 t = (u64)blockIdx.x * blockDim.x + threadIdx.x; t < nchunk;
+         t += (u64)gridDim.x * blockDim.x) {
+        const u64 i0 = t << 6;
+        u64 v = wf_powx(i0, F);
+        const int ne = (int)min((u64)64, F.M - i0);
+        for (int e = 0; e < ne; e++) {
+            if (v - lo < len) L[v - lo] = (E)(i0 + e);
+            v = wf_mulx(v, F);
+        }
+    }
+}
+
+struct WideArgs {
+    WideField F;
+    u64 rmod, smax, lo, len;
+    int nsub, first_slice;
+    u64 subq[6];
+};
+
+template <typename E>
+__global__ void __launch_bounds__(256)
+k_wide_classes(const E *__restrict__ L, const WideArgs a, unsigned long long *__restrict__ best,
+               Prog *__restrict__ heavy, Counters *__restrict__ cnt) {
+    const int d = a.F.d;
+    const u64 M = a.F.M;
+    unsigned long long my_classes = 0, my_marks = 0;
+    for (u64 j = (u64)blockIdx.x * blockDim.x + threadIdx.x + 1; j < M;
+         j += (u64)gridDim.x * blockDim.x) {
+        // least element of its cyclotomic coset {j 2^i mod M}
+        u64 jj = j;
+        bool minimal = true;
+        for (int i = 1; i < d; i++) {
+            jj = ((jj << 1) | (jj >> (d - 1))) & M;
+            if (jj < j) { minimal = false; break; }
+        }
+        if (!minimal) continue;
+        bool sub = false;
+        for (int k = 0; k < a.nsub; k++)
+            if (j % a.subq[k] == 0) { sub = true; break; }
+        if (sub) continue;
+        if (a.first_slice) my_classes++;
+        const u64 u = mulmod_mersenne(j, a.rmod, d, M);
+        if (u == 0) continue;
+        const u64 w = wf_powx(u, a.F) ^ 1ull;            // x^(j r) + 1
+        if (w - a.lo >= a.len) continue;                 // another slice's lookup
+        const u64 v = (u64)L[w - a.lo];
+        const u64 gg = gcd_u64(j, M);
+        if (v % gg) continue;
+        const u64 n = M / gg;
+        const u64 s0 = mulmod_u64(inv_mod(j / gg, n), v / gg, n);
+        const u64 first = s0 ? s0 : n;
+        if (first > a.smax) continue;
+        const u64 count = (a.smax - first) / n + 1;
+        // minimal polynomial of beta = x^j: first linear dependency among
+        // beta^0..beta^d over GF(2)
+        const u64 beta = wf_powx(j, a.F);
+        u64 prow[DMAX_WIDE + 1], ptag[DMAX_WIDE + 1];
+        int pbit[DMAX_WIDE + 1];
+        int np = 0;
+        u64 mask = 0, pw = 1;
+        for (int k = 0; k <= d; k++) {
+            u64 row = pw, tag = 1ull << k;
+            for (int p = 0; p < np; p++)
+                if ((row >> pbit[p]) & 1) { row ^= prow[p]; tag ^= ptag[p]; }
+            if (row == 0) { mask = tag; break; }
+            pbit[np] = 63 - __clzll(row);
+            prow[np] = row;
+            ptag[np] = tag;
+            np++;
+            pw = wf_mul(pw, beta, a.F);
+        }
+        if (!((mask >> d) & 1) || !(mask & 1)) {        // cannot happen
+            atomicAdd(&cnt->bad, 1ull);
+            continue;
+        }
+        const unsigned long long key = ((u64)d << 48) | mask;
+        my_marks += count;
+        if (count <= INLINE) {
+            for (u64 s = first; s <= a.smax; s += n) atomicMin(&best[s], key);
+        } else {
+            unsigned long long slot = atomicAdd(&cnt->nheavy, 1ull);
+            if (slot < HCAP) heavy[slot] = Prog{first, n, key};
+            else atomicAdd(&cnt->overflow, 1ull);
+        }
+    }
+    for (int o = 16; o; o >>= 1) {
+        my_classes += __shfl_down_sync(0xffffffffu, my_classes, o);
+        my_marks += __shfl_down_sync(0xffffffffu, my_marks, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        if (my_classes) atomicAdd(&cnt->classes[d], my_classes);
+        if (my_marks) atomicAdd(&cnt->marks[d], my_marks);
+    }
+}
+
 // ---- host-side field setup (gf2_field_setup.h:14-58 restated)
 u32 h_mul(u32 a, u32 b, u64 q, int d) {
     u64 t = 0, x = a;
@@ -313,12 +515,69 @@ u64 h_primitive(int d) {
     }
     return 0;
 }
+// 64-bit elements for 33 <= d <= 40 (gf2_wide_setup.h:44-53 restated)
+u64 hw_mul(u64 a, u64 b, u64 q, int d) {
+    unsigned __int128 t = 0, x = a;
+    while (b) { if (b & 1) t ^= x; x <<= 1; b >>= 1; }
+    for (int bit = 2 * d - 2; bit >= d; bit--)
+        if ((t >> bit) & 1) t ^= (unsigned __int128)q << (bit - d);
+    return (u64)t;
+}
+u64 hw_pow(u64 base, u64 e, u64 q, int d) {
+    u64 r = 1;
+    while (e) { if (e & 1) r = hw_mul(r, base, q, d); base = hw_mul(base, base, q, d); e >>= 1; }
+    return r;
+}
+bool hw_irreducible(u64 q, int d) {
+    u64 chain[DMAX_WIDE + 1];
+    u64 t = 2;
+    chain[0] = t;
+    for (int i = 1; i <= d; i++) { t = hw_mul(t, t, q, d); chain[i] = t; }
+    if (chain[d] != 2) return false;
+    u64 ps[16];
+    int np = h_prime_factors((u64)d, ps);
+    for (int i = 0; i < np; i++)
+        if (chain[d / ps[i]] == 2) return false;
+    return true;
+}
+u64 hw_primitive(int d) {
+    u64 M = ((u64)1 << d) - 1, ps[64];
+    int np = h_prime_factors(M, ps);
+    for (u64 q = ((u64)1 << d) | 1; q < ((u64)2 << d); q += 2) {
+        if (!hw_irreducible(q, d)) continue;
+        bool prim = true;
+        for (int i = 0; i < np && prim; i++)
+            if (hw_pow(2, M / ps[i], q, d) == 1) prim = false;
+        if (prim) return q;
+    }
+    return 0;
+}
 u64 cached_primitive(int d) {
     static std::mutex mu;
-    static u64 cache[33] = {0};
+    static u64 cache[DMAX_WIDE + 1] = {0};
     std::lock_guard<std::mutex> lk(mu);
-    if (!cache[d]) cache[d] = h_primitive(d);
+    if (!cache[d]) cache[d] = d <= 32 ? h_primitive(d) : hw_primitive(d);
     return cache[d];
+}
+
+// the wide field of degree d on its primitive polynomial; false if the low
+// part of the modulus is too dense or too high for the two-fold reduction
+bool wide_field(int d, WideField &F) {
+    const u64 q = cached_primitive(d);
+    if (!q) return false;
+    const u64 qlow = q ^ ((u64)1 << d);
+    F.d = d;
+    F.M = ((u64)1 << d) - 1;
+    F.qlow = qlow;
+    F.nt = 0;
+    int e = 0;
+    for (int b = 0; b < d; b++)
+        if ((qlow >> b) & 1) {
+            if (F.nt == 12) return false;
+            F.t[F.nt++] = b;
+            e = b;
+        }
+    return 2 * e <= d;
 }
 u64 h_gcd(u64 a, u64 b) { while (b) { u64 t = a % b; a = b; b = t; } return a; }
 
@@ -327,13 +586,14 @@ u64 h_gcd(u64 a, u64 b) { while (b) { u64 t = a % b; a = b; b = t; } return a; }
 extern "C" {
 
 uint64_t gf2e_primitive_poly(int d) {
-    if (d < 2 || d > 32) return 0;
+    if (d < 2 || d > DMAX_WIDE) return 0;
     return cached_primitive(d);
 }
 
 int gf2e_sieve_workspace_size(int dmax, size_t *bytes) {
-    if (dmax < 2 || dmax > DMAX || !bytes) return gf2e::invalid("dmax must be in 2..%d", DMAX);
-    *bytes = layout_for(dmax).total;
+    if (dmax < 2 || dmax > DMAX_WIDE || !bytes)
+        return gf2e::invalid("dmax must be in 2..%d", DMAX_WIDE);
+    *bytes = layout().off_region + region_want(2, dmax);
     return GF2E_OK;
 }
 
@@ -347,35 +607,62 @@ int gf2e_sieve_fill(uint64_t *best_dev, uint64_t smax, void *stream) {
 
 int gf2e_sieve_run(uint64_t r, int dmin, int dmax, uint64_t smax, uint64_t *best_dev,
                    void *workspace, size_t ws_bytes, void *stream) {
-    if (dmin < 2 || dmax > DMAX || dmin > dmax)
-        return gf2e::invalid("degrees must satisfy 2 <= dmin <= dmax <= %d", DMAX);
+    if (dmin < 2 || dmax > DMAX_WIDE || dmin > dmax)
+        return gf2e::invalid("degrees must satisfy 2 <= dmin <= dmax <= %d", DMAX_WIDE);
     if (!best_dev || !workspace || smax < 1 || r < 3)
         return gf2e::invalid("gf2e_sieve_run: bad arguments");
-    Layout lay = layout_for(dmax);
-    if (ws_bytes < lay.total)
-        return gf2e::invalid("sieve workspace %zu < %zu bytes", ws_bytes, lay.total);
+    const Layout lay = layout();
+    const size_t need = lay.off_region + region_min(dmin, dmax);
+    if (ws_bytes < need) return gf2e::invalid("sieve workspace %zu < %zu bytes", ws_bytes, need);
+    const size_t region = ws_bytes - lay.off_region;
     // host-side checks and setup for every degree before any launch
     const int strip_log = gf2e::tune_current().sieve_strip_log;
     const u64 strip_w = (u64)1 << strip_log;
     std::vector<DegreeArgs> args;
+    std::vector<WideArgs> wargs;          // one per (wide degree, slice)
+    const int wfrom = wide_from();
     for (int d = dmin; d <= dmax; d++) {
-        DegreeArgs a;
-        memset(&a, 0, sizeof a);
-        a.d = d;
-        a.M = ((u64)1 << d) - 1;
-        a.q = (u32)cached_primitive(d);
-        a.rmod = r % a.M;
-        a.smax = smax;
-        a.strip = strip_w;
-        if (h_gcd(a.rmod ? a.rmod : a.M, a.M) != 1) {
+        const u64 M = ((u64)1 << d) - 1, rmod = r % M;
+        if (h_gcd(rmod ? rmod : M, M) != 1) {
             gf2e::set_error("d=%d: gcd(r, 2^d-1) != 1; unsupported r", d);
             return GF2E_ERR_UNSUPPORTED_R;
         }
-        u64 ps[16];
-        int np = h_prime_factors((u64)d, ps);
-        a.nsub = np;
-        for (int i = 0; i < np; i++) a.subq[i] = a.M / (((u64)1 << (d / ps[i])) - 1);
-        args.push_back(a);
+        u64 ps[16], subq[6];
+        const int np = h_prime_factors((u64)d, ps);
+        for (int i = 0; i < np; i++) subq[i] = M / (((u64)1 << (d / ps[i])) - 1);
+        if (d < wfrom) {
+            DegreeArgs a;
+            memset(&a, 0, sizeof a);
+            a.d = d;
+            a.M = M;
+            a.q = (u32)cached_primitive(d);
+            a.rmod = rmod;
+            a.smax = smax;
+            a.strip = strip_w;
+            a.nsub = np;
+            for (int i = 0; i < np; i++) a.subq[i] = subq[i];
+            args.push_back(a);
+            continue;
+        }
+        WideArgs w;
+        memset(&w, 0, sizeof w);
+        if (!wide_field(d, w.F)) {
+            gf2e::set_error("d=%d: primitive polynomial unsuitable for the wide field", d);
+            return GF2E_ERR_INTERNAL;
+        }
+        w.rmod = rmod;
+        w.smax = smax;
+        w.nsub = np;
+        for (int i = 0; i < np; i++) w.subq[i] = subq[i];
+        // log-table slices: as few as the table region allows
+        const u64 values = (u64)1 << d, cap = (u64)(region / wide_entry_bytes(d));
+        const u64 nslice = (values + cap - 1) / cap, len = (values + nslice - 1) / nslice;
+        for (u64 b = 0; b < nslice; b++) {
+            w.lo = b * len;
+            w.len = std::min(len, values - w.lo);
+            w.first_slice = b == 0;
+            wargs.push_back(w);
+        }
     }
     {   // k_strip may take up to 2^STRIP_LOG_MAX entries of shared memory
         static bool attr_done[64] = {false};
@@ -390,20 +677,41 @@ int gf2e_sieve_run(uint64_t r, int dmin, int dmax, uint64_t smax, uint64_t *best
     }
     cudaStream_t st = (cudaStream_t)stream;
     char *ws = (char *)workspace;
-    u32 *A = (u32 *)(ws + lay.off_A);
-    u32 *L = (u32 *)(ws + lay.off_L);
     Prog *strip = (Prog *)(ws + lay.off_strip);
     Prog *heavy = (Prog *)(ws + lay.off_heavy);
     Counters *cnt = (Counters *)(ws + lay.off_cnt);
+    char *reg = ws + lay.off_region;
     cudaError_t e = cudaMemsetAsync(cnt, 0, sizeof(Counters), st);
     if (e != cudaSuccess) return gf2e::cuda_status(e, "sieve counters");
     unsigned long long *best = (unsigned long long *)best_dev;
-    for (const DegreeArgs &a : args) {
-        u64 nchunk = (a.M + 31) >> 5;
-        k_tables<<<gf2e::grid_for(nchunk, 256, 16), 256, 0, st>>>(A, L, a.d, a.q, a.M);
-        GF2E_CHECK_LAUNCH("k_tables");
-        k_classes<<<gf2e::grid_for(a.M, 256, 16), 256, 0, st>>>(A, L, a, best, strip, heavy, cnt);
-        GF2E_CHECK_LAUNCH("k_classes");
+    if (!args.empty()) {
+        u32 *A = (u32 *)reg;
+        u32 *L = (u32 *)(reg + dense_table_bytes(std::min(dmax, wfrom - 1)));
+        for (const DegreeArgs &a : args) {
+            u64 nchunk = (a.M + 31) >> 5;
+            k_tables<<<gf2e::grid_for(nchunk, 256, 16), 256, 0, st>>>(A, L, a.d, a.q, a.M);
+            GF2E_CHECK_LAUNCH("k_tables");
+            k_classes<<<gf2e::grid_for(a.M, 256, 16), 256, 0, st>>>(A, L, a, best, strip, heavy,
+                                                                    cnt);
+            GF2E_CHECK_LAUNCH("k_classes");
+        }
+    }
+    for (const WideArgs &w : wargs) {
+        const u64 nchunk = (w.F.M + 63) >> 6;
+        if (w.F.d <= 32) {
+            k_wide_slice<u32><<<gf2e::grid_for(nchunk, 256, 16), 256, 0, st>>>(
+                (u32 *)reg, w.F, w.lo, w.len);
+            GF2E_CHECK_LAUNCH("k_wide_slice");
+            k_wide_classes<u32><<<gf2e::grid_for(w.F.M, 256, 16), 256, 0, st>>>(
+                (const u32 *)reg, w, best, heavy, cnt);
+        } else {
+            k_wide_slice<u64><<<gf2e::grid_for(nchunk, 256, 16), 256, 0, st>>>(
+                (u64 *)reg, w.F, w.lo, w.len);
+            GF2E_CHECK_LAUNCH("k_wide_slice");
+            k_wide_classes<u64><<<gf2e::grid_for(w.F.M, 256, 16), 256, 0, st>>>(
+                (const u64 *)reg, w, best, heavy, cnt);
+        }
+        GF2E_CHECK_LAUNCH("k_wide_classes");
     }
     k_heavy<<<gf2e::sm_count() * 16, 256, 0, st>>>(heavy, cnt, smax, best);
     GF2E_CHECK_LAUNCH("k_heavy");
@@ -429,8 +737,9 @@ int gf2e_sieve_run(uint64_t r, int dmin, int dmax, uint64_t smax, uint64_t *best
 
 int gf2e_sieve_stats(const void *workspace, int dmax, uint64_t *classes_host,
                      uint64_t *marks_host, void *stream) {
-    if (!workspace || dmax < 2 || dmax > DMAX) return gf2e::invalid("gf2e_sieve_stats: bad arguments");
-    Layout lay = layout_for(dmax);
+    if (!workspace || dmax < 2 || dmax > DMAX_WIDE)
+        return gf2e::invalid("gf2e_sieve_stats: bad arguments");
+    const Layout lay = layout();
     Counters c;
     cudaStream_t st = (cudaStream_t)stream;
     cudaError_t e = cudaMemcpyAsync(&c, (const char *)workspace + lay.off_cnt, sizeof c,

@@ -12,10 +12,11 @@
 //   <prefix>.found.cert     "s d p<hex>" ascending s (default on)
 //   <prefix>.found.bin      LE u64 key per s = 1..smax, UINT64_MAX = none (--found)
 // Degrees up to 31 run on dense tables in HBM (the reference needs its
-// bucketed low-memory mode beyond d = 29 on an 8 GB GPU).  Checkpoint flags
-// (--checkpoint, --checkpoint-mins, --checkpoint-keep, --resume) are
-// accepted and ignored with a note: the whole run finishes in seconds.
-// Degrees above 31 (the reference's wide-field mode) are refused.
+// bucketed low-memory mode beyond d = 29 on an 8 GB GPU); degrees 32..40 on
+// the wide path (64-bit elements, the log table in slices of at most
+// GF2E_SIEVE_WIDE_GB, default 64 GB: one slice up to d = 33).  Checkpoint
+// flags (--checkpoint, --checkpoint-mins, --checkpoint-keep, --resume) are
+// accepted and ignored with a note.
 #include <cinttypes>
 #include <cstdio>
 #include <cstdlib>
@@ -56,7 +57,7 @@ static void run_gpu(u64 r, int depth, u64 smax, int min_depth, std::vector<u64> 
     die_on(gf2e_sieve_run(r, min_depth, depth, smax, (u64 *)dbest, ws, ws_bytes, nullptr),
            "sieve");
     double t1 = now_s();
-    u64 classes[32], marks[32];
+    u64 classes[41], marks[41];
     die_on(gf2e_sieve_stats(ws, depth, classes, marks, nullptr), "stats");
     for (int d = min_depth; d <= depth; d++)
         fprintf(stderr, "d=%2d done: %" PRIu64 " classes, %" PRIu64 " marks\n", d, classes[d],
@@ -141,7 +142,7 @@ static int selftest() {
 int main(int argc, char **argv) {
     if (argc >= 2 && !strcmp(argv[1], "--selftest")) return selftest();
     if (argc >= 2 && !strcmp(argv[1], "--selftest-lowmem")) {
-        fprintf(stderr, "note: the bucketed low-memory mode is not needed for d <= 31; "
+        fprintf(stderr, "note: degrees <= 31 use dense tables, 32..40 sliced log tables; "
                         "running the standard selftest\n");
         return selftest();
     }
@@ -183,15 +184,14 @@ int main(int argc, char **argv) {
         else if ((!strcmp(argv[a], "--checkpoint") || !strcmp(argv[a], "--checkpoint-mins") ||
                   !strcmp(argv[a], "--checkpoint-keep") || !strcmp(argv[a], "--resume") ||
                   !strcmp(argv[a], "--gpus")) && a + 1 < argc) {
-            fprintf(stderr, "note: %s %s ignored (one GPU; degrees <= 31 need no checkpoint)\n",
-                    argv[a], argv[a + 1]);
+            fprintf(stderr, "note: %s %s ignored (one GPU, no checkpoints)\n", argv[a],
+                    argv[a + 1]);
             a++;
         } else fprintf(stderr, "warning: ignoring unknown argument '%s'\n", argv[a]);
     }
     if (min_depth < 2) min_depth = 2;
-    if (depth > 31) {
-        fprintf(stderr, "depth %d > 31 is not supported by this engine (dense tables only)\n",
-                depth);
+    if (depth > 40) {
+        fprintf(stderr, "depth %d > 40 is not supported by this engine\n", depth);
         return 1;
     }
     std::vector<u64> preload;

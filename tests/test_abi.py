@@ -61,7 +61,7 @@ def test_argument_errors_without_device(engine):
     assert L.gf2e_trin_square(8, 16, 4424, 5, None) == -1          # even r
     assert b"s <=" in L.gf2e_last_error() or b"r must" in L.gf2e_last_error()
     # sieve degree range and workspace size
-    assert L.gf2e_sieve_run(44687, 2, 32, 100, 8, 8, 1 << 30, None) == -1   # d <= 31
+    assert L.gf2e_sieve_run(44687, 2, 41, 100, 8, 8, 1 << 30, None) == -1   # d <= 40
     assert L.gf2e_sieve_run(44687, 2, 20, 100, 8, 8, 16, None) == -1
     # FFT plan range
     import ctypes
