@@ -183,36 +183,68 @@ struct DegreeArgs {
     u64 strip;                            // strip width (entries of best[] per CTA)
 };
 
+// j is the least element of its cyclotomic coset {j 2^i mod M}
+GF2E_DEV bool coset_least(u64 j, int d, u64 M) {
+    u64 jj = j;
+    for (int i = 1; i < d; i++) {
+        jj = ((jj << 1) | (jj >> (d - 1))) & M;
+        if (jj < j) return false;
+    }
+    return true;
+}
+
+// Calls work(j, true) for every coset leader j in [1, M) (about 1 in d of
+// the j), with full warps: each warp tests 32 consecutive j at a time and
+// queues the leaders in shared memory (wq: 64 entries per warp), running
+// `work` on 32 of them whenever 32 are queued, so the leader path does not
+// execute with one active lane per warp.  work(j, false) pads the final
+// partial batch; every lane of the warp calls work together.
+template <typename Work>
+GF2E_DEV void for_each_leader(u64 M, int d, u64 *wq, Work &&work) {
+    const int lane = threadIdx.x & 31;
+    const u64 gw = ((u64)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const u64 nw = ((u64)gridDim.x * blockDim.x) >> 5;
+    int qn = 0;
+    for (u64 base = 1 + gw * 32; base < M; base += nw * 32) {
+        const u64 j = base + lane;
+        const bool lead = j < M && coset_least(j, d, M);
+        const unsigned b = __ballot_sync(0xffffffffu, lead);
+        if (lead) wq[qn + __popc(b & ((1u << lane) - 1u))] = j;
+        qn += __popc(b);
+        __syncwarp();
+        if (qn >= 32) {
+            const u64 jj = wq[qn - 32 + lane];
+            __syncwarp();
+            qn -= 32;
+            work(jj, true);
+        }
+    }
+    const u64 jj = lane < qn ? wq[lane] : 0;
+    work(jj, lane < qn);
+}
+
 __global__ void __launch_bounds__(256)
 k_classes(const u32 *__restrict__ A, const u32 *__restrict__ L, const DegreeArgs a,
           unsigned long long *__restrict__ best, Prog *__restrict__ strip, Prog *__restrict__ heavy,
           Counters *__restrict__ cnt) {
+    __shared__ u64 wq_all[8][64];
     const int d = a.d;
     const u64 M = a.M;
     unsigned long long my_classes = 0, my_marks = 0;
-    for (u64 j = (u64)blockIdx.x * blockDim.x + threadIdx.x + 1; j < M;
-         j += (u64)gridDim.x * blockDim.x) {
-        bool skip = false;
+    for_each_leader(M, d, wq_all[threadIdx.x >> 5], [&](u64 j, bool valid) {
+        if (!valid) return;
         for (int k = 0; k < a.nsub; k++)
-            if (j % a.subq[k] == 0) { skip = true; break; }
-        if (skip) continue;
-        u64 jj = j;
-        bool minimal = true;
-        for (int i = 1; i < d; i++) {
-            jj = ((jj << 1) | (jj >> (d - 1))) & M;
-            if (jj < j) { minimal = false; break; }
-        }
-        if (!minimal) continue;
+            if (j % a.subq[k] == 0) return;
         my_classes++;
         u64 u = mod_mersenne(j * a.rmod, d, M);
-        if (u == 0) continue;
+        if (u == 0) return;
         u64 v = L[A[u] ^ 1u];
         u64 gg = gcd_u64(j, M);
-        if (v % gg) continue;
+        if (v % gg) return;
         u64 n = M / gg;
         u64 s0 = (inv_mod(j / gg, n) * (v / gg)) % n;
         u64 first = s0 ? s0 : n;
-        if (first > a.smax) continue;
+        if (first > a.smax) return;
         u64 count = (a.smax - first) / n + 1;
         // minimal polynomial of beta = x^j: first linear dependency among
         // beta^0..beta^d over GF(2)
@@ -235,7 +267,7 @@ k_classes(const u32 *__restrict__ A, const u32 *__restrict__ L, const DegreeArgs
         }
         if (!((mask >> d) & 1) || !(mask & 1)) {        // cannot happen
             atomicAdd(&cnt->bad, 1ull);
-            continue;
+            return;
         }
         const unsigned long long key = ((u64)d << 48) | mask;
         my_marks += count;
@@ -250,7 +282,7 @@ k_classes(const u32 *__restrict__ A, const u32 *__restrict__ L, const DegreeArgs
             if (slot < HCAP) heavy[slot] = Prog{first, n, key};
             else atomicAdd(&cnt->overflow, 1ull);
         }
-    }
+    });
     // warp-aggregated statistics
     for (int o = 16; o; o >>= 1) {
         my_classes += __shfl_down_sync(0xffffffffu, my_classes, o);
@@ -399,35 +431,26 @@ template <typename E>
 __global__ void __launch_bounds__(256)
 k_wide_classes(const E *__restrict__ L, const WideArgs a, unsigned long long *__restrict__ best,
                Prog *__restrict__ heavy, Counters *__restrict__ cnt) {
+    __shared__ u64 wq_all[8][64];
     const int d = a.F.d;
     const u64 M = a.F.M;
     unsigned long long my_classes = 0, my_marks = 0;
-    for (u64 j = (u64)blockIdx.x * blockDim.x + threadIdx.x + 1; j < M;
-         j += (u64)gridDim.x * blockDim.x) {
-        // least element of its cyclotomic coset {j 2^i mod M}
-        u64 jj = j;
-        bool minimal = true;
-        for (int i = 1; i < d; i++) {
-            jj = ((jj << 1) | (jj >> (d - 1))) & M;
-            if (jj < j) { minimal = false; break; }
-        }
-        if (!minimal) continue;
-        bool sub = false;
+    for_each_leader(M, d, wq_all[threadIdx.x >> 5], [&](u64 j, bool valid) {
+        if (!valid) return;
         for (int k = 0; k < a.nsub; k++)
-            if (j % a.subq[k] == 0) { sub = true; break; }
-        if (sub) continue;
+            if (j % a.subq[k] == 0) return;
         if (a.first_slice) my_classes++;
         const u64 u = mulmod_mersenne(j, a.rmod, d, M);
-        if (u == 0) continue;
+        if (u == 0) return;
         const u64 w = wf_powx(u, a.F) ^ 1ull;            // x^(j r) + 1
-        if (w - a.lo >= a.len) continue;                 // another slice's lookup
+        if (w - a.lo >= a.len) return;                   // another slice's lookup
         const u64 v = (u64)L[w - a.lo];
         const u64 gg = gcd_u64(j, M);
-        if (v % gg) continue;
+        if (v % gg) return;
         const u64 n = M / gg;
         const u64 s0 = mulmod_u64(inv_mod(j / gg, n), v / gg, n);
         const u64 first = s0 ? s0 : n;
-        if (first > a.smax) continue;
+        if (first > a.smax) return;
         const u64 count = (a.smax - first) / n + 1;
         // minimal polynomial of beta = x^j: first linear dependency among
         // beta^0..beta^d over GF(2)
@@ -449,7 +472,7 @@ k_wide_classes(const E *__restrict__ L, const WideArgs a, unsigned long long *__
         }
         if (!((mask >> d) & 1) || !(mask & 1)) {        // cannot happen
             atomicAdd(&cnt->bad, 1ull);
-            continue;
+            return;
         }
         const unsigned long long key = ((u64)d << 48) | mask;
         my_marks += count;
@@ -460,7 +483,7 @@ k_wide_classes(const E *__restrict__ L, const WideArgs a, unsigned long long *__
             if (slot < HCAP) heavy[slot] = Prog{first, n, key};
             else atomicAdd(&cnt->overflow, 1ull);
         }
-    }
+    });
     for (int o = 16; o; o >>= 1) {
         my_classes += __shfl_down_sync(0xffffffffu, my_classes, o);
         my_marks += __shfl_down_sync(0xffffffffu, my_marks, o);

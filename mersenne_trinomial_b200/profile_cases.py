@@ -4,6 +4,7 @@ capture (inputs larger than L2, a few GB at most, a handful of launches).
     python -m mersenne_trinomial_b200.profile_cases square [--r R] [--n N] [--k K]
     python -m mersenne_trinomial_b200.profile_cases fft [--m M]
     python -m mersenne_trinomial_b200.profile_cases sieve [--r R] [--depth D]
+    python -m mersenne_trinomial_b200.profile_cases sieve_wide --depth D --dmin D --wide-from W
     python -m mersenne_trinomial_b200.profile_cases mul [--m M]
     python -m mersenne_trinomial_b200.profile_cases gcd|hgcd [--r R]
     python -m mersenne_trinomial_b200.profile_cases scan [--r R --n N --k K]
@@ -11,6 +12,7 @@ capture (inputs larger than L2, a few GB at most, a handful of launches).
 from __future__ import annotations
 
 import argparse
+import os
 import sys
 import time
 
@@ -107,18 +109,30 @@ def case_sieve(a):
     M.run_sieve(a.r, a.depth, smax)
 
 
+def case_sieve_wide(a):
+    """Degrees dmin..depth on the wide path (64-bit elements, sliced log
+    table), from degree `wide_from` on."""
+    os.environ["GF2E_SIEVE_WIDE_FROM"] = str(a.wide_from)
+    smax = a.r // 2
+    M.run_sieve(a.r, a.depth, smax, dmin=a.dmin)
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser()
-    ap.add_argument("case", choices=["square", "fft", "mul", "sieve", "gcd", "hgcd", "scan"])
+    ap.add_argument("case", choices=["square", "fft", "mul", "sieve", "sieve_wide", "gcd", "hgcd",
+                                     "scan"])
     ap.add_argument("--r", type=int, default=136279841)
     ap.add_argument("--n", type=int, default=8)
     ap.add_argument("--k", type=int, default=3)
     ap.add_argument("--m", type=int, default=22)
     ap.add_argument("--depth", type=int, default=24)
+    ap.add_argument("--dmin", type=int, default=2)
+    ap.add_argument("--wide-from", type=int, default=32)
     a = ap.parse_args(argv)
     t0 = time.perf_counter()
     {"square": case_square, "fft": case_fft, "mul": case_mul, "sieve": case_sieve,
-     "gcd": case_gcd, "hgcd": case_hgcd, "scan": case_scan}[a.case](a)
+     "sieve_wide": case_sieve_wide, "gcd": case_gcd, "hgcd": case_hgcd,
+     "scan": case_scan}[a.case](a)
     print(f"{a.case}: done in {time.perf_counter() - t0:.3f} s")
     return 0
 
