@@ -66,6 +66,7 @@ struct Counters {
     unsigned long long nstrip, nheavy, overflow, bad;
     unsigned long long classes[DMAX_WIDE + 1];
     unsigned long long marks[DMAX_WIDE + 1];
+    unsigned long long nlist;             // wide leader list fill
 };
 
 // workspace: progression lists and counters first, then the table region
@@ -111,10 +112,36 @@ size_t region_min(int dmin, int dmax) {
     if (dmax >= w) need = std::max<size_t>(need, (size_t)1 << 28);
     return need;
 }
+// number of irreducible polynomials of degree d over GF(2) (the coset
+// leaders of degree d): (1/d) sum over k | d of mu(d/k) 2^k
+u64 irreducible_count(int d) {
+    long long sum = 0;
+    for (int k = 1; k <= d; k++) {
+        if (d % k) continue;
+        int n = d / k, mu = 1;
+        for (int p = 2; p <= n; p++) {
+            if (n % p) continue;
+            n /= p;
+            if (n % p == 0) { mu = 0; break; }
+            mu = -mu;
+        }
+        sum += mu * (long long)(1ull << k);
+    }
+    return (u64)(sum / d);
+}
+
+// wide leader list: (j, x^(j r) + 1) per coset leader, 16 bytes each; used
+// when it fits in the slice budget (d <= 37 by default)
+size_t leader_list_bytes(int d) { return ((size_t)irreducible_count(d) * 16 + 255) & ~(size_t)255; }
+bool leader_list_wanted(int d) { return leader_list_bytes(d) <= wide_budget(); }
+
 size_t region_want(int dmin, int dmax) {
     size_t want = region_min(dmin, dmax);
-    if (dmax >= wide_from())
-        want = std::max(want, std::min(((size_t)1 << dmax) * wide_entry_bytes(dmax), wide_budget()));
+    if (dmax >= wide_from()) {
+        size_t w = std::min(((size_t)1 << dmax) * wide_entry_bytes(dmax), wide_budget());
+        if (leader_list_wanted(dmax)) w += leader_list_bytes(dmax);
+        want = std::max(want, w);
+    }
     return want;
 }
 
@@ -193,34 +220,40 @@ GF2E_DEV bool coset_least(u64 j, int d, u64 M) {
     return true;
 }
 
-// Calls work(j, true) for every coset leader j in [1, M) (about 1 in d of
-// the j), with full warps: each warp tests 32 consecutive j at a time and
-// queues the leaders in shared memory (wq: 64 entries per warp), running
-// `work` on 32 of them whenever 32 are queued, so the leader path does not
-// execute with one active lane per warp.  work(j, false) pads the final
-// partial batch; every lane of the warp calls work together.
-template <typename Work>
-GF2E_DEV void for_each_leader(u64 M, int d, u64 *wq, Work &&work) {
+// Calls work(i, true) for every i in [begin, end) with pred(i), with full
+// warps: each warp tests 32 consecutive i at a time and queues the selected
+// ones in shared memory (wq: 64 entries per warp), running `work` on 32 of
+// them whenever 32 are queued, so a rare, expensive path does not execute
+// with one active lane per warp.  work(i, false) pads the final partial
+// batch; every lane of the warp calls work together.
+template <typename Pred, typename Work>
+GF2E_DEV void for_each_selected(u64 begin, u64 end, u64 *wq, Pred &&pred, Work &&work) {
     const int lane = threadIdx.x & 31;
     const u64 gw = ((u64)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const u64 nw = ((u64)gridDim.x * blockDim.x) >> 5;
     int qn = 0;
-    for (u64 base = 1 + gw * 32; base < M; base += nw * 32) {
-        const u64 j = base + lane;
-        const bool lead = j < M && coset_least(j, d, M);
-        const unsigned b = __ballot_sync(0xffffffffu, lead);
-        if (lead) wq[qn + __popc(b & ((1u << lane) - 1u))] = j;
+    for (u64 base = begin + gw * 32; base < end; base += nw * 32) {
+        const u64 i = base + lane;
+        const bool sel = i < end && pred(i);
+        const unsigned b = __ballot_sync(0xffffffffu, sel);
+        if (sel) wq[qn + __popc(b & ((1u << lane) - 1u))] = i;
         qn += __popc(b);
         __syncwarp();
         if (qn >= 32) {
-            const u64 jj = wq[qn - 32 + lane];
+            const u64 ii = wq[qn - 32 + lane];
             __syncwarp();
             qn -= 32;
-            work(jj, true);
+            work(ii, true);
         }
     }
-    const u64 jj = lane < qn ? wq[lane] : 0;
-    work(jj, lane < qn);
+    const u64 ii = lane < qn ? wq[lane] : 0;
+    work(ii, lane < qn);
+}
+
+// every coset leader j in [1, M) (about 1 in d of the j)
+template <typename Work>
+GF2E_DEV void for_each_leader(u64 M, int d, u64 *wq, Work &&work) {
+    for_each_selected(1, M, wq, [&](u64 j) { return coset_least(j, d, M); }, work);
 }
 
 __global__ void __launch_bounds__(256)
@@ -427,6 +460,67 @@ struct WideArgs {
     u64 subq[6];
 };
 
+// the class of leader j whose Zech logarithm is v: its progression of s,
+// and when it reaches s <= smax the minimal polynomial and the marks
+GF2E_DEV void wide_mark(u64 j, u64 v, const WideArgs &a, unsigned long long *__restrict__ best,
+                        Prog *__restrict__ heavy, Counters *__restrict__ cnt,
+                        unsigned long long &my_marks) {
+    const int d = a.F.d;
+    const u64 M = a.F.M;
+    const u64 gg = gcd_u64(j, M);
+    if (v % gg) return;
+    const u64 n = M / gg;
+    const u64 s0 = mulmod_u64(inv_mod(j / gg, n), v / gg, n);
+    const u64 first = s0 ? s0 : n;
+    if (first > a.smax) return;
+    const u64 count = (a.smax - first) / n + 1;
+    // minimal polynomial of beta = x^j: first linear dependency among
+    // beta^0..beta^d over GF(2)
+    const u64 beta = wf_powx(j, a.F);
+    u64 prow[DMAX_WIDE + 1], ptag[DMAX_WIDE + 1];
+    int pbit[DMAX_WIDE + 1];
+    int np = 0;
+    u64 mask = 0, pw = 1;
+    for (int k = 0; k <= d; k++) {
+        u64 row = pw, tag = 1ull << k;
+        for (int p = 0; p < np; p++)
+            if ((row >> pbit[p]) & 1) { row ^= prow[p]; tag ^= ptag[p]; }
+        if (row == 0) { mask = tag; break; }
+        pbit[np] = 63 - __clzll(row);
+        prow[np] = row;
+        ptag[np] = tag;
+        np++;
+        pw = wf_mul(pw, beta, a.F);
+    }
+    if (!((mask >> d) & 1) || !(mask & 1)) {        // cannot happen
+        atomicAdd(&cnt->bad, 1ull);
+        return;
+    }
+    const unsigned long long key = ((u64)d << 48) | mask;
+    my_marks += count;
+    if (count <= INLINE) {
+        for (u64 s = first; s <= a.smax; s += n) atomicMin(&best[s], key);
+    } else {
+        unsigned long long slot = atomicAdd(&cnt->nheavy, 1ull);
+        if (slot < HCAP) heavy[slot] = Prog{first, n, key};
+        else atomicAdd(&cnt->overflow, 1ull);
+    }
+}
+
+GF2E_DEV void add_stats(unsigned long long my_classes, unsigned long long my_marks, int d,
+                        Counters *cnt) {
+    for (int o = 16; o; o >>= 1) {
+        my_classes += __shfl_down_sync(0xffffffffu, my_classes, o);
+        my_marks += __shfl_down_sync(0xffffffffu, my_marks, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        if (my_classes) atomicAdd(&cnt->classes[d], my_classes);
+        if (my_marks) atomicAdd(&cnt->marks[d], my_marks);
+    }
+}
+
+// one slice without a leader list: every leader recomputes x^(j r) + 1 and
+// looks it up when it falls in this slice
 template <typename E>
 __global__ void __launch_bounds__(256)
 k_wide_classes(const E *__restrict__ L, const WideArgs a, unsigned long long *__restrict__ best,
@@ -444,54 +538,62 @@ k_wide_classes(const E *__restrict__ L, const WideArgs a, unsigned long long *__
         if (u == 0) return;
         const u64 w = wf_powx(u, a.F) ^ 1ull;            // x^(j r) + 1
         if (w - a.lo >= a.len) return;                   // another slice's lookup
-        const u64 v = (u64)L[w - a.lo];
-        const u64 gg = gcd_u64(j, M);
-        if (v % gg) return;
-        const u64 n = M / gg;
-        const u64 s0 = mulmod_u64(inv_mod(j / gg, n), v / gg, n);
-        const u64 first = s0 ? s0 : n;
-        if (first > a.smax) return;
-        const u64 count = (a.smax - first) / n + 1;
-        // minimal polynomial of beta = x^j: first linear dependency among
-        // beta^0..beta^d over GF(2)
-        const u64 beta = wf_powx(j, a.F);
-        u64 prow[DMAX_WIDE + 1], ptag[DMAX_WIDE + 1];
-        int pbit[DMAX_WIDE + 1];
-        int np = 0;
-        u64 mask = 0, pw = 1;
-        for (int k = 0; k <= d; k++) {
-            u64 row = pw, tag = 1ull << k;
-            for (int p = 0; p < np; p++)
-                if ((row >> pbit[p]) & 1) { row ^= prow[p]; tag ^= ptag[p]; }
-            if (row == 0) { mask = tag; break; }
-            pbit[np] = 63 - __clzll(row);
-            prow[np] = row;
-            ptag[np] = tag;
-            np++;
-            pw = wf_mul(pw, beta, a.F);
+        wide_mark(j, (u64)L[w - a.lo], a, best, heavy, cnt, my_marks);
+    });
+    add_stats(my_classes, my_marks, d, cnt);
+}
+
+// once per degree: the leader list (j, x^(j r) + 1) of every class
+__global__ void __launch_bounds__(256)
+k_wide_leaders(const WideArgs a, ulonglong2 *__restrict__ list, u64 cap,
+               Counters *__restrict__ cnt) {
+    __shared__ u64 wq_all[8][64];
+    const int d = a.F.d;
+    const u64 M = a.F.M;
+    const int lane = threadIdx.x & 31;
+    unsigned long long my_classes = 0;
+    for_each_leader(M, d, wq_all[threadIdx.x >> 5], [&](u64 j, bool valid) {
+        bool keep = valid;
+        for (int k = 0; k < a.nsub && keep; k++)
+            if (j % a.subq[k] == 0) keep = false;
+        u64 w = 0;
+        if (keep) {
+            my_classes++;
+            const u64 u = mulmod_mersenne(j, a.rmod, d, M);
+            if (u == 0) keep = false;
+            else w = wf_powx(u, a.F) ^ 1ull;
         }
-        if (!((mask >> d) & 1) || !(mask & 1)) {        // cannot happen
-            atomicAdd(&cnt->bad, 1ull);
-            return;
-        }
-        const unsigned long long key = ((u64)d << 48) | mask;
-        my_marks += count;
-        if (count <= INLINE) {
-            for (u64 s = first; s <= a.smax; s += n) atomicMin(&best[s], key);
-        } else {
-            unsigned long long slot = atomicAdd(&cnt->nheavy, 1ull);
-            if (slot < HCAP) heavy[slot] = Prog{first, n, key};
+        const unsigned b = __ballot_sync(0xffffffffu, keep);
+        if (!b) return;
+        unsigned long long base = 0;
+        if (lane == 0) base = atomicAdd(&cnt->nlist, (unsigned long long)__popc(b));
+        base = __shfl_sync(0xffffffffu, base, 0);
+        if (keep) {
+            const u64 idx = base + __popc(b & ((1u << lane) - 1u));
+            if (idx < cap) list[idx] = make_ulonglong2(j, w);
             else atomicAdd(&cnt->overflow, 1ull);
         }
     });
-    for (int o = 16; o; o >>= 1) {
-        my_classes += __shfl_down_sync(0xffffffffu, my_classes, o);
-        my_marks += __shfl_down_sync(0xffffffffu, my_marks, o);
-    }
-    if ((threadIdx.x & 31) == 0) {
-        if (my_classes) atomicAdd(&cnt->classes[d], my_classes);
-        if (my_marks) atomicAdd(&cnt->marks[d], my_marks);
-    }
+    add_stats(my_classes, 0, d, cnt);
+}
+
+// one slice with the leader list: the entries whose lookup lies in it
+template <typename E>
+__global__ void __launch_bounds__(256)
+k_wide_match(const E *__restrict__ L, const ulonglong2 *__restrict__ list, u64 cap,
+             const WideArgs a, unsigned long long *__restrict__ best, Prog *__restrict__ heavy,
+             Counters *__restrict__ cnt) {
+    __shared__ u64 wq_all[8][64];
+    const u64 n = min((u64)cnt->nlist, cap);
+    unsigned long long my_marks = 0;
+    for_each_selected(
+        0, n, wq_all[threadIdx.x >> 5], [&](u64 i) { return list[i].y - a.lo < a.len; },
+        [&](u64 i, bool valid) {
+            if (!valid) return;
+            const ulonglong2 e = list[i];
+            wide_mark(e.x, (u64)L[e.y - a.lo], a, best, heavy, cnt, my_marks);
+        });
+    add_stats(0, my_marks, a.F.d, cnt);
 }
 
 // ---- host-side field setup (gf2_field_setup.h:14-58 restated)
@@ -642,7 +744,13 @@ int gf2e_sieve_run(uint64_t r, int dmin, int dmax, uint64_t smax, uint64_t *best
     const int strip_log = gf2e::tune_current().sieve_strip_log;
     const u64 strip_w = (u64)1 << strip_log;
     std::vector<DegreeArgs> args;
-    std::vector<WideArgs> wargs;          // one per (wide degree, slice)
+    struct WidePlan {
+        WideArgs a;
+        bool list;                        // leader list at the region start
+        size_t slice_off;                 // log-table slice offset in the region
+        u64 list_cap;
+    };
+    std::vector<WidePlan> wargs;          // one per (wide degree, slice)
     const int wfrom = wide_from();
     for (int d = dmin; d <= dmax; d++) {
         const u64 M = ((u64)1 << d) - 1, rmod = r % M;
@@ -677,14 +785,18 @@ int gf2e_sieve_run(uint64_t r, int dmin, int dmax, uint64_t smax, uint64_t *best
         w.smax = smax;
         w.nsub = np;
         for (int i = 0; i < np; i++) w.subq[i] = subq[i];
-        // log-table slices: as few as the table region allows
-        const u64 values = (u64)1 << d, cap = (u64)(region / wide_entry_bytes(d));
+        // the leader list first in the region when it fits beside a slice of
+        // at least 256 MB, then log-table slices: as few as the rest allows
+        const size_t lb = leader_list_bytes(d);
+        const bool use_list = leader_list_wanted(d) && region >= lb + ((size_t)1 << 28);
+        const size_t slice_off = use_list ? lb : 0;
+        const u64 values = (u64)1 << d, cap = (u64)((region - slice_off) / wide_entry_bytes(d));
         const u64 nslice = (values + cap - 1) / cap, len = (values + nslice - 1) / nslice;
         for (u64 b = 0; b < nslice; b++) {
             w.lo = b * len;
             w.len = std::min(len, values - w.lo);
             w.first_slice = b == 0;
-            wargs.push_back(w);
+            wargs.push_back(WidePlan{w, use_list, slice_off, use_list ? irreducible_count(d) : 0});
         }
     }
     {   // k_strip may take up to 2^STRIP_LOG_MAX entries of shared memory
@@ -719,20 +831,38 @@ int gf2e_sieve_run(uint64_t r, int dmin, int dmax, uint64_t smax, uint64_t *best
             GF2E_CHECK_LAUNCH("k_classes");
         }
     }
-    for (const WideArgs &w : wargs) {
+    for (const WidePlan &P : wargs) {
+        const WideArgs &w = P.a;
         const u64 nchunk = (w.F.M + 63) >> 6;
+        const int gsl = gf2e::grid_for(nchunk, 256, 16), gcl = gf2e::grid_for(w.F.M, 256, 16);
+        ulonglong2 *list = (ulonglong2 *)reg;
+        char *slice = reg + P.slice_off;
+        if (P.list && w.first_slice) {
+            e = cudaMemsetAsync(&cnt->nlist, 0, sizeof(cnt->nlist), st);
+            if (e != cudaSuccess) return gf2e::cuda_status(e, "sieve leader list");
+            k_wide_leaders<<<gcl, 256, 0, st>>>(w, list, P.list_cap, cnt);
+            GF2E_CHECK_LAUNCH("k_wide_leaders");
+        }
         if (w.F.d <= 32) {
-            k_wide_slice<u32><<<gf2e::grid_for(nchunk, 256, 16), 256, 0, st>>>(
-                (u32 *)reg, w.F, w.lo, w.len);
+            k_wide_slice<u32><<<gsl, 256, 0, st>>>((u32 *)slice, w.F, w.lo, w.len);
             GF2E_CHECK_LAUNCH("k_wide_slice");
-            k_wide_classes<u32><<<gf2e::grid_for(w.F.M, 256, 16), 256, 0, st>>>(
-                (const u32 *)reg, w, best, heavy, cnt);
+            if (P.list) {
+                const u64 nl = P.list_cap;
+                k_wide_match<u32><<<gf2e::grid_for(nl, 256, 16), 256, 0, st>>>(
+                    (const u32 *)slice, list, P.list_cap, w, best, heavy, cnt);
+            } else {
+                k_wide_classes<u32><<<gcl, 256, 0, st>>>((const u32 *)slice, w, best, heavy, cnt);
+            }
         } else {
-            k_wide_slice<u64><<<gf2e::grid_for(nchunk, 256, 16), 256, 0, st>>>(
-                (u64 *)reg, w.F, w.lo, w.len);
+            k_wide_slice<u64><<<gsl, 256, 0, st>>>((u64 *)slice, w.F, w.lo, w.len);
             GF2E_CHECK_LAUNCH("k_wide_slice");
-            k_wide_classes<u64><<<gf2e::grid_for(w.F.M, 256, 16), 256, 0, st>>>(
-                (const u64 *)reg, w, best, heavy, cnt);
+            if (P.list) {
+                const u64 nl = P.list_cap;
+                k_wide_match<u64><<<gf2e::grid_for(nl, 256, 16), 256, 0, st>>>(
+                    (const u64 *)slice, list, P.list_cap, w, best, heavy, cnt);
+            } else {
+                k_wide_classes<u64><<<gcl, 256, 0, st>>>((const u64 *)slice, w, best, heavy, cnt);
+            }
         }
         GF2E_CHECK_LAUNCH("k_wide_classes");
     }
