@@ -387,6 +387,23 @@ def run_extras(torch, M, W, sq_rate=None):
             out["sieve_r136279841_d29"].update({"survivors": surv, "factors": smax - surv,
                                                 "reference_published_s": 7.52})
         del wsd
+    # the wide degrees 32..36 one at a time on the d <= 31 result (the
+    # reference's coarse_sieve_wide runs, coarse_sieve.log:42-124); a repeat
+    # of a degree is idempotent (min-merge of the same keys), so the second
+    # run is the timed one
+    published = {32: 162.86, 33: 593.48, 34: 2494.17, 35: None, 36: 44323.71}
+    wide = {}
+    for d in range(32, 37):
+        wsd = M.engine.SieveWorkspace(d)
+        rund = lambda: M.sieve_device(R, d, smax, best, dmin=d, fill=False, workspace=wsd)
+        rund()
+        ms = _ev_time(torch, rund, 1)
+        h = best[1:].cpu().numpy().view(np.uint64)
+        wide[f"d{d}"] = {"ms": ms, "workspace_GB": wsd.buf.nbytes / 2**30,
+                         "survivors": int(np.count_nonzero(h == np.uint64(0xFFFFFFFFFFFFFFFF))),
+                         "reference_published_s": published[d]}
+        del wsd
+    out["sieve_r136279841_wide_d32_d36"] = wide
     # config 1: r in [40000, 50000], d <= 20
     c1 = W.sieve_config(1)
     best1 = torch.empty(c1["smax"] + 1, dtype=torch.int64, device="cuda")
