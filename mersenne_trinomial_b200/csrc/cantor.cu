@@ -19,6 +19,8 @@
 // table is streamed from HBM.
 #include "gf2e_internal.cuh"
 
+#include <cstdlib>
+#include <cstring>
 #include <map>
 #include <mutex>
 #include <vector>
@@ -43,7 +45,28 @@ struct Pass {
     u32 wpt_log;     // log2 windows per tile (only when C == CH)
     u32 nops;
     u32 ops[MAXOPS];
+    u32 stream;      // 1: a streaming Taylor level over HBM (no tile), below
+    u32 sM, sA;      // its block 2^sM and chunk 2^sA elements
 };
+
+// A Taylor level at x^tau + x, tau = 2^(M-1-a), on aligned blocks of 2^M
+// elements in chunks of c = 2^a.  With the Cantor basis x^(2^h) + x is the
+// subspace polynomial of degree 2^h whenever h is a power of two, so the
+// conversion of 2^m coefficients to the products-of-subspace-polynomials
+// basis (what the reference's cascade of x^2 + x levels computes) splits
+// into m - h levels at tau = 2^h (h the largest power of two below m) and
+// two independent conversions of 2^h and 2^(m-h) coefficients (Gao and
+// Mateer's recursion): 52 levels at m = 24 instead of 276.
+//   forward: Hi[0..c) ^= Top; A[c..B) ^= Hi[0..B-c)   (B = 2^(M-1), A = the
+//            first half, Hi the second, Top its last c elements)
+//   inverse: A[c..B) ^= Hi[0..B-c); Hi[0..c) ^= Top
+// tau = 2 is the reference's x^2 + x level.  In a tile, the op word holds
+// the flag TAU_OP, the direction in bit 0, log2 block rows at bits 2..7 and
+// log2 chunk rows at bits 8..14.
+constexpr u32 TAU_OP = 1u << 17;
+__host__ __device__ inline u32 mktau(bool fwd, u32 log_rb, u32 log_rc) {
+    return TAU_OP | (fwd ? 0u : 1u) | (log_rb << 2) | (log_rc << 8);
+}
 
 // W(t) from byte tables: tab[k*256 + b] = XOR of basis[8k+j+1], bits j of b
 GF2E_DEV u64 twiddle(const u64 *__restrict__ tab, u64 t) {
@@ -108,6 +131,32 @@ GF2E_DEV void taylor_stage(u64 *sm, const u32 *off, u32 lg, u32 c_log, u32 tile_
         }
 #pragma unroll
         for (int j = 0; j < R; j++) sm[b0 ^ off[j]] = v[j];
+    }
+}
+
+// one tau level on the tile's rows (blocks of 2^log_rb rows, chunks of
+// 2^log_rc rows, all columns); each thread owns an offset q in the first
+// half of a block, so no two threads touch the same row pair
+GF2E_DEV void tau_stage(u64 *sm, bool fwd, u32 log_rb, u32 log_rc, u32 c_log, u32 rows_total) {
+    const u32 half = 1u << (log_rb - 1), rc = 1u << log_rc, nq = half - rc;
+    const u32 items = (rows_total >> 1) << c_log;
+    for (u32 t = threadIdx.x; t < items; t += FFT_THREADS) {
+        const u32 col = t & ((1u << c_log) - 1), r = t >> c_log;
+        const u32 blk = r >> (log_rb - 1), q = r & (half - 1);
+        if (q >= nq) continue;
+        const u32 b0 = blk << log_rb;
+        const u32 ia = sidx(b0 + rc + q, col, c_log), ih = sidx(b0 + half + q, col, c_log);
+        u64 h = sm[ih];
+        if (fwd) {
+            if (q < rc) {
+                h ^= sm[sidx(b0 + (1u << log_rb) - rc + q, col, c_log)];
+                sm[ih] = h;
+            }
+            sm[ia] ^= h;
+        } else {
+            sm[ia] ^= h;
+            if (q < rc) sm[ih] = h ^ sm[sidx(b0 + (1u << log_rb) - rc + q, col, c_log)];
+        }
     }
 }
 
@@ -291,6 +340,11 @@ k_fft_pass(u64 *__restrict__ f, const u64 *__restrict__ tab, const Pass P, u64 n
             const u32 type = op & 3, lg = (op >> 2) & 63, L = (op >> 8) & 127;
             const u32 K = ((op >> 15) & 3) + 1;
             const u32 *off = s_off + k * 16;
+            if (op & TAU_OP) {
+                tau_stage(sm, !(op & 1), lg, L, P.c_log, rows_total);
+                __syncthreads();
+                continue;
+            }
             switch (type * 4 + K) {
             case TAY_F * 4 + 1: taylor_stage<true, 1>(sm, off, lg, P.c_log, tile_elems); break;
             case TAY_F * 4 + 2: taylor_stage<true, 2>(sm, off, lg, P.c_log, tile_elems); break;
@@ -322,6 +376,70 @@ k_fft_pass(u64 *__restrict__ f, const u64 *__restrict__ tab, const Pass P, u64 n
         __syncthreads();                               // buffer free for the load after next
     }
     if (DB) asm volatile("cp.async.wait_all;\n" ::: "memory");
+}
+
+// one tau level streamed over HBM for levels whose blocks span more rows
+// than a tile holds (tau >= 2^10); V elements per item (16-byte accesses
+// when chunks are at least 2 elements).  blockIdx.y selects the transform.
+template <int V>
+__global__ void k_tau_stream(u64 *__restrict__ f, u64 fstride, u64 n, int M, int a, int fwd) {
+    f += (u64)blockIdx.y * fstride;
+    const u64 half = 1ull << (M - 1), c = 1ull << a, nq = half - c;
+    const u64 items = (n >> 1) / V;
+    for (u64 t = (u64)blockIdx.x * blockDim.x + threadIdx.x; t < items;
+         t += (u64)gridDim.x * blockDim.x) {
+        const u64 e = t * V, blk = e >> (M - 1), q = e & (half - 1);
+        if (q >= nq) continue;
+        const u64 b0 = blk << M;
+        u64 *A = f + b0 + c + q, *H = f + b0 + half + q;
+        const u64 *T = f + b0 + 2 * half - c + q;
+        if (V == 2) {
+            ulonglong2 h = *reinterpret_cast<const ulonglong2 *>(H);
+            ulonglong2 x = *reinterpret_cast<const ulonglong2 *>(A);
+            if (fwd) {
+                if (q < c) {
+                    const ulonglong2 tp = *reinterpret_cast<const ulonglong2 *>(T);
+                    h.x ^= tp.x;
+                    h.y ^= tp.y;
+                    *reinterpret_cast<ulonglong2 *>(H) = h;
+                }
+                x.x ^= h.x;
+                x.y ^= h.y;
+            } else {
+                x.x ^= h.x;
+                x.y ^= h.y;
+                if (q < c) {
+                    const ulonglong2 tp = *reinterpret_cast<const ulonglong2 *>(T);
+                    *reinterpret_cast<ulonglong2 *>(H) = make_ulonglong2(h.x ^ tp.x, h.y ^ tp.y);
+                }
+            }
+            *reinterpret_cast<ulonglong2 *>(A) = x;
+        } else {
+            u64 h = *H;
+            if (fwd) {
+                if (q < c) { h ^= *T; *H = h; }
+                *A ^= h;
+            } else {
+                *A ^= h;
+                if (q < c) *H = h ^ *T;
+            }
+        }
+    }
+}
+
+// 32-bit chunks of each operand into the low halves of its transform buffer
+// (zero beyond nchunks, xor0 into chunk 0), for transforms whose first pass
+// streams instead of loading tiles
+__global__ void k_pack_batch(const u32 *__restrict__ src32, u64 sstride32, u64 nchunks, u64 xor0,
+                             u64 *__restrict__ f, u64 fstride, u64 n) {
+    f += (u64)blockIdx.y * fstride;
+    src32 += (u64)blockIdx.y * sstride32;
+    for (u64 k = (u64)blockIdx.x * blockDim.x + threadIdx.x; k < n;
+         k += (u64)gridDim.x * blockDim.x) {
+        u64 v = k < nchunks ? (u64)__ldg(src32 + k) : 0ull;
+        if (k == 0) v ^= xor0;
+        f[k] = v;
+    }
 }
 
 __global__ void k_pack(const u32 *__restrict__ a32, u64 nchunks, u64 *__restrict__ F, u64 n) {
@@ -451,6 +569,11 @@ void merge_stages(Pass &p, const gf2e_tune &cfg) {
     u32 n = 0;
     for (u32 k = 0; k < p.nops;) {
         const u32 op = p.ops[k], type = op & 3, lg = (op >> 2) & 63, L = (op >> 8) & 127;
+        if (op & TAU_OP) {                               // tau levels stay single
+            out[n++] = op;
+            k++;
+            continue;
+        }
         const bool fwd = (type == TAY_F || type == BF_F);
         u32 run = 1;
         const u32 max_run = (u32)((type >= BF_F) ? cfg.fft_bfly_lv : cfg.fft_taylor_lv);
@@ -472,8 +595,30 @@ void merge_stages(Pass &p, const gf2e_tune &cfg) {
 }
 
 u64 pass_tiles(const Pass &p, u64 n) {
+    if (p.stream) return 0;
     u64 elems = ((u64)1 << (p.ns_log + p.c_log + p.wpt_log));
     return n / elems;
+}
+
+// tau levels (block log M, chunk log a) converting the coefficients whose
+// index bits lie in [lo, hi), in an order valid for the forward transform
+void tau_levels(int lo, int hi, std::vector<std::pair<int, int>> &out) {
+    const int m = hi - lo;
+    if (m <= 1) return;
+    int h = 1;
+    while (2 * h < m) h *= 2;
+    for (int M = m; M > h; M--) out.push_back({lo + M, lo + M - 1 - h});
+    tau_levels(lo + h, hi, out);          // the 2^(m-h)-coefficient conversions
+    tau_levels(lo, lo + h, out);          // the 2^h-coefficient conversions
+}
+
+// the Taylor stage by tau levels (fewer passes) from m = 15 on;
+// GF2E_FFT_TAYLOR=cascade keeps the x^2 + x cascade, =tau forces tau levels
+bool use_tau_levels(int m) {
+    const char *e = getenv("GF2E_FFT_TAYLOR");
+    if (e && !strcmp(e, "cascade")) return false;
+    if (e && !strcmp(e, "tau")) return m >= 2;
+    return m >= 15;
 }
 
 void build_passes(PlanImpl &P) {
@@ -496,8 +641,64 @@ void build_passes(PlanImpl &P) {
     if (m == 1) L0 = 0;
     if (!Cd) Cd = 1;
     std::vector<Pass> fwd, inv;
+    const bool tau = use_tau_levels(m);
+    if (tau) {
+        // tau levels grouped greedily into tile passes whose rows span the
+        // index bits every level of the group touches; a level wider than a
+        // tile streams over HBM on its own
+        std::vector<std::pair<int, int>> lv;
+        tau_levels(0, m, lv);
+        auto fits = [&](int lo, int hi) {
+            return hi - lo <= cfg.fft_tile_log &&
+                   choose((u64)1 << lo, (u64)1 << (hi - lo)) != 0;
+        };
+        auto flush = [&](int lo, int hi, const std::vector<std::pair<int, int>> &g) {
+            if (g.empty()) return;
+            const u64 CH = (u64)1 << lo, NS = (u64)1 << (hi - lo);
+            Pass pf = mk(CH, NS, choose(CH, NS));
+            Pass pi = pf;
+            for (const auto &o : g)
+                pf.ops[pf.nops++] = mktau(true, (u32)(o.first - lo), (u32)(o.second - lo));
+            for (size_t k = g.size(); k-- > 0;)
+                pi.ops[pi.nops++] = mktau(false, (u32)(g[k].first - lo), (u32)(g[k].second - lo));
+            fwd.push_back(pf);
+            inv.push_back(pi);
+        };
+        std::vector<std::pair<int, int>> grp;
+        int glo = 0, ghi = 0;
+        for (const auto &o : lv) {
+            const int M = o.first, a = o.second;
+            if (!fits(a, M)) {
+                flush(glo, ghi, grp);
+                grp.clear();
+                Pass ps;
+                memset(&ps, 0, sizeof ps);
+                ps.stream = 1;
+                ps.sM = (u32)M;
+                ps.sA = (u32)a;
+                fwd.push_back(ps);
+                inv.push_back(ps);
+                continue;
+            }
+            if (!grp.empty()) {
+                const int lo = std::min(glo, a), hi = std::max(ghi, M);
+                if ((int)grp.size() < MAXOPS && fits(lo, hi)) {
+                    glo = lo;
+                    ghi = hi;
+                    grp.push_back(o);
+                    continue;
+                }
+                flush(glo, ghi, grp);
+                grp.clear();
+            }
+            glo = a;
+            ghi = M;
+            grp.push_back(o);
+        }
+        flush(glo, ghi, grp);
+    }
     // Taylor depths 0..L0-1, grouped levels
-    for (int L = 0; L < L0 && L <= m - 2; L++) {
+    for (int L = 0; !tau && L < L0 && L <= m - 2; L++) {
         int b_hi = m - L;
         while (b_hi >= 2) {
             int best_lo = b_hi;
@@ -523,11 +724,11 @@ void build_passes(PlanImpl &P) {
         u64 CH = (u64)1 << L0, NS = n >> L0;
         Pass pf = mk(CH, NS, Cd);
         Pass pi = pf;
-        for (int Lp = 0; Lp <= mp - 2; Lp++)
+        for (int Lp = 0; !tau && Lp <= mp - 2; Lp++)
             for (int e = mp - 2; e >= Lp; e--) pf.ops[pf.nops++] = mkop(TAY_F, e, 0);
         for (int L = m - 1; L >= L0; L--) pf.ops[pf.nops++] = mkop(BF_F, L - L0, L);
         for (int L = L0; L <= m - 1; L++) pi.ops[pi.nops++] = mkop(BF_I, L - L0, L);
-        for (int Lp = mp - 2; Lp >= 0; Lp--)
+        for (int Lp = mp - 2; !tau && Lp >= 0; Lp--)
             for (int e = Lp; e <= mp - 2; e++) pi.ops[pi.nops++] = mkop(TAY_I, e, 0);
         fwd.push_back(pf);
         inv.push_back(pi);
@@ -577,7 +778,30 @@ int run_passes(const PlanImpl &P, bool forward, u64 *f, const u32 *src32, u64 nc
                cudaStream_t st, int batch = 1, Batch bt = Batch{0, 0, 0}) {
     const auto &ps = forward ? P.fwd : P.inv;
     const auto &nt = forward ? P.ntiles_fwd : P.ntiles_inv;
+    if (src32 && !ps.empty() && ps[0].stream) {
+        // the first pass streams: pack the operands first
+        dim3 grid((unsigned)gf2e::grid_for(P.n, 256, 8), (unsigned)batch);
+        k_pack_batch<<<grid, 256, 0, st>>>(src32, bt.sstride32, nchunks, bt.xor0, f, bt.fstride,
+                                          P.n);
+        GF2E_CHECK_LAUNCH("k_pack_batch");
+        src32 = nullptr;
+    }
+    // 16-byte accesses in streaming levels need 16-byte aligned transforms
+    const bool vec2 = ((uintptr_t)f % 16 == 0) && (batch == 1 || bt.fstride % 2 == 0);
     for (size_t i = 0; i < ps.size(); i++) {
+        if (ps[i].stream) {
+            const Pass &p = ps[i];
+            const int V = (vec2 && p.sA >= 1) ? 2 : 1;
+            dim3 grid((unsigned)gf2e::grid_for((P.n >> 1) / V, 256, 8), (unsigned)batch);
+            if (V == 2)
+                k_tau_stream<2><<<grid, 256, 0, st>>>(f, bt.fstride, P.n, (int)p.sM, (int)p.sA,
+                                                      forward ? 1 : 0);
+            else
+                k_tau_stream<1><<<grid, 256, 0, st>>>(f, bt.fstride, P.n, (int)p.sM, (int)p.sA,
+                                                      forward ? 1 : 0);
+            GF2E_CHECK_LAUNCH("k_tau_stream");
+            continue;
+        }
         // many tiles per CTA: two tile buffers, one resident CTA per SM looping
         // over its tiles; otherwise one buffer and up to eight CTAs per SM
         const u64 sms = (u64)gf2e::sm_count();

@@ -170,19 +170,49 @@ GF2E_DEV u64 mod_mersenne(u64 x, int d, u64 M) {
     while (x > M) x = (x & M) + (x >> d);
     return x == M ? 0 : x;
 }
-GF2E_DEV u64 gcd_u64(u64 a, u64 b) {
-    while (b) { u64 t = a % b; a = b; b = t; }
-    return a;
-}
-GF2E_DEV u64 inv_mod(u64 a, u64 m) {
-    long long t = 0, nt = 1, r = (long long)m, nr = (long long)(a % m);
-    while (nr) {
-        long long qq = r / nr, tmp;
-        tmp = t - qq * nt; t = nt; nt = tmp;
-        tmp = r - qq * nr; r = nr; nr = tmp;
+// gcd(a, m) for odd m >= 1 and 1 <= a, by the binary method (shifts and
+// subtractions only); when the gcd is 1, *inv = a^-1 mod m.  Invariants
+// a*x1 = u and a*x2 = v (mod m); halving mod an odd m is (x + m) / 2 for
+// odd x.  Each round removes at least one bit from u + v: at most 2*64.
+GF2E_DEV u64 gcd_inv_odd(u64 a, u64 m, u64 *inv) {
+    u64 u = a, v = m, x1 = 1 % m, x2 = 0;
+    const u64 mh = (m >> 1) + 1;                      // (m + 1) / 2
+    for (int it = 0; it < 4 * 64; it++) {
+        while (!(u & 1)) { u >>= 1; x1 = (x1 & 1) ? (x1 >> 1) + mh : x1 >> 1; }
+        while (!(v & 1)) { v >>= 1; x2 = (x2 & 1) ? (x2 >> 1) + mh : x2 >> 1; }
+        if (u == v) break;
+        if (u > v) { u -= v; x1 = x1 >= x2 ? x1 - x2 : x1 + (m - x2); }
+        else { v -= u; x2 = x2 >= x1 ? x2 - x1 : x2 + (m - x1); }
     }
-    if (t < 0) t += (long long)m;
-    return (u64)t;
+    *inv = x1;
+    return u;
+}
+
+// first s >= 1 of the progression j*s = v (mod M), M = 2^d - 1, and its
+// period n; false when no s exists.  gcd(j, M) = 1 for almost every j, and
+// then the inverse and the product are taken modulo the Mersenne number
+GF2E_DEV bool progression(u64 j, u64 v, int d, u64 M, u64 &first, u64 &n) {
+    u64 inv;
+    const u64 gg = gcd_inv_odd(j, M, &inv);
+    u64 s0;
+    if (gg == 1) {
+        n = M;
+        u64 p = 0;
+        {
+            unsigned __int128 t = (unsigned __int128)inv * v;
+            while (t > M) t = (t & M) + (t >> d);
+            p = t == M ? 0 : (u64)t;
+        }
+        s0 = p;
+    } else {
+        if (v % gg) return false;
+        n = M / gg;
+        u64 inv2;
+        gcd_inv_odd(j / gg, n, &inv2);                // coprime after dividing out gg
+        s0 = (u64)(((unsigned __int128)inv2 * (v / gg)) % n);
+    }
+    first = s0 ? s0 : n;
+    return true;
 }
 
 __global__ void k_tables(u32 *__restrict__ A, u32 *__restrict__ L, int d, u32 q, u64 M) {
@@ -272,12 +302,8 @@ k_classes(const u32 *__restrict__ A, const u32 *__restrict__ L, const DegreeArgs
         u64 u = mod_mersenne(j * a.rmod, d, M);
         if (u == 0) return;
         u64 v = L[A[u] ^ 1u];
-        u64 gg = gcd_u64(j, M);
-        if (v % gg) return;
-        u64 n = M / gg;
-        u64 s0 = (inv_mod(j / gg, n) * (v / gg)) % n;
-        u64 first = s0 ? s0 : n;
-        if (first > a.smax) return;
+        u64 first, n;
+        if (!progression(j, v, d, M, first, n) || first > a.smax) return;
         u64 count = (a.smax - first) / n + 1;
         // minimal polynomial of beta = x^j: first linear dependency among
         // beta^0..beta^d over GF(2)
@@ -433,9 +459,6 @@ GF2E_DEV u64 mulmod_mersenne(u64 a, u64 b, int d, u64 M) {
     while (p > M) p = (p & M) + (p >> d);
     return p == M ? 0 : (u64)p;
 }
-GF2E_DEV u64 mulmod_u64(u64 a, u64 b, u64 n) {
-    return (u64)(((unsigned __int128)a * b) % n);
-}
 
 // log-table slice: L[v - lo] = i for the values v = x^i in [lo, lo + len)
 template <typename E>
@@ -467,12 +490,8 @@ GF2E_DEV void wide_mark(u64 j, u64 v, const WideArgs &a, unsigned long long *__r
                         unsigned long long &my_marks) {
     const int d = a.F.d;
     const u64 M = a.F.M;
-    const u64 gg = gcd_u64(j, M);
-    if (v % gg) return;
-    const u64 n = M / gg;
-    const u64 s0 = mulmod_u64(inv_mod(j / gg, n), v / gg, n);
-    const u64 first = s0 ? s0 : n;
-    if (first > a.smax) return;
+    u64 first, n;
+    if (!progression(j, v, d, M, first, n) || first > a.smax) return;
     const u64 count = (a.smax - first) / n + 1;
     // minimal polynomial of beta = x^j: first linear dependency among
     // beta^0..beta^d over GF(2)
