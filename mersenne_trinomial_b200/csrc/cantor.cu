@@ -56,17 +56,12 @@ struct Pass {
 // basis (what the reference's cascade of x^2 + x levels computes) splits
 // into m - h levels at tau = 2^h (h the largest power of two below m) and
 // two independent conversions of 2^h and 2^(m-h) coefficients (Gao and
-// Mateer's recursion): 52 levels at m = 24 instead of 276.
+// Mateer's recursion): at m = 24, 16 streamed tau levels and three 8-bit
+// cascades (84 levels in 3 tile passes) instead of 276 cascade levels.
 //   forward: Hi[0..c) ^= Top; A[c..B) ^= Hi[0..B-c)   (B = 2^(M-1), A = the
 //            first half, Hi the second, Top its last c elements)
 //   inverse: A[c..B) ^= Hi[0..B-c); Hi[0..c) ^= Top
-// tau = 2 is the reference's x^2 + x level.  In a tile, the op word holds
-// the flag TAU_OP, the direction in bit 0, log2 block rows at bits 2..7 and
-// log2 chunk rows at bits 8..14.
-constexpr u32 TAU_OP = 1u << 17;
-__host__ __device__ inline u32 mktau(bool fwd, u32 log_rb, u32 log_rc) {
-    return TAU_OP | (fwd ? 0u : 1u) | (log_rb << 2) | (log_rc << 8);
-}
+// tau = 2 is the cascade's level (TAY_F / TAY_I ops in tile passes).
 
 // W(t) from byte tables: tab[k*256 + b] = XOR of basis[8k+j+1], bits j of b
 GF2E_DEV u64 twiddle(const u64 *__restrict__ tab, u64 t) {
@@ -131,32 +126,6 @@ GF2E_DEV void taylor_stage(u64 *sm, const u32 *off, u32 lg, u32 c_log, u32 tile_
         }
 #pragma unroll
         for (int j = 0; j < R; j++) sm[b0 ^ off[j]] = v[j];
-    }
-}
-
-// one tau level on the tile's rows (blocks of 2^log_rb rows, chunks of
-// 2^log_rc rows, all columns); each thread owns an offset q in the first
-// half of a block, so no two threads touch the same row pair
-GF2E_DEV void tau_stage(u64 *sm, bool fwd, u32 log_rb, u32 log_rc, u32 c_log, u32 rows_total) {
-    const u32 half = 1u << (log_rb - 1), rc = 1u << log_rc, nq = half - rc;
-    const u32 items = (rows_total >> 1) << c_log;
-    for (u32 t = threadIdx.x; t < items; t += FFT_THREADS) {
-        const u32 col = t & ((1u << c_log) - 1), r = t >> c_log;
-        const u32 blk = r >> (log_rb - 1), q = r & (half - 1);
-        if (q >= nq) continue;
-        const u32 b0 = blk << log_rb;
-        const u32 ia = sidx(b0 + rc + q, col, c_log), ih = sidx(b0 + half + q, col, c_log);
-        u64 h = sm[ih];
-        if (fwd) {
-            if (q < rc) {
-                h ^= sm[sidx(b0 + (1u << log_rb) - rc + q, col, c_log)];
-                sm[ih] = h;
-            }
-            sm[ia] ^= h;
-        } else {
-            sm[ia] ^= h;
-            if (q < rc) sm[ih] = h ^ sm[sidx(b0 + (1u << log_rb) - rc + q, col, c_log)];
-        }
     }
 }
 
@@ -340,11 +309,6 @@ k_fft_pass(u64 *__restrict__ f, const u64 *__restrict__ tab, const Pass P, u64 n
             const u32 type = op & 3, lg = (op >> 2) & 63, L = (op >> 8) & 127;
             const u32 K = ((op >> 15) & 3) + 1;
             const u32 *off = s_off + k * 16;
-            if (op & TAU_OP) {
-                tau_stage(sm, !(op & 1), lg, L, P.c_log, rows_total);
-                __syncthreads();
-                continue;
-            }
             switch (type * 4 + K) {
             case TAY_F * 4 + 1: taylor_stage<true, 1>(sm, off, lg, P.c_log, tile_elems); break;
             case TAY_F * 4 + 2: taylor_stage<true, 2>(sm, off, lg, P.c_log, tile_elems); break;
@@ -569,11 +533,6 @@ void merge_stages(Pass &p, const gf2e_tune &cfg) {
     u32 n = 0;
     for (u32 k = 0; k < p.nops;) {
         const u32 op = p.ops[k], type = op & 3, lg = (op >> 2) & 63, L = (op >> 8) & 127;
-        if (op & TAU_OP) {                               // tau levels stay single
-            out[n++] = op;
-            k++;
-            continue;
-        }
         const bool fwd = (type == TAY_F || type == BF_F);
         u32 run = 1;
         const u32 max_run = (u32)((type >= BF_F) ? cfg.fft_bfly_lv : cfg.fft_taylor_lv);
@@ -601,15 +560,24 @@ u64 pass_tiles(const Pass &p, u64 n) {
 }
 
 // tau levels (block log M, chunk log a) converting the coefficients whose
-// index bits lie in [lo, hi), in an order valid for the forward transform
-void tau_levels(int lo, int hi, std::vector<std::pair<int, int>> &out) {
+// index bits lie in [lo, hi), in an order valid for the forward transform.
+// Conversions of at most `cascade_bits` bits use the reference's x^2 + x
+// cascade (a = M - 2), whose levels a tile pass applies three at a time in
+// registers; wider ones split by Gao and Mateer's recursion into tau levels
+// (each streamed over HBM) and two narrower conversions.
+void tau_levels(int lo, int hi, int cascade_bits, std::vector<std::pair<int, int>> &out) {
     const int m = hi - lo;
     if (m <= 1) return;
+    if (m <= cascade_bits) {
+        for (int L = 0; L <= m - 2; L++)
+            for (int b = m - L; b >= 2; b--) out.push_back({lo + b + L, lo + b + L - 2});
+        return;
+    }
     int h = 1;
     while (2 * h < m) h *= 2;
     for (int M = m; M > h; M--) out.push_back({lo + M, lo + M - 1 - h});
-    tau_levels(lo + h, hi, out);          // the 2^(m-h)-coefficient conversions
-    tau_levels(lo, lo + h, out);          // the 2^h-coefficient conversions
+    tau_levels(lo + h, hi, cascade_bits, out);    // the 2^(m-h)-coefficient conversions
+    tau_levels(lo, lo + h, cascade_bits, out);    // the 2^h-coefficient conversions
 }
 
 // the Taylor stage by tau levels (fewer passes) from m = 15 on;
@@ -643,11 +611,15 @@ void build_passes(PlanImpl &P) {
     std::vector<Pass> fwd, inv;
     const bool tau = use_tau_levels(m);
     if (tau) {
-        // tau levels grouped greedily into tile passes whose rows span the
-        // index bits every level of the group touches; a level wider than a
-        // tile streams over HBM on its own
+        // cascade levels (a = M - 2) grouped greedily into tile passes whose
+        // rows span the index bits every level of the group touches; the
+        // wider tau levels stream over HBM one at a time
+        int cascade_bits = 0;
+        for (int k = 2; k <= cfg.fft_tile_log; k++)
+            if (choose((u64)1 << std::max(0, m - k), (u64)1 << k)) cascade_bits = k;
+        cascade_bits = std::min(cascade_bits, 10);
         std::vector<std::pair<int, int>> lv;
-        tau_levels(0, m, lv);
+        tau_levels(0, m, std::max(cascade_bits, 2), lv);
         auto fits = [&](int lo, int hi) {
             return hi - lo <= cfg.fft_tile_log &&
                    choose((u64)1 << lo, (u64)1 << (hi - lo)) != 0;
@@ -657,10 +629,9 @@ void build_passes(PlanImpl &P) {
             const u64 CH = (u64)1 << lo, NS = (u64)1 << (hi - lo);
             Pass pf = mk(CH, NS, choose(CH, NS));
             Pass pi = pf;
-            for (const auto &o : g)
-                pf.ops[pf.nops++] = mktau(true, (u32)(o.first - lo), (u32)(o.second - lo));
+            for (const auto &o : g) pf.ops[pf.nops++] = mkop(TAY_F, (u32)(o.second - lo), 0);
             for (size_t k = g.size(); k-- > 0;)
-                pi.ops[pi.nops++] = mktau(false, (u32)(g[k].first - lo), (u32)(g[k].second - lo));
+                pi.ops[pi.nops++] = mkop(TAY_I, (u32)(g[k].second - lo), 0);
             fwd.push_back(pf);
             inv.push_back(pi);
         };
@@ -668,7 +639,7 @@ void build_passes(PlanImpl &P) {
         int glo = 0, ghi = 0;
         for (const auto &o : lv) {
             const int M = o.first, a = o.second;
-            if (!fits(a, M)) {
+            if (M - a != 2 || !fits(a, M)) {
                 flush(glo, ghi, grp);
                 grp.clear();
                 Pass ps;
