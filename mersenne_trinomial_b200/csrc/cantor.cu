@@ -18,6 +18,7 @@
 // from four 256-entry byte tables (W is GF(2)-linear in t), so no n/2-entry
 // table is streamed from HBM.
 #include "gf2e_internal.cuh"
+#include "wrapmul.cuh"
 
 #include <cstdlib>
 #include <cstring>
@@ -1061,12 +1062,30 @@ int gf2e_mul(const gf2e_fft_plan *plan, const uint64_t *a_dev, uint64_t abits,
                      (cudaStream_t)stream);
 }
 
+}  // extern "C"
+
+namespace {
+// words of batch workspace one job takes: two transforms of its size, or for
+// a wrapped product two of the smaller size and its top-part scratch
+size_t job_words(const gf2e_mul_job &j, gf2e::WrapMul *wm) {
+    gf2e::WrapMul w;
+    if (!getenv("GF2E_NO_WRAP") && gf2e::wrap_mul_plan(j.abits, j.bbits, w)) {
+        if (wm) *wm = w;
+        return 2 * (size_t)w.n + (size_t)w.per;
+    }
+    if (wm) wm->mb = 0;
+    return 2 * ((size_t)1 << gf2e::mul_fft_m(j.abits, j.bbits));
+}
+}  // namespace
+
+extern "C" {
+
 int gf2e_mul_batch_workspace_size(const gf2e_mul_job *jobs, int njobs, size_t *bytes) {
     if (!jobs || njobs < 0 || !bytes) return gf2e::invalid("bad batch arguments");
     size_t tot = 0;
     for (int i = 0; i < njobs; i++) {
         if (jobs[i].abits == 0 || jobs[i].bbits == 0) return gf2e::invalid("empty operand in job %d", i);
-        tot += 2 * ((size_t)1 << gf2e::mul_fft_m(jobs[i].abits, jobs[i].bbits)) * sizeof(u64);
+        tot += job_words(jobs[i], nullptr) * sizeof(u64);
     }
     *bytes = tot;
     return GF2E_OK;
@@ -1101,14 +1120,23 @@ int gf2e_mul_batch(const gf2e_mul_job *jobs, int njobs, void *workspace, size_t 
         return jobs[x].abits + jobs[x].bbits > jobs[y].abits + jobs[y].bbits;
     });
     std::vector<size_t> offs(njobs);
+    std::vector<gf2e::WrapMul> wms(njobs);
     size_t off = 0;
     for (int i = 0; i < njobs; i++) {
         offs[i] = off;
-        off += 2 * ((size_t)1 << gf2e::mul_fft_m(jobs[i].abits, jobs[i].bbits));
+        off += job_words(jobs[i], &wms[i]);
     }
     u64 *ws = (u64 *)workspace;
     for (int k = 0; k < njobs; k++) {
         int i = order[k];
+        if (wms[i].mb) {                       // one size smaller, top part put back
+            if (!gf2e::wrap_mul_plans(wms[i])) return gf2e::invalid("wrapped product plans");
+            u64 *fa = ws + offs[i], *fb = fa + wms[i].n, *sc = fb + wms[i].n;
+            GF2E_TRY(gf2e::mul_wrapped(wms[i], jobs[i].a_dev, jobs[i].abits, jobs[i].b_dev,
+                                       jobs[i].bbits, jobs[i].out_dev, fa, fb, sc,
+                                       side[k % NSTREAMS]));
+            continue;
+        }
         int m = gf2e::mul_fft_m(jobs[i].abits, jobs[i].bbits);
         gf2e_fft_plan *p = gf2e::cached_plan(m);
         if (!p) return gf2e::invalid("plan creation failed for m=%d", m);

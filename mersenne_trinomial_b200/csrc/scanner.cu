@@ -28,6 +28,7 @@
 // Frobenius steps.
 #include "gf2e_internal.cuh"
 #include "polyhost.h"
+#include "wrapmul.cuh"
 
 #include <algorithm>
 #include <cmath>
@@ -88,6 +89,10 @@ struct gf2e_scanner {
     u64 *H = nullptr, *HS = nullptr, *C = nullptr, *sH = nullptr;
     std::vector<u64> shH;
     gf2e_sched sched{GF2E_SCHED_DOUBLING, 0, 0, 0.0, 0};   // for jobs submitted next
+    // r-bit products one transform size smaller, the wrapped part put back
+    bool wrap = false;
+    gf2e::WrapMul wm;
+    u64 *WS = nullptr;
 };
 
 // operands of at least this many bits take the half-gcd (hgcd.cu) at
@@ -181,6 +186,8 @@ struct Geometry {
     size_t nw, stride, tw, ow, pstride, gcap;
     u64 n, nchunks;
     int m;
+    bool wrap;
+    gf2e::WrapMul wm;
 };
 
 Geometry geometry(u64 r) {
@@ -189,6 +196,8 @@ Geometry geometry(u64 r) {
     g.stride = g.nw + (g.nw & 1);
     g.tw = (size_t)((r + 1 + 63) >> 6);
     g.m = gf2e::mul_fft_m(r, r);
+    g.wrap = !getenv("GF2E_NO_WRAP") && gf2e::wrap_mul_plan(r, r, g.wm);
+    if (g.wrap) g.m = g.wm.mb;
     g.n = (u64)1 << g.m;
     g.nchunks = (r + 31) >> 5;
     g.ow = (size_t)(((2 * r + 63) >> 6) + 1);
@@ -200,6 +209,7 @@ Geometry geometry(u64 r) {
 size_t device_words(const Geometry &g, int B, int m = 1) {
     size_t w = 3 * g.stride * B + 2 * g.n * B + g.pstride * B + g.tw * B + B + g.gcap * B;
     if (m > 1) w += 2 * (size_t)m * g.stride * B + g.stride * B + (size_t)m * B;
+    if (g.wrap) w += (size_t)g.wm.per * B;
     return w;
 }
 
@@ -370,6 +380,15 @@ int fill_slots(gf2e_scanner &S, cudaStream_t st) {
     return GF2E_OK;
 }
 
+// the product's last step: P = ACC * B from the inverse transform in FA
+// (overlap-add, and for wrapped products the top part put back)
+int product_tail(gf2e_scanner &S, int na, const u64 *B, cudaStream_t st) {
+    if (S.wrap)
+        return gf2e::wrap_mul_finish(S.wm, S.FA, S.n, S.ACC, S.stride, B, S.stride, S.P,
+                                     S.pstride, S.ow, na, S.WS, st);
+    return gf2e::overlap_add_batch(S.FA, S.n, 2 * S.nchunks - 1, S.P, S.pstride, S.ow, na, st);
+}
+
 // the launches of one degree for `na` resident s (F -> Fs squared; the
 // product then reads Fs, which becomes F)
 int degree_kernels(gf2e_scanner &S, int na, u64 *F, u64 *Fs, cudaStream_t st) {
@@ -380,7 +399,7 @@ int degree_kernels(gf2e_scanner &S, int na, u64 *F, u64 *Fs, cudaStream_t st) {
                                         2 * S.stride, S.nchunks, 2, na, st));
     GF2E_TRY(gf2e::pointwise(S.FA, S.FB, S.n * na, st));
     GF2E_TRY(gf2e::fft_run_batch(S.plan, false, S.FA, S.n, na, st));
-    GF2E_TRY(gf2e::overlap_add_batch(S.FA, S.n, 2 * S.nchunks - 1, S.P, S.pstride, S.ow, na, st));
+    GF2E_TRY(product_tail(S, na, Fs, st));
     GF2E_TRY(gf2e::trin_reduce_batch(S.P, S.pstride, S.ow, 2 * S.r - 1, S.ACC, S.stride, S.r,
                                      S.sdev, na, st));
     return GF2E_OK;
@@ -401,7 +420,7 @@ int block_kernels(gf2e_scanner &S, int na, cudaStream_t st) {
                                         2 * S.stride, S.nchunks, 0, na, st));
     GF2E_TRY(gf2e::pointwise(S.FA, S.FB, S.n * na, st));
     GF2E_TRY(gf2e::fft_run_batch(S.plan, false, S.FA, S.n, na, st));
-    GF2E_TRY(gf2e::overlap_add_batch(S.FA, S.n, 2 * S.nchunks - 1, S.P, S.pstride, S.ow, na, st));
+    GF2E_TRY(product_tail(S, na, S.C, st));
     GF2E_TRY(gf2e::trin_reduce_batch(S.P, S.pstride, S.ow, 2 * S.r - 1, S.ACC, S.stride, S.r,
                                      S.sdev, na, st));
     for (int t = 0; t < m; t++)
@@ -568,6 +587,12 @@ int gf2e_scanner_create_blocked(uint64_t r, int slots, int block, gf2e_scanner *
     S->gcap = g.gcap; S->n = g.n; S->nchunks = g.nchunks;
     S->plan = gf2e::cached_plan(g.m);
     if (!S->plan) { delete S; return gf2e::invalid("FFT plan m=%d", g.m); }
+    S->wrap = g.wrap;
+    S->wm = g.wm;
+    if (S->wrap && !gf2e::wrap_mul_plans(S->wm)) {
+        delete S;
+        return gf2e::invalid("FFT plans for the wrapped product");
+    }
     S->dmem_bytes = device_words(g, slots, block) * 8;
     cudaError_t e = cudaMalloc(&S->dmem, S->dmem_bytes);
     if (e != cudaSuccess) { delete S; return gf2e::cuda_status(e, "scanner buffers"); }
@@ -588,6 +613,7 @@ int gf2e_scanner_create_blocked(uint64_t r, int slots, int block, gf2e_scanner *
         S->sH = S->C + g.stride * B;
         S->shH.assign((size_t)block * B, 0);
     }
+    if (S->wrap) S->WS = S->dmem + (device_words(g, slots, block) - (size_t)g.wm.per * B);
     std::vector<gf2e_gcd_job> tmp(B, gf2e_gcd_job{S->ACC, r, S->T, r + 1, S->G, g.gcap});
     int st = GF2E_OK;
     if (r < GCD_LARGE_BITS) st = gf2e_gcd_workspace_size(tmp.data(), B, &S->gws_bytes);

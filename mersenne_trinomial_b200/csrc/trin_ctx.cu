@@ -3,6 +3,9 @@
 // the running product ACC (dACC), a 2r-bit product buffer (dT0) and an FFT
 // plan sized for r-bit x r-bit products.
 #include "gf2e_internal.cuh"
+#include "wrapmul.cuh"
+
+#include <cstdlib>
 
 namespace gf2e {
 int trin_reduce(const u64 *P, size_t pw, u64 L, u64 *out, u64 r, u64 s, cudaStream_t st);
@@ -27,7 +30,18 @@ struct gf2e_trin {
     gf2e_fft_plan *plan = nullptr;
     u64 *dA = nullptr, *dACC = nullptr, *dT0 = nullptr, *dT1 = nullptr;
     u64 *dFA = nullptr, *dFB = nullptr;
+    bool wrap = false;                    // r-bit products one size smaller (wrapmul.cu)
+    gf2e::WrapMul wm;
+    u64 *dWS = nullptr;
 };
+
+namespace {
+int ctx_mul(gf2e_trin *c, const u64 *x, const u64 *y, cudaStream_t st) {
+    if (c->wrap)
+        return gf2e::mul_wrapped(c->wm, x, c->r, y, c->r, c->dT0, c->dFA, c->dFB, c->dWS, st);
+    return gf2e::mul(c->plan, x, c->r, y, c->r, c->dT0, c->dFA, c->dFB, st);
+}
+}  // namespace
 
 extern "C" {
 
@@ -38,6 +52,9 @@ int gf2e_trin_create(uint64_t r, gf2e_trin **out) {
     c->r = r;
     c->nw = (size_t)((r + 63) >> 6);
     c->m = gf2e::mul_fft_m(r, r);
+    c->wrap = !getenv("GF2E_NO_WRAP") && gf2e::wrap_mul_plan(r, r, c->wm) &&
+              gf2e::wrap_mul_plans(c->wm);
+    if (c->wrap) c->m = c->wm.mb;
     c->plan = gf2e::cached_plan(c->m);
     if (!c->plan) { delete c; return gf2e::invalid("FFT plan for m=%d failed", c->m); }
     size_t n = (size_t)1 << c->m;
@@ -47,6 +64,7 @@ int gf2e_trin_create(uint64_t r, gf2e_trin **out) {
     if (e == cudaSuccess) e = cudaMalloc(&c->dT1, c->nw * 8);
     if (e == cudaSuccess) e = cudaMalloc(&c->dFA, n * 8);
     if (e == cudaSuccess) e = cudaMalloc(&c->dFB, n * 8);
+    if (e == cudaSuccess && c->wrap) e = cudaMalloc(&c->dWS, c->wm.per * 8);
     if (e != cudaSuccess) {
         gf2e_trin_destroy(c);
         return gf2e::cuda_status(e, "trin context allocation");
@@ -58,7 +76,7 @@ int gf2e_trin_create(uint64_t r, gf2e_trin **out) {
 int gf2e_trin_destroy(gf2e_trin *c) {
     if (!c) return GF2E_OK;
     cudaFree(c->dA); cudaFree(c->dACC); cudaFree(c->dT0); cudaFree(c->dT1);
-    cudaFree(c->dFA); cudaFree(c->dFB);
+    cudaFree(c->dFA); cudaFree(c->dFB); cudaFree(c->dWS);
     delete c;
     return GF2E_OK;
 }
@@ -101,7 +119,7 @@ int gf2e_trin_square_A(gf2e_trin *c, void *stream) {
 
 int gf2e_trin_mul_dev(gf2e_trin *c, const uint64_t *x, const uint64_t *y, void *stream) {
     if (!c || !x || !y) return gf2e::invalid("null argument");
-    return gf2e::mul(c->plan, x, c->r, y, c->r, c->dT0, c->dFA, c->dFB, (cudaStream_t)stream);
+    return ctx_mul(c, x, y, (cudaStream_t)stream);
 }
 
 int gf2e_trin_reduce_T0(gf2e_trin *c, uint64_t *dst, uint64_t L, void *stream) {
@@ -116,7 +134,7 @@ int gf2e_trin_accumulate(gf2e_trin *c, void *stream) {
     cudaStream_t st = (cudaStream_t)stream;
     k_xor_word0<<<1, 32, 0, st>>>(c->dA, 2);                  // F + x
     GF2E_CHECK_LAUNCH("k_xor_word0");
-    GF2E_TRY(gf2e::mul(c->plan, c->dACC, c->r, c->dA, c->r, c->dT0, c->dFA, c->dFB, st));
+    GF2E_TRY(ctx_mul(c, c->dACC, c->dA, st));
     k_xor_word0<<<1, 32, 0, st>>>(c->dA, 2);                  // restore F
     GF2E_CHECK_LAUNCH("k_xor_word0");
     return gf2e::trin_reduce(c->dT0, (size_t)((2 * c->r - 1 + 63) >> 6), 2 * c->r - 1, c->dACC,
