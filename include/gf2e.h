@@ -442,7 +442,7 @@ typedef struct gf2e_tune {
     int fft_tile_log;    /* log2 elements per shared-memory tile, 11..13; 0 = by size */
     int fft_cmin;        /* least contiguous columns per tile row: 1, 2, 4, 8, 16; 0 = by size */
     int fft_taylor_lv;   /* Taylor levels fused per register stage, 1..3 */
-    int fft_bfly_lv;     /* butterfly levels fused per register stage, 1..2 */
+    int fft_bfly_lv;     /* butterfly levels fused per register stage, 1..3 */
     int sieve_strip_log; /* log2 best[] entries per strip CTA, 10..14 */
 } gf2e_tune;
 

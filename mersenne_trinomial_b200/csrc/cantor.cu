@@ -162,12 +162,14 @@ GF2E_DEV void bfly_stage(u64 *sm, const u32 *off, const u64 *__restrict__ tab, u
                 if (j & Dj) continue;
                 const u64 tw = tb ^ ((j >> (lev + 1)) ? __ldg(tab + (j >> (lev + 1))) : 0ull);
                 if (FWD) {
-                    u64 e = v[j] ^ gf64_mul(tw, v[j + Dj]);
+                    // W[0] = 0: the first block of every level multiplies by
+                    // zero (all of level m-1, half of m-2, ...), warp-uniformly
+                    u64 e = v[j] ^ (tw ? gf64_mul(tw, v[j + Dj]) : 0ull);
                     v[j + Dj] ^= e;
                     v[j] = e;
                 } else {
                     u64 hh = v[j] ^ v[j + Dj];
-                    v[j] ^= gf64_mul(tw, hh);
+                    if (tw) v[j] ^= gf64_mul(tw, hh);
                     v[j + Dj] = hh;
                 }
             }
@@ -319,9 +321,11 @@ k_fft_pass(u64 *__restrict__ f, const u64 *__restrict__ tab, const Pass P, u64 n
             case TAY_I * 4 + 3: taylor_stage<false, 3>(sm, off, lg, P.c_log, tile_elems); break;
             case BF_F * 4 + 1: bfly_stage<true, 1>(sm, off, tab, lg, L, P.c_log, tile_elems, base); break;
             case BF_F * 4 + 2: bfly_stage<true, 2>(sm, off, tab, lg, L, P.c_log, tile_elems, base); break;
+            case BF_F * 4 + 3: bfly_stage<true, 3>(sm, off, tab, lg, L, P.c_log, tile_elems, base); break;
             case BF_I * 4 + 1: bfly_stage<false, 1>(sm, off, tab, lg, L, P.c_log, tile_elems, base); break;
             case BF_I * 4 + 2: bfly_stage<false, 2>(sm, off, tab, lg, L, P.c_log, tile_elems, base); break;
-            default: break;                    // butterfly stages hold at most 2 levels
+            case BF_I * 4 + 3: bfly_stage<false, 3>(sm, off, tab, lg, L, P.c_log, tile_elems, base); break;
+            default: break;                    // butterfly stages hold at most 3 levels
             }
             __syncthreads();
         }

@@ -38,7 +38,7 @@ gf2e_tune builtin_default() {
     t.fft_tile_log = 0;              // 0: by transform size (the autotuned B200 choices)
     t.fft_cmin = 0;
     t.fft_taylor_lv = 3;
-    t.fft_bfly_lv = 2;
+    t.fft_bfly_lv = 3;
     t.sieve_strip_log = 12;
     return t;
 }
@@ -51,7 +51,7 @@ const char *tune_problem(const gf2e_tune &t) {
     if (t.fft_cmin != 0 && (!pow2(t.fft_cmin) || t.fft_cmin > 16))
         return "fft_cmin not 0 (by size) or one of 1, 2, 4, 8, 16";
     if (t.fft_taylor_lv < 1 || t.fft_taylor_lv > 3) return "fft_taylor_lv outside 1..3";
-    if (t.fft_bfly_lv < 1 || t.fft_bfly_lv > 2) return "fft_bfly_lv outside 1..2";
+    if (t.fft_bfly_lv < 1 || t.fft_bfly_lv > 3) return "fft_bfly_lv outside 1..3";
     if (t.sieve_strip_log < 10 || t.sieve_strip_log > 14) return "sieve_strip_log outside 10..14";
     return nullptr;
 }
@@ -228,7 +228,7 @@ int gf2e_fft_autotune(int m, int reps, gf2e_tune *best, double *best_ms, char *r
     for (int tl = 11; tl <= 13; tl++)
         for (int cmin : {2, 4, 8, 16})
             for (int tlv = 1; tlv <= 3; tlv++)
-                for (int blv = 1; blv <= 2; blv++) {
+                for (int blv = 1; blv <= 3; blv++) {
                     gf2e_tune c = base;
                     c.fft_tile_log = tl;
                     c.fft_cmin = cmin;

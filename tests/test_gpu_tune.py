@@ -26,7 +26,7 @@ def restore_tune(engine):
 def test_fft_autotune_verifies_every_candidate(restore_tune):
     A = restore_tune
     res = A.fft_autotune(14, reps=1)
-    assert len(res["candidates"]) == 3 * 4 * 3 * 2
+    assert len(res["candidates"]) == 3 * 4 * 3 * 3
     assert all(c["status"] == "ok" for c in res["candidates"])
     assert A.tune_get() == res["best"]
     assert res["best_fwd_inv_ms"] == pytest.approx(min(c["ms"] for c in res["candidates"]),

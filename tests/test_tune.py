@@ -22,14 +22,15 @@ def model_cost(k0, maxd, t_deg, t_gcd, L0, Lmax):
 def test_tune_defaults_and_validation(engine):
     from mersenne_trinomial_b200 import autotune as A
     d = A.tune_default()
-    assert d == {"fft_tile_log": 0, "fft_cmin": 0, "fft_taylor_lv": 3, "fft_bfly_lv": 2,
+    assert d == {"fft_tile_log": 0, "fft_cmin": 0, "fft_taylor_lv": 3, "fft_bfly_lv": 3,
                  "sieve_strip_log": 12}
     saved = A.tune_get()
     try:
         for bad in ({"fft_tile_log": 10}, {"fft_tile_log": 14}, {"fft_tile_log": -1},
                     {"fft_cmin": 3}, {"fft_cmin": -2},
                     {"fft_cmin": 32}, {"fft_taylor_lv": 0}, {"fft_taylor_lv": 4},
-                    {"fft_bfly_lv": 3}, {"sieve_strip_log": 9}, {"sieve_strip_log": 15}):
+                    {"fft_bfly_lv": 4}, {"fft_bfly_lv": 0}, {"sieve_strip_log": 9},
+                    {"sieve_strip_log": 15}):
             with pytest.raises(engine.Gf2eError):
                 A.tune_set(**bad)
             assert A.tune_get() == saved          # a rejected set changes nothing
