@@ -4,8 +4,11 @@ The squaring, the deep scan and the serving work are independent per s (the
 reference scans one s at a time, trinomial_scan.cu:648-689), so ranks take
 disjoint s values and exchange nothing on the data path; the only
 collectives are the barrier and small host-level reductions (max of the
-timed region, gather of result lines).  The functions here hold that host
-logic so it can be tested with `gloo` ranks on CPU.
+timed region, gather of result lines).  The sieve shards by degree and has
+one real exchange: the elementwise minimum of every rank's best[] (the
+reference's multi-GPU merge, coarse_sieve.cu:466-507), one all-reduce of
+8 (smax + 1) bytes.  The functions here hold that host logic so it can be
+tested with `gloo` ranks on CPU.
 """
 from __future__ import annotations
 
@@ -59,3 +62,52 @@ def scan_sharded(r: int, survivors: Sequence[int], k0: int, maxd: int, rank: int
     if any(x is None for x in out):
         raise RuntimeError("missing results after gather")
     return out
+
+
+def sieve_degrees(dmin: int, dmax: int, rank: int, world: int) -> list:
+    """Degrees of [dmin, dmax] for `rank`: costs grow as 2^d, so degrees are
+    dealt largest first to the least-loaded rank (every degree on exactly
+    one rank)."""
+    if not (0 <= rank < world):
+        raise ValueError(f"rank {rank} outside 0..{world - 1}")
+    load = [0] * world
+    mine = {k: [] for k in range(world)}
+    for d in range(dmax, dmin - 1, -1):
+        k = min(range(world), key=lambda i: (load[i], i))
+        load[k] += 1 << d
+        mine[k].append(d)
+    return sorted(mine[rank])
+
+
+def _sieve_degrees_engine(r: int, degrees: Sequence[int], smax: int) -> np.ndarray:
+    from .engine import run_sieve
+    best = None
+    for d in sorted(degrees):
+        best = run_sieve(r, d, smax, dmin=d, preload=best)
+    if best is None:
+        best = np.full(smax + 1, np.uint64(0xFFFFFFFFFFFFFFFF), dtype=np.uint64)
+    return best
+
+
+def min_merge(best: np.ndarray, dist=None, device: Optional[str] = None) -> np.ndarray:
+    """Elementwise minimum of every rank's best[] (all-ones = no factor)."""
+    if dist is None or not dist.is_initialized() or dist.get_world_size() == 1:
+        return best
+    import torch
+    v = np.ascontiguousarray(best, dtype=np.uint64).view(np.int64).copy()
+    none = v == -1                               # UINT64_MAX as int64
+    v[none] = np.iinfo(np.int64).max             # keys are below 2^63
+    t = torch.from_numpy(v).to(device or "cpu")
+    dist.all_reduce(t, op=dist.ReduceOp.MIN)
+    out = t.cpu().numpy()
+    out[out == np.iinfo(np.int64).max] = -1
+    return out.view(np.uint64)
+
+
+def sieve_sharded(r: int, dmin: int, dmax: int, smax: int, rank: int, world: int, dist=None,
+                  sieve_fn: Optional[Callable] = None, device: Optional[str] = None) -> np.ndarray:
+    """best[0..smax] for degrees dmin..dmax with the degrees split over ranks
+    and the keys merged by minimum; every rank returns the full result."""
+    fn = sieve_fn or _sieve_degrees_engine
+    best = fn(r, sieve_degrees(dmin, dmax, rank, world), smax)
+    return min_merge(best, dist, device)
