@@ -8,13 +8,16 @@
 // Degrees 32..40 here ("wide") keep elements in 64 bits and store only the
 // log table, as slices of the value range [lo, hi) sized to the workspace
 // (one slice of 2^d entries when it fits: d = 32 takes 16 GB, d = 33 64 GB):
+//   k_wide_leaders  once per degree: per coset leader j, x^(j r) + 1 by
+//                   square-and-multiply-by-x (no antilog table), written
+//                   with j to a leader list
 //   k_wide_slice    walks the exponents with a multiply-by-x chain and
 //                   writes L[v - lo] = i for the values x^i in the slice
-//   k_wide_classes  per coset leader j: x^(j r) by square-and-multiply-by-x
-//                   (no antilog table), the Zech lookup when x^(j r) + 1 lies
-//                   in the slice, then the same progression and minimal
-//                   polynomial as the dense path
-// so a degree costs one exponent walk and one pass over j per slice.
+//   k_wide_match    the list entries whose lookup lies in the slice: the
+//                   same progression and minimal polynomial as the dense path
+// so a degree costs one pass over j and one exponent walk per slice.  When
+// the list does not fit the budget (d >= 38 by default) every slice redoes
+// the pass over j (k_wide_classes).
 //
 // Number theory (the reference's, sieve_ref.cpp:8-26): in GF(2^d) built on
 // the smallest primitive q_d (x generates the group of order M = 2^d - 1), an
@@ -170,22 +173,25 @@ GF2E_DEV u64 mod_mersenne(u64 x, int d, u64 M) {
     while (x > M) x = (x & M) + (x >> d);
     return x == M ? 0 : x;
 }
-// gcd(a, m) for odd m >= 1 and 1 <= a, by the binary method (shifts and
-// subtractions only); when the gcd is 1, *inv = a^-1 mod m.  Invariants
-// a*x1 = u and a*x2 = v (mod m); halving mod an odd m is (x + m) / 2 for
-// odd x.  Each round removes at least one bit from u + v: at most 2*64.
-GF2E_DEV u64 gcd_inv_odd(u64 a, u64 m, u64 *inv) {
-    u64 u = a, v = m, x1 = 1 % m, x2 = 0;
-    const u64 mh = (m >> 1) + 1;                      // (m + 1) / 2
-    for (int it = 0; it < 4 * 64; it++) {
-        while (!(u & 1)) { u >>= 1; x1 = (x1 & 1) ? (x1 >> 1) + mh : x1 >> 1; }
-        while (!(v & 1)) { v >>= 1; x2 = (x2 & 1) ? (x2 >> 1) + mh : x2 >> 1; }
-        if (u == v) break;
-        if (u > v) { u -= v; x1 = x1 >= x2 ? x1 - x2 : x1 + (m - x2); }
-        else { v -= u; x2 = x2 >= x1 ? x2 - x1 : x2 + (m - x1); }
+// gcd(a, m) for 1 <= a and m >= 2 by the extended Euclidean algorithm; when
+// the gcd is 1, *inv = a^-1 mod m.  One division per step, about
+// 0.84 ln(m) steps (fewer instructions and less divergence than the
+// shift-and-subtract form on these sizes)
+GF2E_DEV u64 gcd_inv(u64 a, u64 m, u64 *inv) {
+    long long t = 0, nt = 1;
+    u64 r = m, nr = a % m;
+    while (nr) {
+        const u64 q = r / nr;
+        const long long tmp = t - (long long)q * nt;
+        t = nt;
+        nt = tmp;
+        const u64 rr = r - q * nr;
+        r = nr;
+        nr = rr;
     }
-    *inv = x1;
-    return u;
+    if (t < 0) t += (long long)m;
+    *inv = (u64)t;
+    return r;
 }
 
 // first s >= 1 of the progression j*s = v (mod M), M = 2^d - 1, and its
@@ -193,7 +199,7 @@ GF2E_DEV u64 gcd_inv_odd(u64 a, u64 m, u64 *inv) {
 // then the inverse and the product are taken modulo the Mersenne number
 GF2E_DEV bool progression(u64 j, u64 v, int d, u64 M, u64 &first, u64 &n) {
     u64 inv;
-    const u64 gg = gcd_inv_odd(j, M, &inv);
+    const u64 gg = gcd_inv(j, M, &inv);
     u64 s0;
     if (gg == 1) {
         n = M;
@@ -208,7 +214,7 @@ GF2E_DEV bool progression(u64 j, u64 v, int d, u64 M, u64 &first, u64 &n) {
         if (v % gg) return false;
         n = M / gg;
         u64 inv2;
-        gcd_inv_odd(j / gg, n, &inv2);                // coprime after dividing out gg
+        gcd_inv(j / gg, n, &inv2);                // coprime after dividing out gg
         s0 = (u64)(((unsigned __int128)inv2 * (v / gg)) % n);
     }
     first = s0 ? s0 : n;
@@ -286,27 +292,69 @@ GF2E_DEV void for_each_leader(u64 M, int d, u64 *wq, Work &&work) {
     for_each_selected(1, M, wq, [&](u64 j) { return coset_least(j, d, M); }, work);
 }
 
+GF2E_DEV void add_stats(unsigned long long my_classes, unsigned long long my_marks, int d,
+                        Counters *cnt) {
+    for (int o = 16; o; o >>= 1) {
+        my_classes += __shfl_down_sync(0xffffffffu, my_classes, o);
+        my_marks += __shfl_down_sync(0xffffffffu, my_marks, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        if (my_classes) atomicAdd(&cnt->classes[d], my_classes);
+        if (my_marks) atomicAdd(&cnt->marks[d], my_marks);
+    }
+}
+
+// Second-level queue: the classes that mark some s <= smax (a few per cent
+// of the leaders once 2^d exceeds smax) wait per warp until 32 are queued,
+// so their minimal-polynomial work also runs on full warps.  Every lane of
+// the warp calls push together; want marks the lanes that enqueue.
+struct ClassQueue {
+    u64 j[64], first[64], n[64];
+};
+template <typename Work>
+GF2E_DEV void class_push(ClassQueue &q, int &qn, bool want, u64 j, u64 first, u64 n,
+                         Work &&work) {
+    const int lane = threadIdx.x & 31;
+    const unsigned b = __ballot_sync(0xffffffffu, want);
+    if (want) {
+        const int pos = qn + __popc(b & ((1u << lane) - 1u));
+        q.j[pos] = j;
+        q.first[pos] = first;
+        q.n[pos] = n;
+    }
+    qn += __popc(b);
+    __syncwarp();
+    if (qn >= 32) {
+        const int pos = qn - 32 + lane;
+        const u64 jj = q.j[pos], ff = q.first[pos], nn = q.n[pos];
+        __syncwarp();
+        qn -= 32;
+        work(jj, ff, nn, true);
+    }
+}
+template <typename Work>
+GF2E_DEV void class_flush(ClassQueue &q, int qn, Work &&work) {
+    const int lane = threadIdx.x & 31;
+    const bool v = lane < qn;
+    work(v ? q.j[lane] : 0, v ? q.first[lane] : 0, v ? q.n[lane] : 1, v);
+}
+
 __global__ void __launch_bounds__(256)
 k_classes(const u32 *__restrict__ A, const u32 *__restrict__ L, const DegreeArgs a,
           unsigned long long *__restrict__ best, Prog *__restrict__ strip, Prog *__restrict__ heavy,
           Counters *__restrict__ cnt) {
     __shared__ u64 wq_all[8][64];
+    __shared__ ClassQueue cq_all[8];
     const int d = a.d;
     const u64 M = a.M;
     unsigned long long my_classes = 0, my_marks = 0;
-    for_each_leader(M, d, wq_all[threadIdx.x >> 5], [&](u64 j, bool valid) {
+    ClassQueue &cq = cq_all[threadIdx.x >> 5];
+    int cqn = 0;
+    // minimal polynomial of beta = x^j (first linear dependency among
+    // beta^0..beta^d over GF(2)) and the marks of its progression
+    auto mark = [&](u64 j, u64 first, u64 n, bool valid) {
         if (!valid) return;
-        for (int k = 0; k < a.nsub; k++)
-            if (j % a.subq[k] == 0) return;
-        my_classes++;
-        u64 u = mod_mersenne(j * a.rmod, d, M);
-        if (u == 0) return;
-        u64 v = L[A[u] ^ 1u];
-        u64 first, n;
-        if (!progression(j, v, d, M, first, n) || first > a.smax) return;
-        u64 count = (a.smax - first) / n + 1;
-        // minimal polynomial of beta = x^j: first linear dependency among
-        // beta^0..beta^d over GF(2)
+        const u64 count = (a.smax - first) / n + 1;
         u32 prow[DMAX + 1], ptag[DMAX + 1];
         int pbit[DMAX + 1];
         int np = 0;
@@ -341,16 +389,22 @@ k_classes(const u32 *__restrict__ A, const u32 *__restrict__ L, const DegreeArgs
             if (slot < HCAP) heavy[slot] = Prog{first, n, key};
             else atomicAdd(&cnt->overflow, 1ull);
         }
+    };
+    for_each_leader(M, d, wq_all[threadIdx.x >> 5], [&](u64 j, bool valid) {
+        bool ok = valid;
+        for (int k = 0; k < a.nsub && ok; k++)
+            if (j % a.subq[k] == 0) ok = false;
+        u64 first = 0, n = 1;
+        if (ok) {
+            my_classes++;
+            const u64 u = mod_mersenne(j * a.rmod, d, M);
+            if (u == 0) ok = false;
+            else ok = progression(j, L[A[u] ^ 1u], d, M, first, n) && first <= a.smax;
+        }
+        class_push(cq, cqn, ok, j, first, n, mark);
     });
-    // warp-aggregated statistics
-    for (int o = 16; o; o >>= 1) {
-        my_classes += __shfl_down_sync(0xffffffffu, my_classes, o);
-        my_marks += __shfl_down_sync(0xffffffffu, my_marks, o);
-    }
-    if ((threadIdx.x & 31) == 0) {
-        if (my_classes) atomicAdd(&cnt->classes[d], my_classes);
-        if (my_marks) atomicAdd(&cnt->marks[d], my_marks);
-    }
+    class_flush(cq, cqn, mark);
+    add_stats(my_classes, my_marks, d, cnt);
 }
 
 // heavy progressions: block-strided over records, threads over marks
@@ -483,15 +537,12 @@ struct WideArgs {
     u64 subq[6];
 };
 
-// the class of leader j whose Zech logarithm is v: its progression of s,
-// and when it reaches s <= smax the minimal polynomial and the marks
-GF2E_DEV void wide_mark(u64 j, u64 v, const WideArgs &a, unsigned long long *__restrict__ best,
-                        Prog *__restrict__ heavy, Counters *__restrict__ cnt,
-                        unsigned long long &my_marks) {
+// a class of leader j whose progression (first, period n) reaches s <= smax:
+// its minimal polynomial and the marks
+GF2E_DEV void wide_mark(u64 j, u64 first, u64 n, const WideArgs &a,
+                        unsigned long long *__restrict__ best, Prog *__restrict__ heavy,
+                        Counters *__restrict__ cnt, unsigned long long &my_marks) {
     const int d = a.F.d;
-    const u64 M = a.F.M;
-    u64 first, n;
-    if (!progression(j, v, d, M, first, n) || first > a.smax) return;
     const u64 count = (a.smax - first) / n + 1;
     // minimal polynomial of beta = x^j: first linear dependency among
     // beta^0..beta^d over GF(2)
@@ -526,17 +577,6 @@ GF2E_DEV void wide_mark(u64 j, u64 v, const WideArgs &a, unsigned long long *__r
     }
 }
 
-GF2E_DEV void add_stats(unsigned long long my_classes, unsigned long long my_marks, int d,
-                        Counters *cnt) {
-    for (int o = 16; o; o >>= 1) {
-        my_classes += __shfl_down_sync(0xffffffffu, my_classes, o);
-        my_marks += __shfl_down_sync(0xffffffffu, my_marks, o);
-    }
-    if ((threadIdx.x & 31) == 0) {
-        if (my_classes) atomicAdd(&cnt->classes[d], my_classes);
-        if (my_marks) atomicAdd(&cnt->marks[d], my_marks);
-    }
-}
 
 // one slice without a leader list: every leader recomputes x^(j r) + 1 and
 // looks it up when it falls in this slice
@@ -545,20 +585,31 @@ __global__ void __launch_bounds__(256)
 k_wide_classes(const E *__restrict__ L, const WideArgs a, unsigned long long *__restrict__ best,
                Prog *__restrict__ heavy, Counters *__restrict__ cnt) {
     __shared__ u64 wq_all[8][64];
+    __shared__ ClassQueue cq_all[8];
     const int d = a.F.d;
     const u64 M = a.F.M;
     unsigned long long my_classes = 0, my_marks = 0;
+    ClassQueue &cq = cq_all[threadIdx.x >> 5];
+    int cqn = 0;
+    auto mark = [&](u64 j, u64 first, u64 n, bool valid) {
+        if (valid) wide_mark(j, first, n, a, best, heavy, cnt, my_marks);
+    };
     for_each_leader(M, d, wq_all[threadIdx.x >> 5], [&](u64 j, bool valid) {
-        if (!valid) return;
-        for (int k = 0; k < a.nsub; k++)
-            if (j % a.subq[k] == 0) return;
-        if (a.first_slice) my_classes++;
-        const u64 u = mulmod_mersenne(j, a.rmod, d, M);
-        if (u == 0) return;
-        const u64 w = wf_powx(u, a.F) ^ 1ull;            // x^(j r) + 1
-        if (w - a.lo >= a.len) return;                   // another slice's lookup
-        wide_mark(j, (u64)L[w - a.lo], a, best, heavy, cnt, my_marks);
+        bool ok = valid;
+        for (int k = 0; k < a.nsub && ok; k++)
+            if (j % a.subq[k] == 0) ok = false;
+        u64 w = 0, first = 0, n = 1;
+        if (ok) {
+            if (a.first_slice) my_classes++;
+            const u64 u = mulmod_mersenne(j, a.rmod, d, M);
+            if (u == 0) ok = false;
+            else w = wf_powx(u, a.F) ^ 1ull;             // x^(j r) + 1
+            ok = ok && w - a.lo < a.len;                  // else another slice's lookup
+        }
+        if (ok) ok = progression(j, (u64)L[w - a.lo], d, M, first, n) && first <= a.smax;
+        class_push(cq, cqn, ok, j, first, n, mark);
     });
+    class_flush(cq, cqn, mark);
     add_stats(my_classes, my_marks, d, cnt);
 }
 
@@ -603,15 +654,29 @@ k_wide_match(const E *__restrict__ L, const ulonglong2 *__restrict__ list, u64 c
              const WideArgs a, unsigned long long *__restrict__ best, Prog *__restrict__ heavy,
              Counters *__restrict__ cnt) {
     __shared__ u64 wq_all[8][64];
-    const u64 n = min((u64)cnt->nlist, cap);
+    __shared__ ClassQueue cq_all[8];
+    const u64 nl = min((u64)cnt->nlist, cap);
+    const int d = a.F.d;
+    const u64 M = a.F.M;
     unsigned long long my_marks = 0;
+    ClassQueue &cq = cq_all[threadIdx.x >> 5];
+    int cqn = 0;
+    auto mark = [&](u64 j, u64 first, u64 n, bool valid) {
+        if (valid) wide_mark(j, first, n, a, best, heavy, cnt, my_marks);
+    };
     for_each_selected(
-        0, n, wq_all[threadIdx.x >> 5], [&](u64 i) { return list[i].y - a.lo < a.len; },
+        0, nl, wq_all[threadIdx.x >> 5], [&](u64 i) { return list[i].y - a.lo < a.len; },
         [&](u64 i, bool valid) {
-            if (!valid) return;
-            const ulonglong2 e = list[i];
-            wide_mark(e.x, (u64)L[e.y - a.lo], a, best, heavy, cnt, my_marks);
+            u64 j = 0, first = 0, n = 1;
+            bool ok = valid;
+            if (ok) {
+                const ulonglong2 e = list[i];
+                j = e.x;
+                ok = progression(j, (u64)L[e.y - a.lo], d, M, first, n) && first <= a.smax;
+            }
+            class_push(cq, cqn, ok, j, first, n, mark);
         });
+    class_flush(cq, cqn, mark);
     add_stats(0, my_marks, a.F.d, cnt);
 }
 
