@@ -391,9 +391,40 @@ int gf2e_trin_frobenius_host(uint64_t r, const uint64_t *s_host, int nstates, ui
     cudaError_t e = cudaMemcpyAsync(sdev, s_host, (size_t)nstates * 8, cudaMemcpyHostToDevice, st);
     if (e != cudaSuccess) return gf2e::cuda_status(e, "frobenius s upload");
     GF2E_TRY(gf2e::trin_set_const(states, stride, nstates, r, 2, st));
-    GF2E_TRY(gf2e_trin_square_batch(states, scratch, stride, nstates, r, sdev, k, stream));
-    e = cudaMemcpy2DAsync(out_host, out_stride_words * 8, states, stride * 8, nw * 8,
-                          (size_t)nstates, cudaMemcpyDeviceToHost, st);
+    // Large batches go in groups of GROUP states, one after another on `st`,
+    // each group's readback on a copy stream while the next group squares,
+    // so only the last group's copy adds to the time.
+    constexpr int GROUP = 16;
+    const bool split = nstates >= 2 * GROUP && (size_t)nstates * nw * 8 >= ((size_t)256 << 20);
+    if (!split) {
+        GF2E_TRY(gf2e_trin_square_batch(states, scratch, stride, nstates, r, sdev, k, stream));
+        e = cudaMemcpy2DAsync(out_host, out_stride_words * 8, states, stride * 8, nw * 8,
+                              (size_t)nstates, cudaMemcpyDeviceToHost, st);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+        return gf2e::cuda_status(e, "frobenius readback");
+    }
+    static thread_local cudaStream_t copy_st = nullptr;
+    static thread_local cudaEvent_t ev_done = nullptr;
+    static thread_local int copy_dev = -1;
+    if (!copy_st || copy_dev != dev) {
+        e = cudaStreamCreateWithFlags(&copy_st, cudaStreamNonBlocking);
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ev_done, cudaEventDisableTiming);
+        if (e != cudaSuccess) return gf2e::cuda_status(e, "frobenius copy stream");
+        copy_dev = dev;
+    }
+    for (int g0 = 0; g0 < nstates; g0 += GROUP) {
+        const int ng = std::min(GROUP, nstates - g0);
+        GF2E_TRY(gf2e_trin_square_batch(states + stride * g0, scratch + stride * g0, stride, ng,
+                                        r, sdev + g0, k, stream));
+        e = cudaEventRecord(ev_done, st);
+        if (e == cudaSuccess) e = cudaStreamWaitEvent(copy_st, ev_done, 0);
+        if (e == cudaSuccess)
+            e = cudaMemcpy2DAsync(out_host + (size_t)g0 * out_stride_words, out_stride_words * 8,
+                                  states + stride * g0, stride * 8, nw * 8, (size_t)ng,
+                                  cudaMemcpyDeviceToHost, copy_st);
+        if (e != cudaSuccess) return gf2e::cuda_status(e, "frobenius group readback");
+    }
+    e = cudaStreamSynchronize(copy_st);
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);
     return gf2e::cuda_status(e, "frobenius readback");
 }

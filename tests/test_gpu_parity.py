@@ -315,3 +315,17 @@ def test_spread_square_equals_fft_square(engine):
     G.square_A()
     assert (G.read("A") == G.read("ACC")).all()
     G.fini()
+
+
+# ------------------------------------------------ host-buffer squaring API
+@pytest.mark.parametrize("r,n,k", [(999961, 8, 5), (136279841, 33, 3)])
+def test_frobenius_host_vs_oracle(engine, oracle, r, n, k):
+    """F_k = x^(2^k) for many s through host buffers; at r = 136279841 the
+    33 states (561 MB) are squared in groups whose readbacks overlap the
+    next group's squarings."""
+    rng = np.random.default_rng(r + n)
+    s_values = rng.integers(3, r // 2, size=n).astype(np.uint64)
+    got = engine.frobenius_host(r, s_values, k)
+    for i in sorted({0, n // 2, n - 1, min(16, n - 1)}):
+        want = oracle.trin_square_k(oracle.x_state(r), r, int(s_values[i]), k)
+        assert (got[i][: want.size] == want).all(), i
