@@ -376,7 +376,9 @@ int gf2e_trin_create(uint64_t r, gf2e_trin **ctx);        /* TrinGPU::init */
 int gf2e_trin_destroy(gf2e_trin *ctx);                    /* TrinGPU::fini */
 int gf2e_trin_set_s(gf2e_trin *ctx, uint64_t s);          /* TrinGPU::set_s */
 /* Device pointers of F (dA) and ACC (dACC), nw words each; product scratch
- * dT0 (2*nw words); FFT size exponent m. */
+ * dT0 (2*nw words); FFT size exponent m of the context's r-bit products
+ * (one less than the plain size when they take the wrapped form, as at
+ * r = 136279841). */
 int gf2e_trin_buffers(gf2e_trin *ctx, uint64_t **dA, uint64_t **dACC,
                       uint64_t **dT0, size_t *nw, int *m);
 int gf2e_trin_reset_A(gf2e_trin *ctx, void *stream);      /* k_set_x on dA */
