@@ -136,3 +136,19 @@ def test_late_hit_resolves_without_testing_cleared_degrees(engine, oracle):
     deep = [l for l in got if l.split()[1] != "u" and int(l.split()[1]) > 2 * k0 + 8]
     assert len(deep) >= 10
     assert check_against_reference(got, fx, oracle) == (104, 102, 2)
+
+
+@pytest.mark.timeout(1200)
+def test_deep_known_degree_r136279841(engine, oracle):
+    """A degree-only known answer from the reference's own runs: at
+    r = 136279841 the least factor of x^r + x^7458 + 1 has degree 30775
+    (so the deep-scan workload, d <= 20000, reports it as u).  Blocked scan
+    with long intervals (three interval gcds at this size), the factor
+    re-verified by the check-ntl restatement."""
+    r, s = 136279841, 7458
+    got = engine.scan(r, [s], 24, 31000, L0=8192, Lmax=16384, batch=1, block=26)
+    parts = got[0].split()
+    assert parts[:2] == [str(s), "30775"], got
+    mask = parts[2][1:]
+    assert int(mask, 16).bit_length() == 30776
+    assert oracle.factor_divides(r, s, 30775, mask) == 1
