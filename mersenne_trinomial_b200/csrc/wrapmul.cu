@@ -16,7 +16,8 @@
 // (which lies at bits >= T): floor(a b / x^T) = floor(a_hi b_hi / x^(D-1))
 // with a_hi, b_hi the top D = |a| + |b| - 1 - T bits of a and b, a product
 // 1/64 the size at r = 136279841.  Exactness needs delta < 2^(m-1) (Q Zlow
-// stays below 2^m); plans use it for delta <= 2^(m-3).
+// stays below 2^m); plans use it for delta <= 2^(m-2), where the two
+// products together still cost at most 3/4 of the plain 2^(m+1) one.
 #include "gf2e_internal.cuh"
 #include "wrapmul.cuh"
 
@@ -136,7 +137,7 @@ bool wrap_mul_plan(u64 abits, u64 bbits, WrapMul &w) {
     const u64 ca = (abits + 31) >> 5, cb = (bbits + 31) >> 5;
     if (ca > n || cb > n) return false;
     const u64 count = ca + cb - 1;
-    if (count <= n || count - n > (n >> 3)) return false;
+    if (count <= n || count - n > (n >> 2)) return false;
     const u64 T = 32 * n;
     if (abits + bbits - 1 < T + 64) return false;
     w.mb = mb;

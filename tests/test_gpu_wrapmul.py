@@ -18,10 +18,10 @@ def _dev(engine, words):
 
 
 # (abits, bbits): chunk counts 2^16 + a little (m = 16 instead of 17), an
-# uneven pair, one with the wrapped part at its largest allowed size, and
-# an ordinary size that does not wrap
+# uneven pair, wrapped parts of 1/10, 1/5 and 2/7 of 2^16 (the last beyond
+# the 1/4 limit, so a plain product), and an ordinary size
 SIZES = [(1 << 20 | 5000, 1 << 20 | 3000), ((1 << 21) - 64, 4000), (1 << 20 | 200000, 1 << 20),
-         (300_000, 200_000)]
+         ((1 << 20) + 400000, 1 << 20), ((1 << 20) + 600000, 1 << 20), (300_000, 200_000)]
 
 
 def test_batch_products_vs_oracle(engine, oracle):
