@@ -411,12 +411,6 @@ __global__ void k_pack_batch(const u32 *__restrict__ src32, u64 sstride32, u64 n
     }
 }
 
-__global__ void k_pack(const u32 *__restrict__ a32, u64 nchunks, u64 *__restrict__ F, u64 n) {
-    for (u64 k = (u64)blockIdx.x * blockDim.x + threadIdx.x; k < n;
-         k += (u64)gridDim.x * blockDim.x)
-        F[k] = (k < nchunks) ? (u64)a32[k] : 0ull;
-}
-
 __global__ void k_pointwise(u64 *__restrict__ fa, const u64 *__restrict__ fb, u64 n) {
     for (u64 k = (u64)blockIdx.x * blockDim.x + threadIdx.x; k < n;
          k += (u64)gridDim.x * blockDim.x)
@@ -939,12 +933,6 @@ int overlap_add_batch(const u64 *F, u64 fstride, u64 nchunks, u64 *out, u64 ostr
     int per = std::max(1, grid_for(ow, 256) / batch);
     k_overlap_add<<<dim3(per, batch), 256, 0, st>>>(F, nchunks, out, ow, fstride, ostride);
     GF2E_CHECK_LAUNCH("k_overlap_add batch");
-    return GF2E_OK;
-}
-
-int pack(const u64 *a, u64 nchunks, u64 *F, u64 n, cudaStream_t st) {
-    k_pack<<<grid_for(n, 256), 256, 0, st>>>(reinterpret_cast<const u32 *>(a), nchunks, F, n);
-    GF2E_CHECK_LAUNCH("k_pack");
     return GF2E_OK;
 }
 
