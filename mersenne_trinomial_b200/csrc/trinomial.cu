@@ -79,13 +79,16 @@ constexpr int WPT = 8;          // output words per thread on the fast path
 // interleave two 16-bit values (low halves of e, o): bit 2i <- e_i,
 // bit 2i+1 <- o_i.  One byte permute places [e.b0, o.b0, e.b1, o.b1], then
 // three delta swaps finish the outer perfect shuffle inside each 16 bits.
+// In each swap the masked bits t and t << k are disjoint, so t ^ (t << k)
+// is t * (2^k + 1): one integer multiply (FMA pipe) instead of a shift and
+// an XOR (ALU pipe, the busier one in this kernel).
 GF2E_DEV u32 shuffle16(u32 x) {
     u32 t = (x ^ (x >> 4)) & 0x00F000F0u;
-    x ^= t ^ (t << 4);
+    x ^= t * 17u;
     t = (x ^ (x >> 2)) & 0x0C0C0C0Cu;
-    x ^= t ^ (t << 2);
+    x ^= t * 5u;
     t = (x ^ (x >> 1)) & 0x22222222u;
-    x ^= t ^ (t << 1);
+    x ^= t * 3u;
     return x;
 }
 // spread(e) ^ (spread(o) << 1) as one 64-bit word
@@ -95,7 +98,8 @@ GF2E_DEV u64 interleave32(u32 e, u32 o) {
     return ((u64)hi << 32) | lo;
 }
 
-// batched squaring: blockIdx.y = state; each thread writes four words.
+// Batched squaring: blockIdx.y = state; each warp writes tiles of 32 WPT
+// words, lane l the words w0 + l + 32 q.
 //
 // Every window is a spread of 32 input bits placed on the even bit
 // positions (window offset even) or on the odd ones (offset odd), and the
@@ -105,21 +109,57 @@ GF2E_DEV u64 interleave32(u32 e, u32 o) {
 // two spreads per output word however many windows are active.  Parities:
 // spread(A_lo) and the last window are even, S<<1 is odd, the two middle
 // windows are odd/even or even/odd with the parity of s.
-// Groups of four words away from every window boundary take this path
-// (32-bit index arithmetic, hoisted offsets, no clipping); the few groups
-// that touch a boundary use the clipped per-word form above.
+// Warp tiles away from every window boundary take this path (32-bit index
+// arithmetic, hoisted offsets, no clipping); the few tiles that touch a
+// boundary use the clipped per-word form above.
+
 // One window for the WPT words of a lane in a warp tile (words
-// w0 + lane + 32q): two coalesced 32-bit loads and a funnel shift per word.
+// w0 + lane + 32q): word i0 + 32q and the next one, funnel-shifted.  The
+// lane's first index i0 is folded into one pointer so that every load of
+// the unrolled loop is that pointer plus a constant offset.
+//
+// Unguarded tiles load each 32-bit word once: the high word of lane l is
+// the low word of lane l + 1, and that of lane 31 is the low word of lane 0
+// for q + 1, so one extra load (lane 0, q = WPT) and a shuffle per word
+// replace the second load (5 % faster at r = 136279841: fewer load
+// instructions queue in the LSU).
 template <bool GUARD>
-GF2E_DEV void window_strided(const u32 *__restrict__ in32, u32 n32, u32 b, u32 sh,
-                             u32 (&acc)[WPT]) {
+GF2E_DEV void window_at(const u32 *__restrict__ in32, u32 i0, u32 n32, u32 sh,
+                        u32 (&acc)[WPT]) {
+    const u32 *__restrict__ p = in32 + i0;
+    if (!GUARD) {
+        const u32 lane = threadIdx.x & 31;
+        u32 lo[WPT + 1];
+#pragma unroll
+        for (int q = 0; q < WPT; q++) lo[q] = __ldg(p + 32 * q);
+        lo[WPT] = lane == 0 ? __ldg(p + 32 * WPT) : 0u;
+#pragma unroll
+        for (int q = 0; q < WPT; q++) {
+            const u32 y = lane == 0 ? lo[q + 1] : lo[q];
+            const u32 hi = __shfl_sync(0xffffffffu, y, (lane + 1) & 31);
+            acc[q] ^= __funnelshift_r(lo[q], hi, sh);
+        }
+        return;
+    }
 #pragma unroll
     for (int q = 0; q < WPT; q++) {
-        const u32 i = b + 32 * q;
-        u32 lo = (!GUARD || i < n32) ? __ldg(in32 + i) : 0u;
-        u32 hi = (!GUARD || i + 1 < n32) ? __ldg(in32 + i + 1) : 0u;
+        const u32 lo = (i0 + 32 * q < n32) ? __ldg(p + 32 * q) : 0u;
+        const u32 hi = (i0 + 32 * q + 1 < n32) ? __ldg(p + 32 * q + 1) : 0u;
         acc[q] ^= __funnelshift_r(lo, hi, sh);
     }
+}
+// The window starting at input bit 32 w + K.  The highest index the warp
+// reads is w0 + 32 WPT + (K >> 5) (the high word of lane 31 at q = WPT - 1,
+// loaded by lane 0 as its word for q = WPT); tiles whose highest index is
+// inside the state skip the bounds tests.  Every lane of the warp takes the
+// same branch (the test depends on w0 and K only), as the shuffle needs.
+GF2E_DEV void window_strided(const u32 *__restrict__ in32, u32 wl, u32 w0, u32 n32, u32 K,
+                             u32 (&acc)[WPT]) {
+    const u32 off = K >> 5;
+    if (w0 + 32 * WPT + off < n32)
+        window_at<false>(in32, wl + off, n32, K & 31, acc);
+    else
+        window_at<true>(in32, wl + off, n32, K & 31, acc);
 }
 
 // A clean warp tile of 32*WPT words: lane handles words w0 + lane + 32q, so
@@ -130,21 +170,23 @@ GF2E_DEV void square_tile_fast(const u32 *__restrict__ in32, u32 n32, u32 w0, u3
                                u32 K4, u32 K5, u64 *__restrict__ o) {
     u32 E[WPT], O[WPT];
     const u32 wl = w0 + lane;
+    const u32 *__restrict__ p1 = in32 + wl;
 #pragma unroll
     for (int q = 0; q < WPT; q++) {
-        E[q] = t1_on ? __ldg(in32 + wl + 32 * q) : 0u;
+        E[q] = t1_on ? __ldg(p1 + 32 * q) : 0u;
         O[q] = 0;
     }
-    window_strided<false>(in32, n32, wl + (K2 >> 5), K2 & 31, O);
-    if (t3_on) window_strided<false>(in32, n32, wl + (K3 >> 5), K3 & 31, SODD ? E : O);
-    if (t4_on) window_strided<true>(in32, n32, wl + (K4 >> 5), K4 & 31, SODD ? O : E);
-    if (t5_on) window_strided<true>(in32, n32, wl + (K5 >> 5), K5 & 31, E);
+    window_strided(in32, wl, w0, n32, K2, O);
+    if (t3_on) window_strided(in32, wl, w0, n32, K3, SODD ? E : O);
+    if (t4_on) window_strided(in32, wl, w0, n32, K4, SODD ? O : E);
+    if (t5_on) window_strided(in32, wl, w0, n32, K5, E);
+    u64 *__restrict__ op = o + wl;
 #pragma unroll
-    for (int q = 0; q < WPT; q++) o[wl + 32 * q] = interleave32(E[q], O[q]);
+    for (int q = 0; q < WPT; q++) op[32 * q] = interleave32(E[q], O[q]);
 }
 
-// Batched squaring: blockIdx.y = state, each thread WPT consecutive words.
-// All clean-group conditions use 32-bit arithmetic (bit positions < 2^32
+// Batched squaring: blockIdx.y = state, warps stride over the state's tiles.
+// All clean-tile conditions use 32-bit arithmetic (bit positions < 2^32
 // for r < 2^31); larger r take the clipped per-word path throughout.
 __global__ void __launch_bounds__(256, 4)
 k_square_batch(const u64 *__restrict__ in, u64 *__restrict__ out, size_t stride,
@@ -272,7 +314,10 @@ int launch_square(const u64 *in, u64 *out, size_t stride, int nstates, u64 r,
                   const u64 *s_dev, u64 s, cudaStream_t st) {
     const size_t nw = (size_t)((r + 63) >> 6);
     const int threads = 256;
-    size_t bx = (nw + (size_t)WPT * threads - 1) / ((size_t)WPT * threads);
+    // two warp tiles per warp: the per-state setup is spread over 16 words
+    // a thread (one tile per warp measured 8 % slower at r = 136279841)
+    const size_t per_block = (size_t)WPT * threads * 2;
+    size_t bx = (nw + per_block - 1) / per_block;
     if (bx > 65535) bx = 65535;
     dim3 grid((unsigned)bx, (unsigned)nstates);
     k_square_batch<<<grid, threads, 0, st>>>(in, out, stride, r, s_dev, s);
