@@ -314,9 +314,14 @@ int launch_square(const u64 *in, u64 *out, size_t stride, int nstates, u64 r,
                   const u64 *s_dev, u64 s, cudaStream_t st) {
     const size_t nw = (size_t)((r + 63) >> 6);
     const int threads = 256;
-    // two warp tiles per warp: the per-state setup is spread over 16 words
-    // a thread (one tile per warp measured 8 % slower at r = 136279841)
-    const size_t per_block = (size_t)WPT * threads * 2;
+    // Two warp tiles per warp spread the per-state setup over 16 words a
+    // thread (one tile per warp measured 8 % slower at r = 136279841), when
+    // the grid still fills every SM (4 blocks each) at least four times;
+    // small states (r ~ 10^6) keep one tile per warp and twice the blocks.
+    const size_t tile_words = (size_t)WPT * threads;
+    const size_t wide_blocks = (nw + 2 * tile_words - 1) / (2 * tile_words);
+    const bool two = wide_blocks * (size_t)nstates >= (size_t)16 * gf2e::sm_count();
+    const size_t per_block = two ? 2 * tile_words : tile_words;
     size_t bx = (nw + per_block - 1) / per_block;
     if (bx > 65535) bx = 65535;
     dim3 grid((unsigned)bx, (unsigned)nstates);
@@ -436,11 +441,15 @@ int gf2e_trin_frobenius_host(uint64_t r, const uint64_t *s_host, int nstates, ui
     cudaError_t e = cudaMemcpyAsync(sdev, s_host, (size_t)nstates * 8, cudaMemcpyHostToDevice, st);
     if (e != cudaSuccess) return gf2e::cuda_status(e, "frobenius s upload");
     GF2E_TRY(gf2e::trin_set_const(states, stride, nstates, r, 2, st));
-    // Large batches go in groups of GROUP states, one after another on `st`,
-    // each group's readback on a copy stream while the next group squares,
-    // so only the last group's copy adds to the time.
-    constexpr int GROUP = 16;
-    const bool split = nstates >= 2 * GROUP && (size_t)nstates * nw * 8 >= ((size_t)256 << 20);
+    // Large batches go in groups, one after another on `st`, each group's
+    // readback on a copy stream while the next group squares, so only the
+    // last group's copy adds to the time.  Group sizes shrink towards the
+    // end (..., 64, 16, 4 states; the first group takes the rest): a
+    // group's readback (17 MB a state at r = 136279841) takes well under
+    // the squaring time of a group a quarter its size for any k worth
+    // batching, the large first group keeps most launches wide, and the
+    // exposed last copy is 4 states.
+    const bool split = nstates >= 8 && (size_t)nstates * nw * 8 >= ((size_t)256 << 20);
     if (!split) {
         GF2E_TRY(gf2e_trin_square_batch(states, scratch, stride, nstates, r, sdev, k, stream));
         e = cudaMemcpy2DAsync(out_host, out_stride_words * 8, states, stride * 8, nw * 8,
@@ -448,6 +457,13 @@ int gf2e_trin_frobenius_host(uint64_t r, const uint64_t *s_host, int nstates, ui
         if (e == cudaSuccess) e = cudaStreamSynchronize(st);
         return gf2e::cuda_status(e, "frobenius readback");
     }
+    int groups[32], ngroups = 0, left = nstates;
+    for (int sz = 4; left > sz && ngroups < 31; sz *= 4) {
+        groups[ngroups++] = sz;
+        left -= sz;
+    }
+    groups[ngroups++] = left;
+    std::reverse(groups, groups + ngroups);
     static thread_local cudaStream_t copy_st = nullptr;
     static thread_local cudaEvent_t ev_done = nullptr;
     static thread_local int copy_dev = -1;
@@ -457,8 +473,8 @@ int gf2e_trin_frobenius_host(uint64_t r, const uint64_t *s_host, int nstates, ui
         if (e != cudaSuccess) return gf2e::cuda_status(e, "frobenius copy stream");
         copy_dev = dev;
     }
-    for (int g0 = 0; g0 < nstates; g0 += GROUP) {
-        const int ng = std::min(GROUP, nstates - g0);
+    for (int gi = 0, g0 = 0; gi < ngroups; g0 += groups[gi], gi++) {
+        const int ng = groups[gi];
         GF2E_TRY(gf2e_trin_square_batch(states + stride * g0, scratch + stride * g0, stride, ng,
                                         r, sdev + g0, k, stream));
         e = cudaEventRecord(ev_done, st);

@@ -321,8 +321,9 @@ def test_spread_square_equals_fft_square(engine):
 @pytest.mark.parametrize("r,n,k", [(999961, 8, 5), (136279841, 33, 3)])
 def test_frobenius_host_vs_oracle(engine, oracle, r, n, k):
     """F_k = x^(2^k) for many s through host buffers; at r = 136279841 the
-    33 states (561 MB) are squared in groups whose readbacks overlap the
-    next group's squarings."""
+    33 states (561 MB) are squared in groups of 13, 16 and 4 states whose
+    readbacks overlap the next group's squarings (states 0, 16 and 32 are
+    checked: one from each group)."""
     rng = np.random.default_rng(r + n)
     s_values = rng.integers(3, r // 2, size=n).astype(np.uint64)
     got = engine.frobenius_host(r, s_values, k)
