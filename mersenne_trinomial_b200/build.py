@@ -70,7 +70,7 @@ def build_tools(verbose: bool = False) -> list:
     os.makedirs(BIN, exist_ok=True)
     out = []
     srcs = sorted(glob.glob(os.path.join(TOOLS, "*.cpp")))
-    hdrs = glob.glob(os.path.join(ROOT, "include", "*"))
+    hdrs = glob.glob(os.path.join(ROOT, "include", "*")) + glob.glob(os.path.join(TOOLS, "*.h"))
     for src in srcs:
         exe = os.path.join(BIN, os.path.splitext(os.path.basename(src))[0])
         if _newer([src, LIB] + hdrs, exe):

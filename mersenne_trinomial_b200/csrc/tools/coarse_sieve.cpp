@@ -3,7 +3,8 @@
 //
 //   coarse_sieve <r> <depth> <out_prefix> [--smax S] [--found] [--cert|--no-cert]
 //                [--no-survivors] [--load f.found.bin] [--load-survivors f]
-//                [--min-depth D] [--gpus N]
+//                [--min-depth D] [--checkpoint f] [--checkpoint-mins N]
+//                [--checkpoint-keep G] [--resume f] [--gpus N]
 //   coarse_sieve <r> <depth> <smax> <out_prefix> ...      (legacy positional form)
 //   coarse_sieve --selftest
 //
@@ -14,18 +15,34 @@
 // Degrees up to 31 run on dense tables in HBM (the reference needs its
 // bucketed low-memory mode beyond d = 29 on an 8 GB GPU); degrees 32..40 on
 // the wide path (64-bit elements, the log table in slices of at most
-// GF2E_SIEVE_WIDE_GB, default 64 GB: one slice up to d = 33).  Checkpoint
-// flags (--checkpoint, --checkpoint-mins, --checkpoint-keep, --resume) are
-// accepted and ignored with a note.
+// GF2E_SIEVE_WIDE_GB, default 64 GB: one slice up to d = 33).
+//
+// Checkpoints (coarse_sieve.cu:509-831, 1383-1480) use the reference's file
+// layout (sieve_ckpt.h), so a stopped run resumes under either tool.  With
+// --checkpoint the degrees run one library call each; best[] is saved at
+// degree boundaries every --checkpoint-mins minutes and on SIGTERM/SIGINT,
+// which stop the run with exit status 0.  A stop is honoured when the
+// current degree ends; during degrees of 36 and up (seconds to minutes at
+// r = 136279841) a watcher thread saves the last boundary at once instead.
+// --resume continues from a checkpoint (into the same file unless
+// --checkpoint names another); COARSE_TEST_STOP_AFTER_BUCKETS=N stops after
+// N completed degrees, the reference's deterministic test hook with a
+// degree as this engine's unit of resumable work.
 #include <cinttypes>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <atomic>
 #include <chrono>
+#include <csignal>
+#include <mutex>
 #include <string>
+#include <thread>
+#include <unistd.h>
 #include <vector>
 
 #include "gf2e.h"
+#include "sieve_ckpt.h"
 
 typedef uint64_t u64;
 
@@ -41,6 +58,84 @@ static void die_on(int st, const char *what) {
     }
 }
 
+// Checkpointing state of this run.  The signal handler only sets `stop`;
+// files are written by the main thread between degrees, or by the watcher
+// thread while a long degree is on the device.
+struct CkptRun {
+    bool on = false;
+    std::string path;
+    int keep = 3;
+    double period_s = 0, last_write = 0;
+    u64 r = 0, smax = 0;
+    int depth = 0;
+    sieve_ckpt::Baseline base;
+    long stop_after = 0, degrees_done = 0;   // COARSE_TEST_STOP_AFTER_BUCKETS
+    volatile sig_atomic_t stop = 0;
+    std::mutex mu;                           // guards snap / snap_pt
+    std::vector<u64> snap;                   // best[] at snap_pt
+    sieve_ckpt::Point snap_pt;
+    bool snap_valid = false;
+    std::atomic<bool> long_degree{false};    // the watcher may write for us
+    std::atomic<bool> writer_claimed{false}; // one final write, by one thread
+    std::atomic<bool> done{false};
+};
+static CkptRun g_ck;
+
+extern "C" void ckpt_on_signal(int) { g_ck.stop = 1; }
+
+// degrees from here on take seconds to minutes at full smax (d = 36: 4.5 s,
+// d = 38: 151 s at r = 136279841), too long to wait for before saving
+constexpr int kLongDegree = 36;
+
+// write g_ck.snap (caller holds g_ck.mu)
+static void ckpt_write_snapshot() {
+    sieve_ckpt::WriteInfo info;
+    const double t0 = now_s();
+    if (!sieve_ckpt::write(g_ck.path, g_ck.keep, g_ck.r, g_ck.smax, g_ck.depth, g_ck.period_s,
+                           g_ck.snap_pt, g_ck.snap, g_ck.base, &info))
+        return;
+    g_ck.last_write = now_s();
+    if (info.delta)
+        fprintf(stderr, "[checkpoint: d=%d, delta %" PRIu64 " entries (%.2f MB) -> %s, %.2fs]\n",
+                g_ck.snap_pt.d, info.entries, info.bytes / 1048576.0, g_ck.path.c_str(),
+                now_s() - t0);
+    else
+        fprintf(stderr, "[checkpoint: d=%d, full image (%.0f MB) -> %s, %.2fs]\n", g_ck.snap_pt.d,
+                info.bytes / 1048576.0, g_ck.path.c_str(), now_s() - t0);
+}
+
+// host copy of best[] as the state "every degree below next_d is done"
+static void ckpt_take(const u64 *dbest, int next_d) {
+    std::lock_guard<std::mutex> lk(g_ck.mu);
+    g_ck.snap.resize(g_ck.smax + 1);
+    die_on(gf2e_copy_to_host(g_ck.snap.data(), dbest, (g_ck.smax + 1) * 8, nullptr), "snapshot");
+    g_ck.snap_pt = sieve_ckpt::Point();
+    g_ck.snap_pt.d = next_d;
+    g_ck.snap_valid = true;
+}
+
+static void ckpt_stop_message() {
+    fprintf(stderr, "stopping on request; resume with --resume %s\n", g_ck.path.c_str());
+}
+
+// Saves the last degree boundary when a stop arrives during a long degree,
+// then ends the process (the degree in flight is abandoned and runs again
+// on resume).
+static void ckpt_watcher() {
+    while (!g_ck.done.load()) {
+        if (g_ck.stop && g_ck.long_degree.load() && !g_ck.writer_claimed.exchange(true)) {
+            {
+                std::lock_guard<std::mutex> lk(g_ck.mu);
+                if (g_ck.snap_valid) ckpt_write_snapshot();
+            }
+            ckpt_stop_message();
+            fflush(stderr);
+            _exit(0);
+        }
+        std::this_thread::sleep_for(std::chrono::milliseconds(100));
+    }
+}
+
 // run the sieve on the device; best has smax+1 entries (index 0 unused)
 static void run_gpu(u64 r, int depth, u64 smax, int min_depth, std::vector<u64> &best,
                     const std::vector<u64> *preload) {
@@ -53,12 +148,51 @@ static void run_gpu(u64 r, int depth, u64 smax, int min_depth, std::vector<u64> 
         die_on(gf2e_copy_to_device(dbest, preload->data(), (smax + 1) * 8, nullptr), "upload");
     else
         die_on(gf2e_sieve_fill((u64 *)dbest, smax, nullptr), "fill");
-    double t0 = now_s();
-    die_on(gf2e_sieve_run(r, min_depth, depth, smax, (u64 *)dbest, ws, ws_bytes, nullptr),
-           "sieve");
-    double t1 = now_s();
-    u64 classes[41], marks[41];
-    die_on(gf2e_sieve_stats(ws, depth, classes, marks, nullptr), "stats");
+    u64 classes[41] = {0}, marks[41] = {0};
+    const double t0 = now_s();
+    if (min_depth > depth) {
+        // resumed after the last degree: nothing left but the outputs
+    } else if (!g_ck.on) {
+        die_on(gf2e_sieve_run(r, min_depth, depth, smax, (u64 *)dbest, ws, ws_bytes, nullptr),
+               "sieve");
+        die_on(gf2e_sieve_stats(ws, depth, classes, marks, nullptr), "stats");
+    } else {
+        std::thread watcher(ckpt_watcher);
+        for (int d = min_depth; d <= depth; d++) {
+            if (d >= kLongDegree) {
+                ckpt_take((const u64 *)dbest, d);       // what the watcher would save
+                g_ck.long_degree = true;
+            }
+            die_on(gf2e_sieve_run(r, d, d, smax, (u64 *)dbest, ws, ws_bytes, nullptr), "sieve");
+            g_ck.long_degree = false;
+            u64 c[41] = {0}, m[41] = {0};
+            die_on(gf2e_sieve_stats(ws, depth, c, m, nullptr), "stats");
+            classes[d] = c[d];
+            marks[d] = m[d];
+            g_ck.degrees_done++;
+            const bool test_stop = g_ck.stop_after > 0 && g_ck.degrees_done >= g_ck.stop_after;
+            if ((g_ck.stop || test_stop) && d < depth) {
+                if (g_ck.writer_claimed.exchange(true))   // the watcher is saving and exiting
+                    for (;;) pause();
+                ckpt_take((const u64 *)dbest, d + 1);
+                {
+                    std::lock_guard<std::mutex> lk(g_ck.mu);
+                    ckpt_write_snapshot();
+                }
+                ckpt_stop_message();
+                fflush(nullptr);
+                _exit(0);     // the watcher thread still runs: no static destructors
+            }
+            if (d < depth && g_ck.period_s > 0 && now_s() - g_ck.last_write >= g_ck.period_s) {
+                ckpt_take((const u64 *)dbest, d + 1);
+                std::lock_guard<std::mutex> lk(g_ck.mu);
+                ckpt_write_snapshot();
+            }
+        }
+        g_ck.done = true;
+        watcher.join();
+    }
+    const double t1 = now_s();
     for (int d = min_depth; d <= depth; d++)
         fprintf(stderr, "d=%2d done: %" PRIu64 " classes, %" PRIu64 " marks\n", d, classes[d],
                 marks[d]);
@@ -67,34 +201,6 @@ static void run_gpu(u64 r, int depth, u64 smax, int min_depth, std::vector<u64> 
     die_on(gf2e_copy_to_host(best.data(), dbest, (smax + 1) * 8, nullptr), "download");
     gf2e_device_free(ws);
     gf2e_device_free(dbest);
-}
-
-static bool read_found_image(const char *path, u64 smax, std::vector<u64> &out) {
-    FILE *f = fopen(path, "rb");
-    if (!f) { perror(path); return false; }
-    out.assign(smax + 1, ~0ULL);
-    size_t got = fread(out.data() + 1, 8, smax, f);
-    fclose(f);
-    if (got != smax) {
-        fprintf(stderr, "%s: expected %" PRIu64 " keys, got %zu\n", path, smax, got);
-        return false;
-    }
-    return true;
-}
-
-static bool read_survivors(const char *path, u64 smax, int min_depth, std::vector<u64> &out) {
-    FILE *f = fopen(path, "r");
-    if (!f) { perror(path); return false; }
-    // every s not listed already has a factor of degree < min_depth; a
-    // sentinel below (min_depth << 48) blocks all new marks exactly as the
-    // real key would (coarse_sieve.cu:1466-1480)
-    out.assign(smax + 1, 0);
-    u64 s;
-    while (fscanf(f, "%" SCNu64, &s) == 1)
-        if (s >= 1 && s <= smax) out[s] = ~0ULL;
-    fclose(f);
-    (void)min_depth;
-    return true;
 }
 
 static int selftest() {
@@ -150,7 +256,9 @@ int main(int argc, char **argv) {
         fprintf(stderr, "usage: %s <r> <depth> <out_prefix> [options]\n"
                         "       %s --selftest\n"
                         "options: --smax S --found --cert --no-cert --no-survivors\n"
-                        "         --load f.found.bin --load-survivors f --min-depth D --gpus N\n",
+                        "         --load f.found.bin --load-survivors f --min-depth D --gpus N\n"
+                        "         --checkpoint f --checkpoint-mins N --checkpoint-keep G "
+                        "--resume f\n",
                 argv[0], argv[0]);
         return 1;
     }
@@ -171,6 +279,9 @@ int main(int argc, char **argv) {
                         "(default floor(r/2) = %" PRIu64 ") is preferred\n", r / 2);
     bool write_found = false, write_surv = true, write_cert = true;
     const char *load_path = nullptr, *loadsurv = nullptr;
+    const char *ckpt_path = nullptr, *resume_path = nullptr;
+    double ckpt_mins = -1;                       // < 0: not given
+    int ckpt_keep = 3;
     int min_depth = 2;
     for (int a = legacy ? 5 : 4; a < argc; a++) {
         if (!strcmp(argv[a], "--found")) write_found = true;
@@ -181,11 +292,12 @@ int main(int argc, char **argv) {
         else if (!strcmp(argv[a], "--load") && a + 1 < argc) load_path = argv[++a];
         else if (!strcmp(argv[a], "--load-survivors") && a + 1 < argc) loadsurv = argv[++a];
         else if (!strcmp(argv[a], "--min-depth") && a + 1 < argc) min_depth = atoi(argv[++a]);
-        else if ((!strcmp(argv[a], "--checkpoint") || !strcmp(argv[a], "--checkpoint-mins") ||
-                  !strcmp(argv[a], "--checkpoint-keep") || !strcmp(argv[a], "--resume") ||
-                  !strcmp(argv[a], "--gpus")) && a + 1 < argc) {
-            fprintf(stderr, "note: %s %s ignored (one GPU, no checkpoints)\n", argv[a],
-                    argv[a + 1]);
+        else if (!strcmp(argv[a], "--checkpoint") && a + 1 < argc) ckpt_path = argv[++a];
+        else if (!strcmp(argv[a], "--checkpoint-mins") && a + 1 < argc) ckpt_mins = atof(argv[++a]);
+        else if (!strcmp(argv[a], "--checkpoint-keep") && a + 1 < argc) ckpt_keep = atoi(argv[++a]);
+        else if (!strcmp(argv[a], "--resume") && a + 1 < argc) resume_path = argv[++a];
+        else if (!strcmp(argv[a], "--gpus") && a + 1 < argc) {
+            fprintf(stderr, "note: --gpus %s ignored (this tool drives one GPU)\n", argv[a + 1]);
             a++;
         } else fprintf(stderr, "warning: ignoring unknown argument '%s'\n", argv[a]);
     }
@@ -194,17 +306,72 @@ int main(int argc, char **argv) {
         fprintf(stderr, "depth %d > 40 is not supported by this engine\n", depth);
         return 1;
     }
+    if (ckpt_keep < 1) ckpt_keep = 1;
+    if (const char *e = getenv("COARSE_TEST_STOP_AFTER_BUCKETS")) g_ck.stop_after = atol(e);
     std::vector<u64> preload;
     const std::vector<u64> *pre = nullptr;
-    if (load_path) {
-        if (!read_found_image(load_path, smax, preload)) return 1;
+    double stored_period_s = 0;
+    if (resume_path) {
+        sieve_ckpt::Point pt;
+        std::string used;
+        if (!sieve_ckpt::read(resume_path, r, smax, preload, pt, stored_period_s, g_ck.base, &used))
+            return 1;
         pre = &preload;
+        min_depth = pt.d;
+        u64 open = 0;
+        for (u64 s = 1; s <= smax; s++) open += preload[s] == ~0ULL;
+        if (pt.next > 0)
+            fprintf(stderr, "note: %s stopped inside degree %d (bucket %d/%d); degree %d runs "
+                            "again whole\n", used.c_str(), pt.d, pt.next, pt.nbuckets, pt.d);
+        fprintf(stderr, "resumed %s: %" PRIu64 " survivors carried in; continuing at degree %d, "
+                        "up to depth %d\n", used.c_str(), open, min_depth, depth);
+        if (min_depth < 2) min_depth = 2;
+    } else if (load_path) {
+        if (!sieve_ckpt::load_found(load_path, smax, preload)) return 1;
+        pre = &preload;
+        g_ck.base.kind = 1;                       // baseline of delta checkpoints
+        g_ck.base.path = load_path;
+        g_ck.base.image = preload;
+        g_ck.base.hash = sieve_ckpt::image_hash(preload.data() + 1, smax);
     } else if (loadsurv) {
-        if (!read_survivors(loadsurv, smax, min_depth, preload)) return 1;
+        u64 listed = 0, oor = 0;
+        if (!sieve_ckpt::load_survivors(loadsurv, smax, preload, &listed, &oor)) return 1;
+        if (oor)
+            fprintf(stderr, "warning: %" PRIu64 " survivor entries outside 1..%" PRIu64
+                            " ignored\n", oor, smax);
         pre = &preload;
+        g_ck.base.kind = 2;
+        g_ck.base.path = loadsurv;
+        g_ck.base.image = preload;
+        g_ck.base.hash = sieve_ckpt::image_hash(preload.data() + 1, smax);
     } else if (min_depth > 2) {
         fprintf(stderr, "warning: --min-depth %d without --load means degrees 2..%d are not "
                         "computed\n", min_depth, min_depth - 1);
+    }
+    if (resume_path && !ckpt_path) ckpt_path = resume_path;   // keep saving to the same file
+    if (ckpt_path) {
+        g_ck.on = true;
+        g_ck.path = ckpt_path;
+        g_ck.keep = ckpt_keep;
+        g_ck.period_s = ckpt_mins >= 0 ? ckpt_mins * 60.0 : stored_period_s;
+        g_ck.last_write = now_s();
+        g_ck.r = r;
+        g_ck.smax = smax;
+        g_ck.depth = depth;
+        struct sigaction sa;
+        memset(&sa, 0, sizeof sa);
+        sa.sa_handler = ckpt_on_signal;
+        sigaction(SIGTERM, &sa, nullptr);
+        sigaction(SIGINT, &sa, nullptr);
+        fprintf(stderr, "checkpointing to %s (%s, keeping %d generation%s)", ckpt_path,
+                g_ck.base.usable(smax) ? "delta vs baseline" : "full image", g_ck.keep,
+                g_ck.keep == 1 ? "" : "s");
+        if (g_ck.period_s > 0) fprintf(stderr, ", every %.1f min", g_ck.period_s / 60.0);
+        fprintf(stderr, "; SIGTERM/SIGINT saves and exits\n");
+    }
+    if (min_depth > depth) {
+        fprintf(stderr, "nothing to sieve: degrees up to %d are already done\n", depth);
+        min_depth = depth + 1;
     }
     double t0 = now_s();
     std::vector<u64> best;
@@ -236,7 +403,7 @@ int main(int argc, char **argv) {
             u64 b = best[s];
             if (b == ~0ULL || b == 0) continue;
             fprintf(fc, "%" PRIu64 " %u p%" PRIx64 "\n", s, (unsigned)(b >> 48),
-                    b & 0xFFFFFFFFFFFFULL);
+                    (u64)(b & 0xFFFFFFFFFFFFULL));
             nc++;
         }
         fclose(fc);
