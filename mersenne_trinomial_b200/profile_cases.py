@@ -7,6 +7,7 @@ capture (inputs larger than L2, a few GB at most, a handful of launches).
     python -m mersenne_trinomial_b200.profile_cases sieve_wide --depth D --dmin D --wide-from W
     python -m mersenne_trinomial_b200.profile_cases mul [--m M]
     python -m mersenne_trinomial_b200.profile_cases gcd|hgcd [--r R]
+    python -m mersenne_trinomial_b200.profile_cases hgcd_many [--r R] [--n N]
     python -m mersenne_trinomial_b200.profile_cases scan [--r R --n N --k K]
 """
 from __future__ import annotations
@@ -104,6 +105,28 @@ def case_hgcd(a):
     print(f"hgcd: {r} bits in {time.perf_counter() - t0:.3f} s, degree {degs[0]}, {st}")
 
 
+def case_hgcd_many(a):
+    """n half-gcds at once (one host thread and stream each): random r-bit
+    operands against x^r + x^s + 1, s = 1000 + 7919 i; aggregate wall time."""
+    r, n = a.r, a.n
+    pairs, keep = [], []
+    for i in range(n):
+        s = 1000 + 7919 * i
+        T = np.zeros((r + 1 + 63) // 64, dtype=np.uint64)
+        for e in (0, s, r):
+            T[e >> 6] |= np.uint64(1 << (e & 63))
+        da = M.DeviceBuffer.from_array(W.random_bits(r, 100 + i))
+        db = M.DeviceBuffer.from_array(T)
+        keep += [da, db]
+        pairs.append((da, r, db, r + 1))
+    M.stream_sync()
+    t0 = time.perf_counter()
+    degs, _, _ = M.gcd_large(pairs, max_parallel=n)
+    dt = time.perf_counter() - t0
+    print(f"hgcd_many: {n} x {r} bits in {dt:.1f} s, {dt / n:.2f} s per gcd, "
+          f"degrees {sorted(set(degs.tolist()))[:4]}")
+
+
 def case_sieve(a):
     smax = a.r // 2
     M.run_sieve(a.r, a.depth, smax)
@@ -120,7 +143,7 @@ def case_sieve_wide(a):
 def main(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("case", choices=["square", "fft", "mul", "sieve", "sieve_wide", "gcd", "hgcd",
-                                     "scan"])
+                                     "hgcd_many", "scan"])
     ap.add_argument("--r", type=int, default=136279841)
     ap.add_argument("--n", type=int, default=8)
     ap.add_argument("--k", type=int, default=3)
@@ -132,7 +155,7 @@ def main(argv=None):
     t0 = time.perf_counter()
     {"square": case_square, "fft": case_fft, "mul": case_mul, "sieve": case_sieve,
      "sieve_wide": case_sieve_wide, "gcd": case_gcd, "hgcd": case_hgcd,
-     "scan": case_scan}[a.case](a)
+     "hgcd_many": case_hgcd_many, "scan": case_scan}[a.case](a)
     print(f"{a.case}: done in {time.perf_counter() - t0:.3f} s")
     return 0
 
