@@ -8,6 +8,8 @@
 #include <cstdlib>
 #include <vector>
 
+#include "certfmt.h"
+
 typedef uint64_t u64;
 
 int main(int argc, char **argv) {
@@ -17,13 +19,14 @@ int main(int argc, char **argv) {
     }
     FILE *f = fopen(argv[1], "rb");
     if (!f) { perror("Error opening file"); return 1; }
-    std::vector<u64> rec(8192);
+    // records in rounds of 2^22, each round's lines formatted by several
+    // threads (certfmt.h) and written in order
+    std::vector<u64> rec((size_t)1 << 22);
     u64 s = 1;
-    for (size_t n; (n = fread(rec.data(), 8, rec.size(), f)) > 0;)
-        for (size_t i = 0; i < n; i++, s++) {
-            const u64 v = rec[i];
-            if (v == ~0ull) printf("%" PRIu64 " u\n", s);
-            else printf("%" PRIu64 " %u p%" PRIx64 "\n", s, (unsigned)(v >> 48), v & 0xFFFFFFFFFFFFull);
+    for (size_t n; (n = fread(rec.data(), 8, rec.size(), f)) > 0; s += n)
+        if (certfmt::write_lines(stdout, rec.data(), n, s, certfmt::Lines::Bin2Cert) < 0) {
+            fclose(f);
+            return 1;
         }
     const bool bad = ferror(f);
     fclose(f);

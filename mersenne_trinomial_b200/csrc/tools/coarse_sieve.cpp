@@ -41,6 +41,7 @@
 #include <unistd.h>
 #include <vector>
 
+#include "certfmt.h"
 #include "gf2e.h"
 #include "sieve_ckpt.h"
 
@@ -385,9 +386,9 @@ int main(int argc, char **argv) {
         snprintf(path, sizeof path, "%s.survivors.txt", prefix);
         FILE *fs = fopen(path, "w");
         if (!fs) { perror(path); return 1; }
-        for (u64 s = 1; s <= smax; s++)
-            if (best[s] == ~0ULL) fprintf(fs, "%" PRIu64 "\n", s);
-        fclose(fs);
+        const bool ok = certfmt::write_lines(fs, best.data() + 1, smax, 1,
+                                             certfmt::Lines::Survivors) >= 0;
+        if (fclose(fs) != 0 || !ok) { fprintf(stderr, "%s: write failed\n", path); return 1; }
         fprintf(stderr, "%" PRIu64 " survivors (no factor of degree <= %d) -> %s\n", nsurv,
                 depth, path);
     } else {
@@ -398,16 +399,10 @@ int main(int argc, char **argv) {
         snprintf(path, sizeof path, "%s.found.cert", prefix);
         FILE *fc = fopen(path, "w");
         if (!fc) { perror(path); return 1; }
-        u64 nc = 0;
-        for (u64 s = 1; s <= smax; s++) {
-            u64 b = best[s];
-            if (b == ~0ULL || b == 0) continue;
-            fprintf(fc, "%" PRIu64 " %u p%" PRIx64 "\n", s, (unsigned)(b >> 48),
-                    (u64)(b & 0xFFFFFFFFFFFFULL));
-            nc++;
-        }
-        fclose(fc);
-        fprintf(stderr, "%" PRIu64 " factors -> %s\n", nc, path);
+        const long long nc = certfmt::write_lines(fc, best.data() + 1, smax, 1,
+                                                  certfmt::Lines::Cert);
+        if (fclose(fc) != 0 || nc < 0) { fprintf(stderr, "%s: write failed\n", path); return 1; }
+        fprintf(stderr, "%lld factors -> %s\n", nc, path);
     }
     if (write_found) {
         snprintf(path, sizeof path, "%s.found.bin", prefix);
