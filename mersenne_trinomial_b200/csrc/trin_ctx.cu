@@ -56,7 +56,11 @@ int gf2e_trin_create(uint64_t r, gf2e_trin **out) {
               gf2e::wrap_mul_plans(c->wm);
     if (c->wrap) c->m = c->wm.mb;
     c->plan = gf2e::cached_plan(c->m);
-    if (!c->plan) { delete c; return gf2e::invalid("FFT plan for m=%d failed", c->m); }
+    if (!c->plan) {
+        const int m = c->m;
+        delete c;
+        return gf2e::invalid("FFT plan for m=%d failed", m);
+    }
     size_t n = (size_t)1 << c->m;
     cudaError_t e = cudaMalloc(&c->dA, c->nw * 8);
     if (e == cudaSuccess) e = cudaMalloc(&c->dACC, c->nw * 8);

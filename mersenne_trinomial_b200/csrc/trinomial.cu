@@ -139,13 +139,13 @@ GF2E_DEV void window_at(const u32 *__restrict__ in32, u32 i0, u32 n32, u32 sh,
             const u32 hi = __shfl_sync(0xffffffffu, y, (lane + 1) & 31);
             acc[q] ^= __funnelshift_r(lo[q], hi, sh);
         }
-        return;
-    }
+    } else {
 #pragma unroll
-    for (int q = 0; q < WPT; q++) {
-        const u32 lo = (i0 + 32 * q < n32) ? __ldg(p + 32 * q) : 0u;
-        const u32 hi = (i0 + 32 * q + 1 < n32) ? __ldg(p + 32 * q + 1) : 0u;
-        acc[q] ^= __funnelshift_r(lo, hi, sh);
+        for (int q = 0; q < WPT; q++) {
+            const u32 lo = (i0 + 32 * q < n32) ? __ldg(p + 32 * q) : 0u;
+            const u32 hi = (i0 + 32 * q + 1 < n32) ? __ldg(p + 32 * q + 1) : 0u;
+            acc[q] ^= __funnelshift_r(lo, hi, sh);
+        }
     }
 }
 // The window starting at input bit 32 w + K.  The highest index the warp
