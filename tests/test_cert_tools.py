@@ -60,7 +60,7 @@ def test_cert2bin_matches_reference(image, limit):
         assert a.read_bytes() == path.read_bytes()
 
 
-@pytest.mark.parametrize("corrupt", ["order", "bits", "hex"])
+@pytest.mark.parametrize("corrupt", ["order", "bits", "hex", "nop", "nodeg"])
 def test_cert2bin_rejects_what_the_reference_rejects(image, corrupt):
     _need(os.path.join(BIN, "cert2bin"), os.path.join(REF, "cert2bin"))
     d, path, _ = image
@@ -71,13 +71,19 @@ def test_cert2bin_rejects_what_the_reference_rejects(image, corrupt):
         lines[i] = f"{int(s) + 1} {deg} {mask}"
     elif corrupt == "bits":
         lines[i] = f"{s} {int(deg) + 1} {mask}"
-    else:
+    elif corrupt == "hex":
         lines[i] = f"{s} {deg} {mask}z"
+    elif corrupt == "nop":
+        lines[i] = f"{s} {deg} {mask[1:]}"
+    else:
+        lines[i] = f"{s} x{deg} {mask}"
     cert = d / f"bad_{corrupt}.cert"
     cert.write_text("\n".join(lines) + "\n")
     ro = _run([os.path.join(BIN, "cert2bin"), cert, d / "o.bin", 40])
     rr = _run([os.path.join(REF, "cert2bin"), cert, d / "r.bin", 40])
     assert ro.returncode != 0 and rr.returncode != 0
+    assert ro.stderr == rr.stderr                  # same message, same line number
+    assert str(i + 1) in ro.stderr
 
 
 def _summary(out):
