@@ -71,7 +71,7 @@ struct CkptRun {
     int depth = 0;
     sieve_ckpt::Baseline base;
     long stop_after = 0, degrees_done = 0;   // COARSE_TEST_STOP_AFTER_BUCKETS
-    volatile sig_atomic_t stop = 0;
+    std::atomic<int> stop{0};                // set by the signal handler (lock-free)
     std::mutex mu;                           // guards snap / snap_pt
     std::vector<u64> snap;                   // best[] at snap_pt
     sieve_ckpt::Point snap_pt;
@@ -82,7 +82,8 @@ struct CkptRun {
 };
 static CkptRun g_ck;
 
-extern "C" void ckpt_on_signal(int) { g_ck.stop = 1; }
+static_assert(std::atomic<int>::is_always_lock_free, "the stop flag is set in a signal handler");
+extern "C" void ckpt_on_signal(int) { g_ck.stop.store(1); }
 
 // degrees from here on take seconds to minutes at full smax (d = 36: 4.5 s,
 // d = 38: 151 s at r = 136279841), too long to wait for before saving
@@ -124,7 +125,7 @@ static void ckpt_stop_message() {
 // on resume).
 static void ckpt_watcher() {
     while (!g_ck.done.load()) {
-        if (g_ck.stop && g_ck.long_degree.load() && !g_ck.writer_claimed.exchange(true)) {
+        if (g_ck.stop.load() && g_ck.long_degree.load() && !g_ck.writer_claimed.exchange(true)) {
             {
                 std::lock_guard<std::mutex> lk(g_ck.mu);
                 if (g_ck.snap_valid) ckpt_write_snapshot();
@@ -172,7 +173,7 @@ static void run_gpu(u64 r, int depth, u64 smax, int min_depth, std::vector<u64> 
             marks[d] = m[d];
             g_ck.degrees_done++;
             const bool test_stop = g_ck.stop_after > 0 && g_ck.degrees_done >= g_ck.stop_after;
-            if ((g_ck.stop || test_stop) && d < depth) {
+            if ((g_ck.stop.load() || test_stop) && d < depth) {
                 if (g_ck.writer_claimed.exchange(true))   // the watcher is saving and exiting
                     for (;;) pause();
                 ckpt_take((const u64 *)dbest, d + 1);
