@@ -9,6 +9,7 @@ capture (inputs larger than L2, a few GB at most, a handful of launches).
     python -m mersenne_trinomial_b200.profile_cases gcd|hgcd [--r R]
     python -m mersenne_trinomial_b200.profile_cases hgcd_many [--r R] [--n N]
     python -m mersenne_trinomial_b200.profile_cases scan [--r R --n N --k K]
+    python -m mersenne_trinomial_b200.profile_cases scan_step [--r R --n N --block B]
 """
 from __future__ import annotations
 
@@ -82,6 +83,31 @@ def case_scan(a):
           lines[:3])
 
 
+def case_scan_step(a):
+    """The deep scan's per-degree work at r: n d <= 24 survivors on a
+    scanner with the blocked DDF (block a.block; 1 = per degree), a ramp
+    and one block, then 4 blocks of degrees; no interval end (no gcd)."""
+    import ctypes as C
+    from mersenne_trinomial_b200._lib import call
+    smax = 200000
+    best = M.run_sieve(a.r, 24, smax)
+    surv = [s for s in range(3, smax + 1) if int(best[s]) == 0xFFFFFFFFFFFFFFFF][:a.n]
+    h = C.c_void_p()
+    call("gf2e_scanner_create_blocked", a.r, len(surv), a.block, C.byref(h))
+    s_arr = np.asarray(surv, dtype=np.uint64)
+    call("gf2e_scanner_submit", h.value, s_arr.ctypes.data, len(surv), 24, 24 + 1000000,
+         1 << 30, 1 << 30, 0)
+    call("gf2e_scanner_step", h.value, a.block, None)
+    M.stream_sync()
+    t0 = time.perf_counter()
+    call("gf2e_scanner_step", h.value, 4 * a.block, None)
+    M.stream_sync()
+    dt = time.perf_counter() - t0
+    M.lib().gf2e_scanner_destroy(h.value)
+    print(f"scan_step: {len(surv)} s x {4 * a.block} degrees (block {a.block}) in {dt:.3f} s, "
+          f"{dt * 1e3 / (4 * a.block * len(surv)):.3f} ms per (s, degree)")
+
+
 def case_hgcd(a):
     """One half-gcd of a scan-like accumulator against x^r + x^s + 1."""
     r, s = a.r, 1001
@@ -143,7 +169,7 @@ def case_sieve_wide(a):
 def main(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("case", choices=["square", "fft", "mul", "sieve", "sieve_wide", "gcd", "hgcd",
-                                     "hgcd_many", "scan"])
+                                     "hgcd_many", "scan", "scan_step"])
     ap.add_argument("--r", type=int, default=136279841)
     ap.add_argument("--n", type=int, default=8)
     ap.add_argument("--k", type=int, default=3)
@@ -151,11 +177,12 @@ def main(argv=None):
     ap.add_argument("--depth", type=int, default=24)
     ap.add_argument("--dmin", type=int, default=2)
     ap.add_argument("--wide-from", type=int, default=32)
+    ap.add_argument("--block", type=int, default=28)
     a = ap.parse_args(argv)
     t0 = time.perf_counter()
     {"square": case_square, "fft": case_fft, "mul": case_mul, "sieve": case_sieve,
      "sieve_wide": case_sieve_wide, "gcd": case_gcd, "hgcd": case_hgcd,
-     "hgcd_many": case_hgcd_many, "scan": case_scan}[a.case](a)
+     "hgcd_many": case_hgcd_many, "scan": case_scan, "scan_step": case_scan_step}[a.case](a)
     print(f"{a.case}: done in {time.perf_counter() - t0:.3f} s")
     return 0
 
