@@ -60,12 +60,19 @@ def test_cert2bin_matches_reference(image, limit):
         assert a.read_bytes() == path.read_bytes()
 
 
+@pytest.mark.parametrize("where", ["early", "middle", "last"])
 @pytest.mark.parametrize("corrupt", ["order", "bits", "hex", "nop", "nodeg"])
-def test_cert2bin_rejects_what_the_reference_rejects(image, corrupt):
+def test_cert2bin_rejects_what_the_reference_rejects(image, corrupt, where):
+    """Same exit, message and line number as the reference, for errors in
+    the first and in later pieces of the parallel parse."""
     _need(os.path.join(BIN, "cert2bin"), os.path.join(REF, "cert2bin"))
     d, path, _ = image
     lines = _run([os.path.join(REF, "bin2cert"), path]).stdout.splitlines()
-    i = next(k for k, l in enumerate(lines) if " p" in l and k > 10)
+    start = {"early": 10, "middle": len(lines) * 3 // 5, "last": 0}[where]
+    if where == "last":
+        i = max(k for k, l in enumerate(lines) if " p" in l)
+    else:
+        i = next(k for k, l in enumerate(lines) if " p" in l and k > start)
     s, deg, mask = lines[i].split()
     if corrupt == "order":
         lines[i] = f"{int(s) + 1} {deg} {mask}"
@@ -77,7 +84,7 @@ def test_cert2bin_rejects_what_the_reference_rejects(image, corrupt):
         lines[i] = f"{s} {deg} {mask[1:]}"
     else:
         lines[i] = f"{s} x{deg} {mask}"
-    cert = d / f"bad_{corrupt}.cert"
+    cert = d / f"bad_{corrupt}_{where}.cert"
     cert.write_text("\n".join(lines) + "\n")
     ro = _run([os.path.join(BIN, "cert2bin"), cert, d / "o.bin", 40])
     rr = _run([os.path.join(REF, "cert2bin"), cert, d / "r.bin", 40])

@@ -70,7 +70,7 @@ def test_lines_match_printf_format(driver, tmp_path, kind, threads):
 
 def test_bin2cert_large_image_matches_reference(tmp_path):
     """4.5 M records (two formatter rounds) against the reference's own
-    bin2cert built from its sources."""
+    bin2cert built from its sources, and the text back through cert2bin."""
     ours, ref = os.path.join(BIN, "bin2cert"), os.path.join(REF, "bin2cert")
     for p in (ours, ref):
         if not os.path.exists(p):
@@ -82,3 +82,23 @@ def test_bin2cert_large_image_matches_reference(tmp_path):
     b = subprocess.run([ref, str(img)], capture_output=True, timeout=300)
     assert a.returncode == b.returncode == 0
     assert a.stdout == b.stdout
+    # and back (about 90 MB of text: more than one 64 MB read block of the
+    # parallel cert2bin), against the reference's cert2bin
+    c2b, rc2b = os.path.join(BIN, "cert2bin"), os.path.join(REF, "cert2bin")
+    if os.path.exists(c2b) and os.path.exists(rc2b):
+        rng = np.random.default_rng(3)                 # valid keys: masks of exactly d+1 bits
+        d = rng.integers(2, 48, size=k.size).astype(np.uint64)
+        m = rng.integers(0, 1 << 48, size=k.size, dtype=np.uint64)
+        m = (m & ((np.uint64(1) << d) - np.uint64(1))) | (np.uint64(1) << d)
+        k = (d << np.uint64(48)) | m
+        k[rng.random(k.size) < 0.2] = np.uint64(NONE)
+        k.astype("<u8").tofile(img)
+        cert = tmp_path / "big.cert"
+        cert.write_bytes(subprocess.run([ours, str(img)], capture_output=True, timeout=300).stdout)
+        for lim in (20, 47):
+            ro = subprocess.run([c2b, str(cert), str(tmp_path / "o.bin"), str(lim)], timeout=300)
+            rr = subprocess.run([rc2b, str(cert), str(tmp_path / "r.bin"), str(lim)], timeout=300)
+            assert ro.returncode == rr.returncode == 0
+            assert (tmp_path / "o.bin").read_bytes() == (tmp_path / "r.bin").read_bytes()
+        assert (tmp_path / "o.bin").read_bytes() == img.read_bytes()   # LIMIT 47: the image itself
+        assert (tmp_path / "o.bin").stat().st_size == 8 * k.size
