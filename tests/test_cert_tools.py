@@ -125,3 +125,64 @@ def test_check_ref_matches_reference(image, plant):
     rr = _run([os.path.join(REF, "check_ref")] + args)
     assert ro.returncode == rr.returncode == (0 if plant is None else 1)
     assert _summary(ro.stdout) == _summary(rr.stdout)
+
+
+def _random_cert(rng, n):
+    """A certificate of n records in the shapes cert2bin.c accepts, then
+    (half the time) one random corruption."""
+    out = []
+    for s in range(1, n + 1):
+        sp = rng.choice([" ", "  ", "\t", " \t"])
+        if rng.random() < 0.25:
+            tail = rng.choice(["", " trailing", "\tx"])
+            out.append(f"{s}{sp}u{tail}")
+            continue
+        d = int(rng.integers(1, 60))
+        mask = (int(rng.integers(0, 1 << 62)) & ((1 << d) - 1)) | (1 << d)
+        h = format(mask, "x")
+        if rng.random() < 0.2:
+            h = h.upper()
+        out.append(f"{s}{sp}{d}{sp}p{h}")
+    if rng.random() < 0.5 and n > 1:
+        i = int(rng.integers(0, n))
+        kind = rng.choice(["swap", "drop", "letter", "noP", "bits", "dup", "lead", "hexz"])
+        if kind == "swap" and i + 1 < n:
+            out[i], out[i + 1] = out[i + 1], out[i]
+        elif kind == "drop":
+            out.pop(i)
+        elif kind == "letter":
+            out[i] = "x" + out[i]
+        elif kind == "noP":
+            out[i] = out[i].replace(" p", " q").replace("\tp", "\tq")
+        elif kind == "bits":
+            out[i] = out[i] + "0"
+        elif kind == "dup":
+            out.insert(i, out[i])
+        elif kind == "lead":
+            out[i] = out[i].split(None, 1)[0] + " ?"
+        else:
+            out[i] = out[i] + "z"
+    sep = "\r\n" if rng.random() < 0.3 else "\n"
+    blank = sep * int(rng.integers(0, 3))
+    text = sep.join(l + (blank if rng.random() < 0.05 else "") for l in out)
+    return text + (sep if rng.random() < 0.8 else "")
+
+
+@pytest.mark.parametrize("seed", range(8))
+def test_cert2bin_fuzz_against_reference(tmp_path, seed):
+    """Random certificates and corruptions: the same exit code, message and
+    output as the reference's cert2bin, for small inputs (cut into as many
+    pieces as there are lines) and larger ones."""
+    _need(os.path.join(BIN, "cert2bin"), os.path.join(REF, "cert2bin"))
+    rng = np.random.default_rng(1000 + seed)
+    for case in range(25):
+        n = int(rng.choice([1, 2, 3, 7, 40, 3000]))
+        cert = tmp_path / f"c{case}.cert"
+        cert.write_bytes(_random_cert(rng, n).encode())
+        lim = int(rng.choice([47, 30, 10, 0]))
+        a, b = tmp_path / f"o{case}.bin", tmp_path / f"r{case}.bin"
+        ro = _run([os.path.join(BIN, "cert2bin"), cert, a, lim])
+        rr = _run([os.path.join(REF, "cert2bin"), cert, b, lim])
+        assert (ro.returncode, ro.stderr) == (rr.returncode, rr.stderr), (seed, case, n, lim)
+        if rr.returncode == 0:
+            assert a.read_bytes() == b.read_bytes(), (seed, case)
