@@ -228,6 +228,7 @@ inline bool read_one(const std::string &path, u64 r, u64 smax, std::vector<u64> 
         return false;
     }
     const int kind = (int)h32[4];
+    if (h32[5] > 4096) return fail("implausible baseline path length");
     std::string bpath(h32[5], '\0');
     if (h32[5] && fread(&bpath[0], 1, h32[5], f) != h32[5]) return fail("truncated baseline path");
     if (kind != 0) {

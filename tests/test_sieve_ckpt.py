@@ -205,3 +205,40 @@ def test_other_run_rejected(driver, tmp_path):
     assert read(driver, tmp_path / "c", tmp_path)[0] is None
     (tmp_path / "c").write_bytes(b"GF2SVCK1" + bytes(72))
     assert read(driver, tmp_path / "c", tmp_path)[0] is None
+
+
+def test_damaged_files_never_crash_the_reader(driver, tmp_path):
+    """A delta checkpoint cut at every length and with single bytes
+    flipped: the reader rejects it (or falls back to the older generation)
+    and never crashes."""
+    smax = 60
+    base = keys(11, smax)
+    best = base.copy()
+    best[[3, 17, 41]] = np.uint64((9 << 48) | 0x3FF)
+    save(tmp_path / "base.found.bin", base)
+    save(tmp_path / "best.bin", best)
+    save(tmp_path / "older.bin", keys(12, smax))
+    c = tmp_path / "c"
+    assert run(driver, "write", c, 2, R, smax, 24, 0, 9, 0, 0, tmp_path / "older.bin").returncode == 0
+    assert run(driver, "write", c, 2, R, smax, 24, 0, 10, 0, 0, tmp_path / "best.bin", 1,
+               tmp_path / "base.found.bin").returncode == 0
+    good = open(c, "rb").read()
+    rng = np.random.default_rng(5)
+    damaged = [good[:n] for n in range(len(good))]
+    for _ in range(60):
+        b = bytearray(good)
+        i = int(rng.integers(0, len(b)))
+        b[i] ^= 1 << int(rng.integers(0, 8))
+        damaged.append(bytes(b))
+    for bit in range(32):                          # every bit of the path length
+        b = bytearray(good)
+        b[28 + bit // 8] ^= 1 << (bit % 8)
+        damaged.append(bytes(b))
+    for data in damaged:
+        open(c, "wb").write(data)
+        # bytes: a damaged baseline path may be echoed in the message
+        p = subprocess.run([str(driver), "read", str(c), str(R), str(smax),
+                            str(tmp_path / "o.bin")], capture_output=True, timeout=60)
+        assert p.returncode in (0, 1), (len(data), p.returncode, p.stderr[-300:])
+        if p.returncode == 0 and p.stdout.split()[9].endswith(b"c.1"):
+            assert (load(tmp_path / "o.bin") == keys(12, smax)).all()
