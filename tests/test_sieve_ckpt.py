@@ -242,3 +242,30 @@ def test_damaged_files_never_crash_the_reader(driver, tmp_path):
         assert p.returncode in (0, 1), (len(data), p.returncode, p.stderr[-300:])
         if p.returncode == 0 and p.stdout.split()[9].endswith(b"c.1"):
             assert (load(tmp_path / "o.bin") == keys(12, smax)).all()
+
+
+def test_coarse_sieve_rejects_foreign_checkpoints(tmp_path):
+    """The tool reads --resume files before any device call: a checkpoint of
+    another r or smax, or not a checkpoint, ends the run with exit 1 and the
+    reason, as the reference's ckpt_read does (coarse_sieve.cu:742-760)."""
+    tool = os.path.join(ROOT, "mersenne_trinomial_b200", "bin", "coarse_sieve")
+    if not os.path.exists(tool):
+        pytest.skip("coarse_sieve not built")
+    smax = 22343
+    ref_file(tmp_path / "other_r", 17, 0, 0, r=R + 2, smax=smax, image=keys(1, smax))
+    ref_file(tmp_path / "other_smax", 17, 0, 0, r=R, smax=smax - 1, image=keys(1, smax - 1))
+    (tmp_path / "junk").write_bytes(b"not a checkpoint at all" * 4)
+    for name, why in [("other_r", "written for r="), ("other_smax", "written for r="),
+                      ("junk", "not a version-2 sieve checkpoint")]:
+        p = subprocess.run([tool, str(R), "20", str(tmp_path / "out"), "--resume",
+                            str(tmp_path / name)], capture_output=True, text=True, timeout=60)
+        assert p.returncode == 1, (name, p.stderr)
+        assert why in p.stderr and "no usable checkpoint generation" in p.stderr, p.stderr
+        assert not os.path.exists(f"{tmp_path / 'out'}.found.cert")
+    # a valid one is read and the resume point reported before the first
+    # device call (without a GPU the run stops there; with one it finishes)
+    ref_file(tmp_path / "ok", 17, 3, 8, r=R, smax=smax, image=keys(1, smax))
+    p = subprocess.run([tool, str(R), "20", str(tmp_path / "out"), "--resume", str(tmp_path / "ok")],
+                       capture_output=True, text=True, timeout=300)
+    assert p.returncode in (0, 1), p.stderr
+    assert "degree 17 runs again whole" in p.stderr and "continuing at degree 17" in p.stderr
