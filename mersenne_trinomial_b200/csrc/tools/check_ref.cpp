@@ -13,12 +13,21 @@
 // reference s with no sieve data, and in-range sieve factors the reference
 // lacks.  Exit 1 and "*** DISCREPANCIES FOUND ***" if any check fails, else
 // "ALL CHECKS PASSED".
+//
+// Input lines are read as fgets(buf, 512) would return them and parsed by
+// several threads (lines.h); each line is read either by a fast path for
+// the canonical forms ("s d p<hex>", "s"), whose result equals that of the
+// sscanf / strtoull calls below, or by those calls themselves, and the
+// lines are applied in file order.  At r = 136279841 that is 64 M
+// certificate lines in seconds instead of a quarter of a minute.
 #include <cinttypes>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
 #include <map>
 #include <vector>
+
+#include "lines.h"
 
 typedef uint64_t u64;
 
@@ -33,6 +42,69 @@ bool parse_factor(const char *line, u64 &s, int &d, u64 &mask) {
     if (sscanf(line, "%llu %d p%127s", &ss, &d, hex) != 3) return false;
     s = ss;
     mask = strtoull(hex, nullptr, 16);
+    return true;
+}
+
+bool dig(char c) { return c >= '0' && c <= '9'; }
+int hexd(char c) { return dig(c) ? c - '0' : (c >= 'a' && c <= 'f') ? c - 'a' + 10 : -1; }
+
+// One fgets chunk of a certificate or reference file.  The fast path takes
+// exactly "S D pH" with an optional final newline, S of 1..19 digits, D of
+// 1..9, H of 1..16 lowercase hex digits: no value can overflow there, so it
+// gives what parse_factor gives.  Anything else goes to parse_factor.
+struct Factor {
+    u64 s, mask;
+    int d;
+};
+bool factor_chunk(const char *p, size_t n, Factor &f) {
+    size_t i = 0, j;
+    u64 s = 0, mask = 0;
+    int d = 0;
+    for (j = i; j < n && j - i < 20 && dig(p[j]); j++) s = s * 10 + (u64)(p[j] - '0');
+    bool fast = j > i && j - i <= 19 && j < n && p[j] == ' ';
+    if (fast) {
+        i = j + 1;
+        for (j = i; j < n && j - i < 10 && dig(p[j]); j++) d = d * 10 + (p[j] - '0');
+        fast = j > i && j - i <= 9 && j + 1 < n && p[j] == ' ' && p[j + 1] == 'p';
+    }
+    if (fast) {
+        i = j + 2;
+        int h = 0;
+        for (j = i; j < n && j - i < 17 && (h = hexd(p[j])) >= 0; j++) mask = (mask << 4) | (u64)h;
+        fast = j > i && j - i <= 16 && (j == n || (j + 1 == n && p[j] == '\n'));
+    }
+    if (fast) {
+        f.s = s;
+        f.d = d;
+        f.mask = mask;
+        return true;
+    }
+    char line[lines::kFgetsBytes + 1];
+    lines::c_string(p, n, line);
+    return parse_factor(line, f.s, f.d, f.mask);
+}
+
+// One fgets chunk of a survivors file: strtoull(line, &end, 10), fast for
+// 1..19 digits and an optional newline.  Every chunk yields a record; `ok`
+// is end != line.
+struct Surv {
+    u64 s;
+    bool ok;
+};
+bool surv_chunk(const char *p, size_t n, Surv &r) {
+    size_t j = 0;
+    u64 s = 0;
+    for (; j < n && j < 20 && dig(p[j]); j++) s = s * 10 + (u64)(p[j] - '0');
+    if (j > 0 && j <= 19 && (j == n || (j + 1 == n && p[j] == '\n'))) {
+        r.s = s;
+        r.ok = true;
+        return true;
+    }
+    char line[lines::kFgetsBytes + 1];
+    lines::c_string(p, n, line);
+    char *end = nullptr;
+    r.s = strtoull(line, &end, 10);
+    r.ok = end != line;
     return true;
 }
 }  // namespace
@@ -60,21 +132,19 @@ int main(int argc, char **argv) {
                 "          [--found <f.found.bin>]\n", argv[0]);
         return 1;
     }
-    char line[512];
+    const int threads = lines::default_threads();
     // reference lines in the degree range (they also fix smax if not given)
     std::map<u64, std::pair<int, u64>> ref;
     u64 ref_lines = 0, ref_top = 0;
     {
         FILE *f = fopen(ref_path, "r");
         if (!f) { perror(ref_path); return 1; }
-        while (fgets(line, sizeof line, f)) {
-            u64 s, mask;
-            int d;
-            if (!parse_factor(line, s, d, mask) || d < dmin || d > dmax) continue;
-            ref[s] = {d, mask};
+        lines::for_each<Factor>(f, factor_chunk, [&](const Factor &x) {
+            if (x.d < dmin || x.d > dmax) return;
+            ref[x.s] = {x.d, x.mask};
             ref_lines++;
-            if (s > ref_top) ref_top = s;
-        }
+            if (x.s > ref_top) ref_top = x.s;
+        }, threads);
         fclose(f);
     }
     if (!smax) smax = ref_top;
@@ -83,29 +153,25 @@ int main(int argc, char **argv) {
     if (surv_path) {
         FILE *f = fopen(surv_path, "r");
         if (!f) { perror(surv_path); return 1; }
-        while (fgets(line, sizeof line, f)) {
-            char *end = nullptr;
-            const u64 s = strtoull(line, &end, 10);
-            if (end == line || s < 1 || s > smax) continue;
-            view[s] = SURVIVOR;
+        lines::for_each<Surv>(f, surv_chunk, [&](const Surv &x) {
+            if (!x.ok || x.s < 1 || x.s > smax) return;
+            view[x.s] = SURVIVOR;
             n_surv++;
-        }
+        }, threads);
         fclose(f);
     }
     for (const char *path : certs) {
         FILE *f = fopen(path, "r");
         if (!f) { perror(path); return 1; }
-        while (fgets(line, sizeof line, f)) {
-            u64 s, mask;
-            int d;
-            if (!parse_factor(line, s, d, mask) || s < 1 || s > smax) continue;
-            const u64 key = ((u64)d << 48) | mask;
-            if (view[s] == SURVIVOR)
+        lines::for_each<Factor>(f, factor_chunk, [&](const Factor &x) {
+            if (x.s < 1 || x.s > smax) return;
+            const u64 key = ((u64)x.d << 48) | x.mask;
+            if (view[x.s] == SURVIVOR)
                 printf("INCONSISTENT INPUT: s=%" PRIu64 " is in %s but also in the survivors file\n",
-                       s, path);
-            if (view[s] == NO_DATA || key < view[s]) view[s] = key;
+                       x.s, path);
+            if (view[x.s] == NO_DATA || key < view[x.s]) view[x.s] = key;
             n_cert++;
-        }
+        }, threads);
         fclose(f);
     }
     if (found_path) {

@@ -186,3 +186,63 @@ def test_cert2bin_fuzz_against_reference(tmp_path, seed):
         assert (ro.returncode, ro.stderr) == (rr.returncode, rr.stderr), (seed, case, n, lim)
         if rr.returncode == 0:
             assert a.read_bytes() == b.read_bytes(), (seed, case)
+
+
+def _odd_factor_line(rng, s):
+    """A certificate line in one of the forms sscanf("%llu %d p%127s") and
+    strtoull(hex, 16) read, canonical or not."""
+    d = int(rng.integers(1, 40))
+    mask = (int(rng.integers(0, 1 << 40)) & ((1 << d) - 1)) | (1 << d)
+    h = format(mask, "x")
+    form = int(rng.integers(0, 12))
+    if form == 0:
+        return f"{s} {d} p{h.upper()}"
+    if form == 1:
+        return f"{s} {d} p0x{h}"
+    if form == 2:
+        return f"  {s}\t{d}   p{h} trailing words"
+    if form == 3:
+        return f"{s:020d} {d} p{h}"
+    if form == 4:
+        return f"+{s} {d} p{h}"
+    if form == 5:
+        return f"{s} {d} p{h}" + "x" * 600           # split by fgets(512)
+    if form == 6:
+        return f"{s} {d} p{h}\r"
+    if form == 7:
+        return f"{s} {d} p{h}\0{s + 1} 3 p9"
+    if form == 8:
+        return f"garbage {s}"
+    if form == 9:
+        return ""
+    return f"{s} {d} p{h}"
+
+
+@pytest.mark.parametrize("seed", range(6))
+def test_check_ref_fuzz_against_reference(tmp_path, seed):
+    """Random certificate, survivors and reference files mixing canonical
+    lines with other forms the reference's parsing accepts or skips: the
+    same report and exit code as the reference's check_ref."""
+    _need(os.path.join(BIN, "check_ref"), os.path.join(REF, "check_ref"))
+    rng = np.random.default_rng(2000 + seed)
+    for case in range(6):
+        smax = int(rng.choice([50, 400, 3000]))
+        surv = sorted(set(int(x) for x in rng.integers(1, smax + 1, size=smax // 4)))
+        cert_s = [s for s in range(1, smax + 1) if s not in set(surv) or rng.random() < 0.02]
+        cert = "\n".join(_odd_factor_line(rng, s) if rng.random() < 0.3 else
+                         f"{s} {int(rng.integers(2, 36))} p{format((1 << 35) | int(rng.integers(0, 1 << 30)), 'x')}"
+                         for s in cert_s)
+        surv_txt = "\n".join(str(s) if rng.random() < 0.9 else rng.choice([f" {s}", f"{s}\r", f"+{s}", "x"])
+                             for s in surv)
+        ref = "\n".join(f"{s} {int(rng.integers(30, 35))} p{format((1 << 34) | s, 'x')}"
+                        for s in sorted(rng.choice(np.arange(1, smax + 1), size=smax // 5, replace=False).tolist()))
+        (tmp_path / "c.cert").write_bytes(cert.encode() + b"\n")
+        (tmp_path / "s.txt").write_bytes(surv_txt.encode() + (b"\n" if rng.random() < 0.7 else b""))
+        (tmp_path / "r.txt").write_bytes(ref.encode() + b"\n")
+        args = ["--ref", tmp_path / "r.txt", "--cert", tmp_path / "c.cert", "--survivors",
+                tmp_path / "s.txt", "--dmin", int(rng.choice([2, 30])), "--dmax", 34]
+        if rng.random() < 0.5:
+            args += ["--smax", smax]
+        ro = _run([os.path.join(BIN, "check_ref")] + args)
+        rr = _run([os.path.join(REF, "check_ref")] + args)
+        assert (ro.returncode, ro.stdout) == (rr.returncode, rr.stdout), (seed, case)
