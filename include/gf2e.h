@@ -190,7 +190,9 @@ int gf2e_mul(const gf2e_fft_plan *plan, const uint64_t *a_dev, uint64_t abits,
  * before any stream capture.  All calls share the scratch, which keeps the
  * last call's contents (nothing is read from it before being written): calls
  * that overlap on the GPU, e.g. on two streams, race.  a_dev, b_dev and
- * out_dev (gf2e_mul_out_words words) are the caller's device buffers. */
+ * out_dev (gf2e_mul_out_words words) are the caller's device buffers.  Calls
+ * after a cudaDeviceReset in the same process are not supported (the reset
+ * drops the uploaded tables the set-up left on the device). */
 #define GF2E_MUL_NOALLOC_MAX_M 18
 int gf2e_mul_noalloc(const uint64_t *a_dev, uint64_t abits, const uint64_t *b_dev,
                      uint64_t bbits, uint64_t *out_dev, void *stream);

@@ -26,6 +26,7 @@
 #include <mutex>
 #include <vector>
 #include <algorithm>
+#include <atomic>
 
 namespace {
 
@@ -820,10 +821,11 @@ void twiddle_byte_tables(u64 *tab) {
 int twiddle_table_words() { return NTWTAB * 256; }
 
 static int allow_tile_smem() {
-    static bool done[64] = {false};
+    // set once per device; two threads racing here both set the same values
+    static std::atomic<bool> done[64];
     int dev = 0;
     cudaGetDevice(&dev);
-    if (dev >= 0 && dev < 64 && !done[dev]) {
+    if (dev >= 0 && dev < 64 && !done[dev].load(std::memory_order_acquire)) {
         cudaError_t e = cudaSuccess;
 #define GF2E_FFT_ATTR(T, D, N)                                                              \
     if (e == cudaSuccess)                                                                   \
@@ -834,7 +836,7 @@ static int allow_tile_smem() {
         GF2E_FFT_ATTR(13, false, 1) GF2E_FFT_ATTR(13, true, 2)
 #undef GF2E_FFT_ATTR
         if (e != cudaSuccess) return cuda_status(e, "k_fft_pass smem attribute");
-        done[dev] = true;
+        done[dev].store(true, std::memory_order_release);
     }
     return GF2E_OK;
 }

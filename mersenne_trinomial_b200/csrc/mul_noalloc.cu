@@ -12,9 +12,14 @@
 // The fixed arrays are host-side stand-ins in host code; their device
 // addresses come from cudaGetSymbolAddress, taken once per device, with that
 // device current, by the set-up in the first call on that device (which also
-// fills the twiddle tables and builds the pass schedules on the host).
+// fills the twiddle tables and builds the pass schedules on the host).  The
+// set-up is published with release/acquire ordering, so a thread that sees a
+// device as ready also sees its addresses and plans.  A cudaDeviceReset
+// reloads the module and drops what the set-up uploaded; calls after one in
+// the same process are not supported.
 #include "gf2e_internal.cuh"
 
+#include <atomic>
 #include <mutex>
 
 namespace gf2e {
@@ -36,7 +41,7 @@ static __device__ __align__(256) uint64_t g_noalloc_scratch[2ull << MAX_M];
 static __device__ __align__(256) uint64_t g_noalloc_twiddles[TAB_WORDS];
 
 struct DeviceState {
-    bool ready = false;
+    std::atomic<bool> ready{false};
     u64 *scratch = nullptr;      // device address of g_noalloc_scratch
     u64 *twiddles = nullptr;     // device address of g_noalloc_twiddles
     gf2e_fft_plan *plan[MAX_M + 1] = {};
@@ -57,9 +62,18 @@ int setup_device(int dev) {
     gf2e::twiddle_byte_tables(host_tab);
     e = cudaMemcpyToSymbol(g_noalloc_twiddles, host_tab, sizeof host_tab);
     if (e != cudaSuccess) return gf2e::cuda_status(e, "noalloc twiddle upload");
-    for (int m = 1; m <= MAX_M; m++)
-        GF2E_TRY(gf2e::fft_plan_create_tables(m, d.twiddles, &d.plan[m]));
-    d.ready = true;
+    // plans go into a local table first: a failure part way destroys the
+    // ones already made, and the next call starts the set-up afresh
+    gf2e_fft_plan *plans[MAX_M + 1] = {};
+    for (int m = 1; m <= MAX_M; m++) {
+        int st = gf2e::fft_plan_create_tables(m, d.twiddles, &plans[m]);
+        if (st != GF2E_OK) {
+            for (int k = 1; k < m; k++) gf2e_fft_plan_destroy(plans[k]);
+            return st;
+        }
+    }
+    for (int m = 1; m <= MAX_M; m++) d.plan[m] = plans[m];
+    d.ready.store(true, std::memory_order_release);
     return GF2E_OK;
 }
 
@@ -82,9 +96,9 @@ int gf2e_mul_noalloc(const uint64_t *a_dev, uint64_t abits, const uint64_t *b_de
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return gf2e::cuda_status(e, "cudaGetDevice");
     if (dev < 0 || dev >= 64) return gf2e::invalid("device index %d out of range", dev);
-    if (!g_state[dev].ready) {
+    if (!g_state[dev].ready.load(std::memory_order_acquire)) {
         std::lock_guard<std::mutex> lk(g_mu);
-        if (!g_state[dev].ready) GF2E_TRY(setup_device(dev));
+        if (!g_state[dev].ready.load(std::memory_order_acquire)) GF2E_TRY(setup_device(dev));
     }
     const DeviceState &d = g_state[dev];
     // the first forward pass writes every point of FA and FB (operand chunks,

@@ -49,6 +49,7 @@
 #include "gf2e_internal.cuh"
 
 #include <algorithm>
+#include <atomic>
 #include <cstdlib>
 #include <mutex>
 #include <vector>
@@ -884,14 +885,15 @@ int gf2e_sieve_run(uint64_t r, int dmin, int dmax, uint64_t smax, uint64_t *best
         }
     }
     {   // k_strip may take up to 2^STRIP_LOG_MAX entries of shared memory
-        static bool attr_done[64] = {false};
+        // set once per device; two threads racing here both set the same value
+        static std::atomic<bool> attr_done[64];
         int dev = 0;
         cudaGetDevice(&dev);
-        if (dev >= 0 && dev < 64 && !attr_done[dev]) {
+        if (dev >= 0 && dev < 64 && !attr_done[dev].load(std::memory_order_acquire)) {
             cudaError_t e = cudaFuncSetAttribute(k_strip, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                                  (int)(sizeof(u64) << STRIP_LOG_MAX));
             if (e != cudaSuccess) return gf2e::cuda_status(e, "k_strip smem attribute");
-            attr_done[dev] = true;
+            attr_done[dev].store(true, std::memory_order_release);
         }
     }
     cudaStream_t st = (cudaStream_t)stream;

@@ -412,6 +412,60 @@ int gf2e_trin_set_one(uint64_t *states_dev, size_t stride_words, int nstates, ui
     return gf2e::trin_set_const(states_dev, stride_words, nstates, r, 1, (cudaStream_t)stream);
 }
 
+}  // extern "C"
+
+namespace {
+
+// The host-buffer entry point's device workspace, its copy stream and event:
+// one set per host thread, kept between calls, released on a device switch
+// (on the device that owns them) and when the thread exits.
+struct FrobeniusWorkspace {
+    u64 *buf = nullptr;
+    size_t bytes = 0;
+    int dev = -1;
+    cudaStream_t copy_st = nullptr;
+    cudaEvent_t ev_done = nullptr;
+    int copy_dev = -1;
+
+    template <class F>
+    static void on_device(int dev, F &&f) {
+        int cur = -1;
+        if (cudaGetDevice(&cur) != cudaSuccess) return;
+        if (cur != dev && cudaSetDevice(dev) != cudaSuccess) return;
+        f();
+        if (cur != dev) cudaSetDevice(cur);
+    }
+    void release_buffer() {
+        if (buf) on_device(dev, [&] { cudaFree(buf); });
+        buf = nullptr;
+        bytes = 0;
+        dev = -1;
+    }
+    void release_stream() {
+        if (copy_st || ev_done)
+            on_device(copy_dev < 0 ? 0 : copy_dev, [&] {
+                if (ev_done) cudaEventDestroy(ev_done);
+                if (copy_st) cudaStreamDestroy(copy_st);
+            });
+        copy_st = nullptr;
+        ev_done = nullptr;
+        copy_dev = -1;
+    }
+    ~FrobeniusWorkspace() {
+        release_buffer();
+        release_stream();
+    }
+};
+
+FrobeniusWorkspace &frobenius_workspace() {
+    static thread_local FrobeniusWorkspace w;
+    return w;
+}
+
+}  // namespace
+
+extern "C" {
+
 int gf2e_trin_frobenius_host(uint64_t r, const uint64_t *s_host, int nstates, uint32_t k,
                              uint64_t *out_host, size_t out_stride_words, void *stream) {
     GF2E_TRY(check_rs(r, 1));
@@ -423,22 +477,22 @@ int gf2e_trin_frobenius_host(uint64_t r, const uint64_t *s_host, int nstates, ui
     const size_t stride = nw + (nw & 1);
     const size_t need = 2 * stride * (size_t)nstates * 8 + (size_t)nstates * 8;
     // per-thread device workspace, grown on demand and kept between calls
-    static thread_local u64 *ws = nullptr;
-    static thread_local size_t ws_bytes = 0;
-    static thread_local int ws_dev = -1;
+    FrobeniusWorkspace &W = frobenius_workspace();
     int dev = 0;
-    cudaGetDevice(&dev);
-    if (ws_bytes < need || ws_dev != dev) {
-        if (ws && ws_dev == dev) cudaFree(ws);
-        ws = nullptr;
-        ws_bytes = 0;
-        cudaError_t e = cudaMalloc(&ws, need);
-        if (e != cudaSuccess) return gf2e::cuda_status(e, "frobenius workspace");
-        ws_bytes = need;
-        ws_dev = dev;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return gf2e::cuda_status(e, "cudaGetDevice");
+    if (W.bytes < need || W.dev != dev) {
+        W.release_buffer();
+        e = cudaMalloc(&W.buf, need);
+        if (e != cudaSuccess) {
+            W.buf = nullptr;
+            return gf2e::cuda_status(e, "frobenius workspace");
+        }
+        W.bytes = need;
+        W.dev = dev;
     }
-    u64 *states = ws, *scratch = ws + stride * nstates, *sdev = scratch + stride * nstates;
-    cudaError_t e = cudaMemcpyAsync(sdev, s_host, (size_t)nstates * 8, cudaMemcpyHostToDevice, st);
+    u64 *states = W.buf, *scratch = W.buf + stride * nstates, *sdev = scratch + stride * nstates;
+    e = cudaMemcpyAsync(sdev, s_host, (size_t)nstates * 8, cudaMemcpyHostToDevice, st);
     if (e != cudaSuccess) return gf2e::cuda_status(e, "frobenius s upload");
     GF2E_TRY(gf2e::trin_set_const(states, stride, nstates, r, 2, st));
     // Large batches go in groups, one after another on `st`, each group's
@@ -464,15 +518,18 @@ int gf2e_trin_frobenius_host(uint64_t r, const uint64_t *s_host, int nstates, ui
     }
     groups[ngroups++] = left;
     std::reverse(groups, groups + ngroups);
-    static thread_local cudaStream_t copy_st = nullptr;
-    static thread_local cudaEvent_t ev_done = nullptr;
-    static thread_local int copy_dev = -1;
-    if (!copy_st || copy_dev != dev) {
-        e = cudaStreamCreateWithFlags(&copy_st, cudaStreamNonBlocking);
-        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ev_done, cudaEventDisableTiming);
-        if (e != cudaSuccess) return gf2e::cuda_status(e, "frobenius copy stream");
-        copy_dev = dev;
+    if (!W.copy_st || W.copy_dev != dev) {
+        W.release_stream();
+        e = cudaStreamCreateWithFlags(&W.copy_st, cudaStreamNonBlocking);
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&W.ev_done, cudaEventDisableTiming);
+        if (e != cudaSuccess) {
+            W.release_stream();
+            return gf2e::cuda_status(e, "frobenius copy stream");
+        }
+        W.copy_dev = dev;
     }
+    cudaStream_t copy_st = W.copy_st;
+    cudaEvent_t ev_done = W.ev_done;
     for (int gi = 0, g0 = 0; gi < ngroups; g0 += groups[gi], gi++) {
         const int ng = groups[gi];
         GF2E_TRY(gf2e_trin_square_batch(states + stride * g0, scratch + stride * g0, stride, ng,

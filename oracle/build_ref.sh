@@ -20,9 +20,15 @@
 # enabled but no host-specific ISA so the binaries also run on the GPU
 # hosts' CPUs.
 set -euo pipefail
-REF="${GF2E_REFERENCE_SRC:-/root/reference/src}"
+# GF2E_REFERENCE_SRC names the reference's src/ directory; without it (or
+# with a directory that does not exist) nothing is built.
+REF="${GF2E_REFERENCE_SRC:-}"
 HERE="$(cd "$(dirname "$0")" && pwd)"
 OUT="$HERE/_ref"
+if [ -z "$REF" ]; then
+    echo "build_ref: set GF2E_REFERENCE_SRC to the reference's src/ directory; skipping" >&2
+    exit 0
+fi
 if [ ! -d "$REF" ]; then
     echo "build_ref: reference sources not present ($REF); skipping" >&2
     exit 0

@@ -161,7 +161,9 @@ def gen_scan():
 
 def gen_verify():
     """Divisibility verdicts of the reference's Python verifier (verify_gf2_trinomial.py)."""
-    src = os.environ.get("GF2E_REFERENCE_SRC", "/root/reference/src")
+    src = os.environ.get("GF2E_REFERENCE_SRC")
+    if not src or not os.path.isdir(src):
+        raise SystemExit("make_golden: set GF2E_REFERENCE_SRC to the reference's src/ directory")
     sys.path.insert(0, src)
     import verify_gf2_trinomial as V  # the reference's own checker
     lines = [(136279841, "474 41 p3991ef16129"), (136279841, "33 5 p29"),
@@ -181,6 +183,8 @@ def gen_verify():
 
 
 if __name__ == "__main__":
+    if not os.environ.get("GF2E_REFERENCE_SRC"):
+        raise SystemExit("make_golden: set GF2E_REFERENCE_SRC to the reference's src/ directory")
     if not os.path.exists(os.path.join(REF, "sieve_ref")):
         O.build()
     gen_sieve()

@@ -53,6 +53,10 @@ def test_noalloc_matches_allocating_entry_two_calls(engine):
         assert (got1 == want1).all(), (ab, bb)
         assert (got2 == want2).all(), (ab, bb)
         assert (got1b == want1).all(), (ab, bb)
+        if ab * bb <= 10**10:
+            # and against the oracle's schoolbook product where that is quick
+            from oracle import oracle as O
+            assert (got2 == O.comb_mul(a2, ab, b2, bb)).all(), (ab, bb)
 
 
 def test_noalloc_rejects_products_beyond_the_fixed_scratch(engine):
