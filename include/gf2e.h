@@ -111,11 +111,18 @@ int gf2e_trin_square(const uint64_t *in_dev, uint64_t *out_dev, uint64_t r,
 /* Batched repeated squaring: each of `nstates` states (state i at
  * states_dev + i*stride_words, stride_words >= nw, even) is squared k times
  * mod x^r + x^(s_i) + 1, s_i = s_dev[i] (device array).  scratch_dev has the
- * same shape as states_dev; the result is left in states_dev.
+ * same shape as states_dev; the result is left in states_dev.  Two squarings
+ * run per pass over the states (F -> F^4 mod T) where r < 2^31; the word
+ * after an odd nw in each stride is padding and may be overwritten.
  * (trinomial_stage2.cu run loop 232-253: F_k = x^(2^k) mod T, many s at once.) */
 int gf2e_trin_square_batch(uint64_t *states_dev, uint64_t *scratch_dev,
                            size_t stride_words, int nstates, uint64_t r,
                            const uint64_t *s_dev, uint32_t k, void *stream);
+
+/* Squarings per pass that gf2e_trin_square_batch uses for this r and
+ * stride: 2, or 1 where the fused pass does not apply (r >= 2^31, an odd
+ * stride, or GF2E_SQUARINGS_PER_PASS=1 in the environment).  Host only. */
+int gf2e_trin_squarings_per_pass(uint64_t r, size_t stride_words);
 
 /* Host-buffer form of the above, the whole of trinomial_stage2.cu `run`
  * (195-277) for many s with k0 > k1: F_k = x^(2^k) mod x^r + x^(s_i) + 1 for
@@ -164,6 +171,20 @@ int gf2e_fft_inv(const gf2e_fft_plan *plan, uint64_t *f_dev, void *stream);
 
 /* Twiddle table W[t], t < n/2 (CudaFFT::dW / CantorFFT::W), to host memory. */
 int gf2e_fft_twiddles(const gf2e_fft_plan *plan, uint64_t *W_host);
+
+/* The product's element-wise steps on device buffers, as the reference's
+ * kernels (gf2_cantor_cuda.h:114-156):
+ *   pack:        f[k] = 32-bit chunk k of a (nwords words) for k < nchunks,
+ *                0 for nchunks <= k < n (k_pack);
+ *   pointwise:   fa[k] = fa[k] * fb[k] in GF(2^64), k < n (k_pointwise);
+ *   overlap_add: out[w] = XOR of the 64-bit coefficients f[k], k < nchunks,
+ *                placed at bit 32 k, for w < owords (k_overlap_add). */
+int gf2e_fft_pack(const uint64_t *a_dev, size_t nwords, uint64_t *f_dev,
+                  size_t nchunks, size_t n, void *stream);
+int gf2e_fft_pointwise(uint64_t *fa_dev, const uint64_t *fb_dev, size_t n,
+                       void *stream);
+int gf2e_fft_overlap_add(const uint64_t *f_dev, size_t nchunks, uint64_t *out_dev,
+                         size_t owords, void *stream);
 
 /* FFT size exponent for an abits x bbits product (gf2_cantor_engine.h:232-238)
  * and the product's word count (mul_out_words, :201-203). */
@@ -333,6 +354,13 @@ int gf2e_scanner_status(const gf2e_scanner *scanner, int *queued, int *resident,
 int gf2e_scanner_poll(gf2e_scanner *scanner, gf2e_scan_result *results_host,
                       uint64_t *tags_host, uint64_t *masks_host, size_t mask_cap_words,
                       int cap, int *nout);
+/* Verified frontier of every resident s: every degree <= k_host[i] is known
+ * clear (the last interval gcd that came back 1 ended there; k0 before
+ * the first).  A job resubmitted with k0 = that frontier continues the
+ * scan, which is what trinomial_scan's resume state records
+ * (trinomial_scan.cu:144-170, 262-275). */
+int gf2e_scanner_frontiers(const gf2e_scanner *scanner, uint64_t *s_host, uint64_t *k_host,
+                           uint64_t *tags_host, int cap, int *nout);
 
 /* ======================================================================
  * (f) Serving: continuous batching of (r, s-set, d-range) search jobs.  No
@@ -383,9 +411,18 @@ int gf2e_trin_set_s(gf2e_trin *ctx, uint64_t s);          /* TrinGPU::set_s */
  * r = 136279841). */
 int gf2e_trin_buffers(gf2e_trin *ctx, uint64_t **dA, uint64_t **dACC,
                       uint64_t **dT0, size_t *nw, int *m);
+/* The context's other scratch with the reference's sizes (TrinGPU::dT1,
+ * 2*nw words; dFA and dFB, 2^m_full points each) and m_full, the plain FFT
+ * size exponent of an r-bit x r-bit product (TrinGPU::m,
+ * gf2_trinomial_cuda.h:97-115).  The context's own products overwrite them. */
+int gf2e_trin_scratch(gf2e_trin *ctx, uint64_t **dT1, uint64_t **dFA,
+                      uint64_t **dFB, int *m_full);
 int gf2e_trin_reset_A(gf2e_trin *ctx, void *stream);      /* k_set_x on dA */
 int gf2e_trin_reset_acc(gf2e_trin *ctx, void *stream);    /* ACC <- 1 */
 int gf2e_trin_square_A(gf2e_trin *ctx, void *stream);     /* dA <- dA^2 mod T */
+/* dA <- dA^(2^k) mod T, two squarings per pass over dA (no counterpart in
+ * the reference's TrinGPU, whose callers loop over square_A). */
+int gf2e_trin_square_A_k(gf2e_trin *ctx, uint64_t k, void *stream);
 /* dT0 (2r-1 bits) <- x * y, both r-bit device operands (TrinGPU::mul_dev). */
 int gf2e_trin_mul_dev(gf2e_trin *ctx, const uint64_t *x_dev,
                       const uint64_t *y_dev, void *stream);

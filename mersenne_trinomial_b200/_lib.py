@@ -96,6 +96,7 @@ SIGNATURES = {
     "gf2e_trin_square": (_i32, [_vp, _vp, _u64, _u64, _vp]),
     "gf2e_trin_square_batch": (_i32, [_vp, _vp, _sz, _i32, _u64, _vp, C.c_uint32, _vp]),
     "gf2e_trin_frobenius_host": (_i32, [_u64, _vp, _i32, C.c_uint32, _vp, _sz, _vp]),
+    "gf2e_trin_squarings_per_pass": (_i32, [_u64, _sz]),
     "gf2e_trin_set_x": (_i32, [_vp, _sz, _i32, _u64, _vp]),
     "gf2e_trin_set_one": (_i32, [_vp, _sz, _i32, _u64, _vp]),
     "gf2e_trin_reduce": (_i32, [_vp, _u64, _vp, _u64, _u64, _vp]),
@@ -106,6 +107,9 @@ SIGNATURES = {
     "gf2e_fft_fwd": (_i32, [_vp, _vp, _vp]),
     "gf2e_fft_inv": (_i32, [_vp, _vp, _vp]),
     "gf2e_fft_twiddles": (_i32, [_vp, _vp]),
+    "gf2e_fft_pack": (_i32, [_vp, _sz, _vp, _sz, _sz, _vp]),
+    "gf2e_fft_pointwise": (_i32, [_vp, _vp, _sz, _vp]),
+    "gf2e_fft_overlap_add": (_i32, [_vp, _sz, _vp, _sz, _vp]),
     "gf2e_mul_fft_m": (_i32, [_u64, _u64]),
     "gf2e_mul_out_words": (_sz, [_u64, _u64]),
     "gf2e_mul": (_i32, [_vp, _vp, _u64, _vp, _u64, _vp, _vp, _vp, _vp]),
@@ -141,13 +145,16 @@ SIGNATURES = {
     "gf2e_scanner_step": (_i32, [_vp, _i32, _vp]),
     "gf2e_scanner_status": (_i32, [_vp, _P(_i32), _P(_i32), _P(_i32), _P(_u64)]),
     "gf2e_scanner_poll": (_i32, [_vp, _P(ScanResult), _vp, _vp, _sz, _i32, _P(_i32)]),
+    "gf2e_scanner_frontiers": (_i32, [_vp, _vp, _vp, _vp, _i32, _P(_i32)]),
     "gf2e_trin_create": (_i32, [_u64, _P(_vp)]),
     "gf2e_trin_destroy": (_i32, [_vp]),
     "gf2e_trin_set_s": (_i32, [_vp, _u64]),
     "gf2e_trin_buffers": (_i32, [_vp, _P(_vp), _P(_vp), _P(_vp), _P(_sz), _P(_i32)]),
+    "gf2e_trin_scratch": (_i32, [_vp, _P(_vp), _P(_vp), _P(_vp), _P(_i32)]),
     "gf2e_trin_reset_A": (_i32, [_vp, _vp]),
     "gf2e_trin_reset_acc": (_i32, [_vp, _vp]),
     "gf2e_trin_square_A": (_i32, [_vp, _vp]),
+    "gf2e_trin_square_A_k": (_i32, [_vp, _u64, _vp]),
     "gf2e_trin_mul_dev": (_i32, [_vp, _vp, _vp, _vp]),
     "gf2e_trin_reduce_T0": (_i32, [_vp, _vp, _u64, _vp]),
     "gf2e_trin_accumulate": (_i32, [_vp, _vp]),

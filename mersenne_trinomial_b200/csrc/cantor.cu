@@ -1028,6 +1028,30 @@ int gf2e_fft_inv(const gf2e_fft_plan *plan, uint64_t *f_dev, void *stream) {
     return gf2e::fft_run(plan, false, f_dev, (cudaStream_t)stream);
 }
 
+int gf2e_fft_pack(const uint64_t *a_dev, size_t nwords, uint64_t *f_dev, size_t nchunks,
+                  size_t n, void *stream) {
+    if (!a_dev || !f_dev || n == 0) return gf2e::invalid("gf2e_fft_pack: bad arguments");
+    const u64 nc = std::min<u64>(nchunks, 2 * (u64)nwords);
+    cudaStream_t st = (cudaStream_t)stream;
+    k_pack_batch<<<gf2e::grid_for(n, 256), 256, 0, st>>>(
+        reinterpret_cast<const u32 *>(a_dev), 0, nc, 0, f_dev, 0, n);
+    GF2E_CHECK_LAUNCH("k_pack_batch");
+    return GF2E_OK;
+}
+
+int gf2e_fft_pointwise(uint64_t *fa_dev, const uint64_t *fb_dev, size_t n, void *stream) {
+    if (!fa_dev || !fb_dev) return gf2e::invalid("gf2e_fft_pointwise: null argument");
+    if (n == 0) return GF2E_OK;
+    return gf2e::pointwise(fa_dev, fb_dev, n, (cudaStream_t)stream);
+}
+
+int gf2e_fft_overlap_add(const uint64_t *f_dev, size_t nchunks, uint64_t *out_dev,
+                         size_t owords, void *stream) {
+    if (!f_dev || !out_dev) return gf2e::invalid("gf2e_fft_overlap_add: null argument");
+    if (owords == 0) return GF2E_OK;
+    return gf2e::overlap_add(f_dev, nchunks, out_dev, owords, (cudaStream_t)stream);
+}
+
 int gf2e_fft_twiddles(const gf2e_fft_plan *plan, uint64_t *W_host) {
     if (!plan || !W_host) return gf2e::invalid("gf2e_fft_twiddles: null argument");
     const u64 *b = basis_host();

@@ -38,6 +38,8 @@
 namespace gf2e {
 int trin_square_states(const u64 *in, u64 *out, size_t stride, int nstates, u64 r,
                        const u64 *s_dev, cudaStream_t st);
+int frobenius_states(u64 *a, u64 *b, size_t stride, int nstates, u64 r, const u64 *s_dev,
+                     u64 k, cudaStream_t st, u64 s_uniform);
 int trin_set_const(u64 *states, size_t stride, int nstates, u64 r, u64 w0, cudaStream_t st);
 int trin_reduce_batch(const u64 *P, size_t pstride, size_t pw, u64 L, u64 *out, size_t ostride,
                       u64 r, const u64 *s_dev, int batch, cudaStream_t st);
@@ -319,27 +321,14 @@ int load_slot(gf2e_scanner &S, int j, const gf2e_scanner::Job &job, cudaStream_t
             k_esym_step<<<dim3(gx, jj), 256, 0, st>>>(Hj, HSj, S.stride, jj, S.nw, S.r, job.s);
             GF2E_CHECK_LAUNCH("k_esym_step");
         }
-        for (u64 k = 0; k <= job.k0; k++) {
-            const bool even = (k & 1) == 0;
-            GF2E_TRY(gf2e::trin_square_states(even ? Hj : HSj, even ? HSj : Hj, S.stride, m, S.r,
-                                              sHj, st));
-        }
-        if ((job.k0 + 1) & 1) {
-            e = cudaMemcpyAsync(Hj, HSj, (size_t)m * S.stride * 8, cudaMemcpyDeviceToDevice, st);
-            if (e != cudaSuccess) return gf2e::cuda_status(e, "scanner block ramp");
-        }
+        GF2E_TRY(gf2e::frobenius_states(Hj, HSj, S.stride, m, S.r, sHj, job.k0 + 1, st, 0));
         S.slot[j] = gf2e_scanner::Slot{
             job, job.k0, job.k0, gf2e::sched_first(job.sched, (u64)m, job.k0 + 1, job.L0)};
         return GF2E_OK;
     }
     GF2E_TRY(gf2e::trin_set_const(S.F + S.stride * j, S.stride, 1, S.r, 2, st));
-    for (u64 k = 0; k < job.k0; k++) {
-        GF2E_TRY(gf2e::trin_square_states(S.F + S.stride * j, S.Fs + S.stride * j, S.stride, 1,
-                                          S.r, S.sdev + j, st));
-        e = cudaMemcpyAsync(S.F + S.stride * j, S.Fs + S.stride * j, S.nw * 8,
-                            cudaMemcpyDeviceToDevice, st);
-        if (e != cudaSuccess) return gf2e::cuda_status(e, "scanner ramp");
-    }
+    GF2E_TRY(gf2e::frobenius_states(S.F + S.stride * j, S.Fs + S.stride * j, S.stride, 1, S.r,
+                                    S.sdev + j, job.k0, st, 0));
     S.slot[j] = gf2e_scanner::Slot{job, job.k0, job.k0,
                                    gf2e::sched_first(job.sched, 1, job.k0 + 1, job.L0)};
     return GF2E_OK;
@@ -423,10 +412,8 @@ int block_kernels(gf2e_scanner &S, int na, cudaStream_t st) {
     GF2E_TRY(product_tail(S, na, S.C, st));
     GF2E_TRY(gf2e::trin_reduce_batch(S.P, S.pstride, S.ow, 2 * S.r - 1, S.ACC, S.stride, S.r,
                                      S.sdev, na, st));
-    for (int t = 0; t < m; t++)
-        GF2E_TRY(gf2e::trin_square_states((t & 1) ? S.HS : S.H, (t & 1) ? S.H : S.HS, S.stride,
-                                          na * m, S.r, S.sH, st));
-    return GF2E_OK;
+    // h <- h^(2^m): m squarings of every residue, two per pass, back in H
+    return gf2e::frobenius_states(S.H, S.HS, S.stride, na * m, S.r, S.sH, (u64)m, st, 0);
 }
 
 int step_kernels(gf2e_scanner &S, int na, cudaStream_t st) {
@@ -707,6 +694,20 @@ int gf2e_scanner_status(const gf2e_scanner *S, int *queued, int *resident, int *
     if (resident) *resident = S->nact;
     if (finished) *finished = (int)S->done.size();
     if (sd_pairs) *sd_pairs = S->sd_pairs;
+    return GF2E_OK;
+}
+
+int gf2e_scanner_frontiers(const gf2e_scanner *S, uint64_t *s_host, uint64_t *k_host,
+                           uint64_t *tags_host, int cap, int *nout) {
+    if (!S || !s_host || !k_host || !nout || cap < 0)
+        return gf2e::invalid("scanner frontiers: bad arguments");
+    int n = 0;
+    for (int j = 0; j < S->nact && n < cap; j++, n++) {
+        s_host[n] = S->slot[j].job.s;
+        k_host[n] = S->slot[j].iv;
+        if (tags_host) tags_host[n] = S->slot[j].job.tag;
+    }
+    *nout = n;
     return GF2E_OK;
 }
 

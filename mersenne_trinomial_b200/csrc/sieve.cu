@@ -45,7 +45,9 @@
 //               short-period progression with shared-memory atomics and
 //               writes the slice back once (last writer, so plain min).
 // All degrees are enqueued on one stream with no host round trip; the only
-// synchronisation is the final overflow/status read.
+// synchronisation is the final overflow/status read.  A progression that
+// finds the strip or heavy list full is marked inline by its class thread
+// (same marks, so the same best[]; only slower).
 #include "gf2e_internal.cuh"
 
 #include <algorithm>
@@ -71,7 +73,23 @@ struct Counters {
     unsigned long long classes[DMAX_WIDE + 1];
     unsigned long long marks[DMAX_WIDE + 1];
     unsigned long long nlist;             // wide leader list fill
+    unsigned long long spilled;           // progressions marked inline for want of list room
 };
+
+// List capacities in force: the workspace holds SCAP / HCAP records, and
+// GF2E_SIEVE_STRIP_CAP / GF2E_SIEVE_HEAVY_CAP may lower them (tests use tiny
+// ones to drive every progression through the spill path).
+struct ListCaps {
+    u64 strip, heavy;
+};
+
+// A progression that finds its list full is marked at once by the thread
+// that found it: the same atomicMin marks the list kernels would make, so
+// the result is unchanged, only slower.
+GF2E_DEV void mark_inline(u64 first, u64 n, u64 smax, unsigned long long key,
+                          unsigned long long *__restrict__ best) {
+    for (u64 s = first; s <= smax; s += n) atomicMin(&best[s], key);
+}
 
 // workspace: progression lists and counters first, then the table region
 // (dense A and L tables, or the wide log-table slice), whose size may be
@@ -88,6 +106,16 @@ constexpr Layout layout() {
 size_t dense_table_bytes(int d) {
     size_t tab = ((size_t)1 << d) * sizeof(u32);
     return (tab + 255) & ~(size_t)255;
+}
+
+ListCaps list_caps() {
+    auto cap = [](const char *name, u64 full) {
+        const char *e = getenv(name);
+        if (!e) return full;
+        const unsigned long long v = strtoull(e, nullptr, 10);
+        return (u64)std::min<unsigned long long>(std::max<unsigned long long>(v, 1), full);
+    };
+    return ListCaps{cap("GF2E_SIEVE_STRIP_CAP", SCAP), cap("GF2E_SIEVE_HEAVY_CAP", HCAP)};
 }
 
 // log-table entry bytes of a wide degree (exponents below 2^d)
@@ -245,6 +273,7 @@ struct DegreeArgs {
     int nsub;
     u64 subq[6];
     u64 strip;                            // strip width (entries of best[] per CTA)
+    ListCaps caps;
 };
 
 // j is the least element of its cyclotomic coset {j 2^i mod M}
@@ -381,14 +410,22 @@ k_classes(const u32 *__restrict__ A, const u32 *__restrict__ L, const DegreeArgs
         my_marks += count;
         if (n < a.strip) {
             unsigned long long slot = atomicAdd(&cnt->nstrip, 1ull);
-            if (slot < SCAP) strip[slot] = Prog{first, n, key};
-            else atomicAdd(&cnt->overflow, 1ull);
+            if (slot < a.caps.strip) {
+                strip[slot] = Prog{first, n, key};
+            } else {
+                atomicAdd(&cnt->spilled, 1ull);
+                mark_inline(first, n, a.smax, key, best);
+            }
         } else if (count <= INLINE) {
-            for (u64 s = first; s <= a.smax; s += n) atomicMin(&best[s], key);
+            mark_inline(first, n, a.smax, key, best);
         } else {
             unsigned long long slot = atomicAdd(&cnt->nheavy, 1ull);
-            if (slot < HCAP) heavy[slot] = Prog{first, n, key};
-            else atomicAdd(&cnt->overflow, 1ull);
+            if (slot < a.caps.heavy) {
+                heavy[slot] = Prog{first, n, key};
+            } else {
+                atomicAdd(&cnt->spilled, 1ull);
+                mark_inline(first, n, a.smax, key, best);
+            }
         }
     };
     for_each_leader(M, d, wq_all[threadIdx.x >> 5], [&](u64 j, bool valid) {
@@ -410,9 +447,9 @@ k_classes(const u32 *__restrict__ A, const u32 *__restrict__ L, const DegreeArgs
 
 // heavy progressions: block-strided over records, threads over marks
 __global__ void k_heavy(const Prog *__restrict__ heavy, const Counters *__restrict__ cnt,
-                        u64 smax, unsigned long long *__restrict__ best) {
+                        u64 smax, unsigned long long *__restrict__ best, u64 hcap) {
     u64 nh = cnt->nheavy;
-    if (nh > HCAP) nh = HCAP;
+    if (nh > hcap) nh = hcap;
     for (u64 rec = blockIdx.x; rec < nh; rec += gridDim.x) {
         Prog p = heavy[rec];
         for (u64 s = p.s0 + (u64)threadIdx.x * p.n; s <= smax; s += (u64)blockDim.x * p.n)
@@ -423,10 +460,10 @@ __global__ void k_heavy(const Prog *__restrict__ heavy, const Counters *__restri
 // short-period progressions, one STRIP-wide slice of best[] per CTA
 __global__ void __launch_bounds__(512)
 k_strip(const Prog *__restrict__ strip, const Counters *__restrict__ cnt, u64 smax,
-        unsigned long long *__restrict__ best, const u64 STRIP) {
+        unsigned long long *__restrict__ best, const u64 STRIP, u64 scap) {
     extern __shared__ unsigned long long sb[];
     u64 ns = cnt->nstrip;
-    if (ns > SCAP) ns = SCAP;
+    if (ns > scap) ns = scap;
     const u64 nstrips = (smax + 1 + STRIP - 1) / STRIP;
     for (u64 sid = blockIdx.x; sid < nstrips; sid += gridDim.x) {
         const u64 lo = sid * STRIP;
@@ -536,6 +573,7 @@ struct WideArgs {
     u64 rmod, smax, lo, len;
     int nsub, first_slice;
     u64 subq[6];
+    ListCaps caps;
 };
 
 // a class of leader j whose progression (first, period n) reaches s <= smax:
@@ -570,11 +608,15 @@ GF2E_DEV void wide_mark(u64 j, u64 first, u64 n, const WideArgs &a,
     const unsigned long long key = ((u64)d << 48) | mask;
     my_marks += count;
     if (count <= INLINE) {
-        for (u64 s = first; s <= a.smax; s += n) atomicMin(&best[s], key);
+        mark_inline(first, n, a.smax, key, best);
     } else {
         unsigned long long slot = atomicAdd(&cnt->nheavy, 1ull);
-        if (slot < HCAP) heavy[slot] = Prog{first, n, key};
-        else atomicAdd(&cnt->overflow, 1ull);
+        if (slot < a.caps.heavy) {
+            heavy[slot] = Prog{first, n, key};
+        } else {
+            atomicAdd(&cnt->spilled, 1ull);
+            mark_inline(first, n, a.smax, key, best);
+        }
     }
 }
 
@@ -837,6 +879,7 @@ int gf2e_sieve_run(uint64_t r, int dmin, int dmax, uint64_t smax, uint64_t *best
     };
     std::vector<WidePlan> wargs;          // one per (wide degree, slice)
     const int wfrom = wide_from();
+    const ListCaps caps = list_caps();
     for (int d = dmin; d <= dmax; d++) {
         const u64 M = ((u64)1 << d) - 1, rmod = r % M;
         if (h_gcd(rmod ? rmod : M, M) != 1) {
@@ -855,6 +898,7 @@ int gf2e_sieve_run(uint64_t r, int dmin, int dmax, uint64_t smax, uint64_t *best
             a.rmod = rmod;
             a.smax = smax;
             a.strip = strip_w;
+            a.caps = caps;
             a.nsub = np;
             for (int i = 0; i < np; i++) a.subq[i] = subq[i];
             args.push_back(a);
@@ -868,6 +912,7 @@ int gf2e_sieve_run(uint64_t r, int dmin, int dmax, uint64_t smax, uint64_t *best
         }
         w.rmod = rmod;
         w.smax = smax;
+        w.caps = caps;
         w.nsub = np;
         for (int i = 0; i < np; i++) w.subq[i] = subq[i];
         // the leader list first in the region when it fits beside a slice of
@@ -952,11 +997,11 @@ int gf2e_sieve_run(uint64_t r, int dmin, int dmax, uint64_t smax, uint64_t *best
         }
         GF2E_CHECK_LAUNCH("k_wide_classes");
     }
-    k_heavy<<<gf2e::sm_count() * 16, 256, 0, st>>>(heavy, cnt, smax, best);
+    k_heavy<<<gf2e::sm_count() * 16, 256, 0, st>>>(heavy, cnt, smax, best, caps.heavy);
     GF2E_CHECK_LAUNCH("k_heavy");
     u64 nstrips = (smax + strip_w) / strip_w;
     k_strip<<<gf2e::grid_for(nstrips * 512, 512, 2), 512, strip_w * sizeof(u64), st>>>(
-        strip, cnt, smax, best, strip_w);
+        strip, cnt, smax, best, strip_w, caps.strip);
     GF2E_CHECK_LAUNCH("k_strip");
     // status: overflow / internal failures (one small read, synchronizes)
     unsigned long long flags[4];
@@ -964,7 +1009,7 @@ int gf2e_sieve_run(uint64_t r, int dmin, int dmax, uint64_t smax, uint64_t *best
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);
     if (e != cudaSuccess) return gf2e::cuda_status(e, "sieve status");
     if (flags[2]) {
-        gf2e::set_error("sieve progression list overflow (%llu)", flags[2]);
+        gf2e::set_error("sieve leader list overflow (%llu)", flags[2]);
         return GF2E_ERR_OVERFLOW;
     }
     if (flags[3]) {

@@ -6,7 +6,8 @@
 //                  [--interval Lmax] [--l0 L0] [--batch B] [--block m] [--verbose 0..3]
 //                  [--sched doubling|linear|opt] [--q0 N] [--sched-G N] [--sched-rho R]
 //                  [--Zq N]                              (tsfactor's interval schedules)
-//                  [--gcd-threads N] [--state FILE]      (accepted, unused)
+//                  [--state FILE]                        (resume state, see below)
+//                  [--gcd-threads N]                     (accepted, unused)
 //   trinomial_scan --selftest
 //
 // Output <out_prefix>.results.txt, appended, resumable (s already listed are
@@ -18,6 +19,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <map>
 #include <set>
 #include <string>
 #include <vector>
@@ -91,34 +93,138 @@ static bool divides(u64 r, u64 s, const u64 *p, size_t pw, u64 d) {
     return true;
 }
 
+// Resume state (trinomial_scan.cu:144-170): records {0x4E435354, r, s, k, nw}
+// followed by F_k = x^(2^k) mod T, k the verified frontier of an s in
+// progress (every degree <= k clear).  The reference keeps one record, its
+// one s in progress; this tool scans many s at once and writes one record
+// per resident s, and reads every record of a file (a reference file is the
+// one-record case).  Only k is needed to resume: the scan restarts that s
+// at k0 = k, computing F_k again on the GPU.
+static const u64 kStateMagic = 0x4E435354ULL;
+
+static std::map<u64, u64> load_states(const char *path, u64 r, size_t nw) {
+    std::map<u64, u64> out;
+    FILE *f = path ? fopen(path, "rb") : nullptr;
+    if (!f) return out;
+    u64 hdr[5];
+    std::vector<u64> F(nw);
+    while (fread(hdr, 8, 5, f) == 5 && hdr[0] == kStateMagic && hdr[1] == r && hdr[4] == nw &&
+           fread(F.data(), 8, nw, f) == nw)
+        out[hdr[2]] = hdr[3];
+    fclose(f);
+    return out;
+}
+
+static bool save_states(const char *path, u64 r, size_t nw, const std::map<u64, u64> &fr) {
+    std::string tmp = std::string(path) + ".tmp";
+    FILE *f = fopen(tmp.c_str(), "wb");
+    if (!f) return false;
+    std::vector<u64> F(nw);
+    bool ok = true;
+    for (const auto &e : fr) {
+        const u64 s = e.first, k = e.second;
+        ok = gf2e_trin_frobenius_host(r, &s, 1, (uint32_t)k, F.data(), nw, nullptr) == GF2E_OK;
+        if (!ok) break;
+        const u64 hdr[5] = {kStateMagic, r, s, k, (u64)nw};
+        ok = fwrite(hdr, 8, 5, f) == 5 && fwrite(F.data(), 8, nw, f) == nw;
+        if (!ok) break;
+    }
+    ok = (fclose(f) == 0) && ok;
+    if (ok) ok = rename(tmp.c_str(), path) == 0;
+    return ok;
+}
+
+// Scan every s, writing each result line as soon as its s finishes (the
+// reference appends per survivor too), with the resume state saved every
+// 30 s (GF2E_SCAN_STATE_SECS) when a frontier moved.  `fres` null: results
+// only counted.
 static int run(u64 r, const std::vector<u64> &surv, u64 k0, u64 maxd, u64 L0, u64 Lmax,
                int batch, int block, const gf2e_sched &sched, FILE *fres, int verbose,
-               u64 *nfound, u64 *nu, u64 *nbad) {
-    const size_t cap = 4096;
-    std::vector<gf2e_scan_result> res(surv.size());
-    std::vector<u64> masks(surv.size() * cap);
-    int st = gf2e_scan_sched(r, surv.data(), (int)surv.size(), k0, maxd, &sched, L0, Lmax, batch,
-                             block, res.data(), masks.data(), cap, nullptr);
-    if (st != GF2E_OK) {
-        fprintf(stderr, "scan failed: %s (%s)\n", gf2e_status_string(st), gf2e_last_error());
+               const char *state_path, u64 *nfound, u64 *nu, u64 *nbad) {
+    const size_t cap = 4096, nw = (size_t)((r + 63) >> 6);
+    std::map<u64, u64> resume = load_states(state_path, r, nw);
+    gf2e_scanner *S = nullptr;
+    int st = gf2e_scanner_create_blocked(r, std::max(1, std::min<int>(batch, (int)surv.size())),
+                                         block, &S);
+    if (st == GF2E_OK) st = gf2e_scanner_set_schedule(S, &sched);
+    auto fail = [&](int code) {
+        fprintf(stderr, "scan failed: %s (%s)\n", gf2e_status_string(code), gf2e_last_error());
+        if (S) gf2e_scanner_destroy(S);
         return 1;
-    }
+    };
+    if (st != GF2E_OK) return fail(st);
+    size_t pending = 0;
     for (size_t i = 0; i < surv.size(); i++) {
-        const gf2e_scan_result &R = res[i];
-        if (R.status == 1) {
-            std::string hx = hexmask(&masks[i * cap], R.mask_words);
-            if (fres) fprintf(fres, "%" PRIu64 " %" PRIu64 " p%s\n", R.s, R.d, hx.c_str());
-            if (!divides(r, R.s, &masks[i * cap], R.mask_words, R.d)) ++*nbad;
-            ++*nfound;
-            if (verbose >= 1) fprintf(stderr, "  s=%" PRIu64 ": d=%" PRIu64 "\n", R.s, R.d);
-        } else if (R.status == 2) {
-            if (fres) fprintf(fres, "%" PRIu64 " u\n", R.s);
+        u64 start = k0;
+        auto it = resume.find(surv[i]);
+        if (it != resume.end() && it->second > k0) {
+            start = std::min(it->second, maxd);
+            if (verbose >= 1)
+                fprintf(stderr, "  s=%" PRIu64 ": resumed at k=%" PRIu64 "\n", surv[i], start);
+        }
+        if (start >= maxd) {                            // nothing left below maxd
+            if (fres) { fprintf(fres, "%" PRIu64 " u\n", surv[i]); fflush(fres); }
             ++*nu;
-        } else {
-            if (fres) fprintf(fres, "%" PRIu64 " r%" PRIu64 "-%" PRIu64 "\n", R.s, R.rlo, R.rhi);
-            ++*nfound;
+            continue;
+        }
+        st = gf2e_scanner_submit(S, &surv[i], 1, start, maxd, L0, Lmax, (u64)i);
+        if (st != GF2E_OK) return fail(st);
+        pending++;
+    }
+    std::vector<gf2e_scan_result> res(64);
+    std::vector<u64> tags(64), masks(64 * cap);
+    std::vector<u64> fs(batch), fk(batch);
+    std::map<u64, u64> saved;
+    double last_save = now_s(), save_every = 30.0;
+    if (const char *e = getenv("GF2E_SCAN_STATE_SECS")) save_every = atof(e);
+    while (pending > 0) {
+        st = gf2e_scanner_step(S, 256, nullptr);
+        if (st != GF2E_OK) return fail(st);
+        int n = 0;
+        do {
+            st = gf2e_scanner_poll(S, res.data(), tags.data(), masks.data(), cap, 64, &n);
+            if (st != GF2E_OK) return fail(st);
+            for (int q = 0; q < n; q++) {
+                const gf2e_scan_result &R = res[q];
+                if (R.status == 1) {
+                    std::string hx = hexmask(&masks[q * cap], R.mask_words);
+                    if (fres) fprintf(fres, "%" PRIu64 " %" PRIu64 " p%s\n", R.s, R.d, hx.c_str());
+                    if (!divides(r, R.s, &masks[q * cap], R.mask_words, R.d)) ++*nbad;
+                    ++*nfound;
+                    if (verbose >= 1) fprintf(stderr, "  s=%" PRIu64 ": d=%" PRIu64 "\n", R.s, R.d);
+                } else if (R.status == 2) {
+                    if (fres) fprintf(fres, "%" PRIu64 " u\n", R.s);
+                    ++*nu;
+                } else {
+                    if (fres) fprintf(fres, "%" PRIu64 " r%" PRIu64 "-%" PRIu64 "\n", R.s, R.rlo, R.rhi);
+                    ++*nfound;
+                }
+                pending--;
+            }
+            if (n && fres) fflush(fres);
+        } while (n == 64);
+        int q = 0, a = 0;
+        gf2e_scanner_status(S, &q, &a, nullptr, nullptr);
+        if (pending > 0 && q == 0 && a == 0) {
+            fprintf(stderr, "scan failed: %zu results lost\n", pending);
+            gf2e_scanner_destroy(S);
+            return 1;
+        }
+        if (state_path && now_s() - last_save >= save_every) {
+            int nf = 0;
+            gf2e_scanner_frontiers(S, fs.data(), fk.data(), nullptr, batch, &nf);
+            std::map<u64, u64> now;
+            for (int i = 0; i < nf; i++)
+                if (fk[i] > k0) now[fs[i]] = fk[i];
+            if (!now.empty() && now != saved) {
+                if (!save_states(state_path, r, nw, now))
+                    fprintf(stderr, "warning: could not write state file %s\n", state_path);
+                saved = now;
+            }
+            last_save = now_s();
         }
     }
+    gf2e_scanner_destroy(S);
     return 0;
 }
 
@@ -147,7 +253,8 @@ static int selftest() {
         {64, 4096, 6, {GF2E_SCHED_OPT, 0, 60, 1.25, 0}, "block m=6 sched-opt G=60"}};
     for (const Pol &p : pol) {
         u64 nf = 0, nu = 0, nb = 0;
-        if (run(r, surv, k0, maxd, p.L0, p.Lmax, 64, p.block, p.sched, nullptr, 0, &nf, &nu, &nb))
+        if (run(r, surv, k0, maxd, p.L0, p.Lmax, 64, p.block, p.sched, nullptr, 0, nullptr, &nf,
+                &nu, &nb))
             return 1;
         bool ok = surv.size() == 104 && nf == 102 && nu == 2 && nb == 0;
         printf("scan r=4423 k0=5 maxd=200 %s: %zu survivors, "
@@ -174,6 +281,7 @@ int main(int argc, char **argv) {
     std::string prefix = argv[5];
     u64 L0 = 64, Lmax = 4096;
     int batch = 64, verbose = 1, block = 1;
+    const char *state_path = nullptr;
     gf2e_sched sched{GF2E_SCHED_DOUBLING, 0, 4000, 1.25, 0};
     for (int i = 6; i < argc; i++) {
         if (!strcmp(argv[i], "--sched") && i + 1 < argc) {
@@ -197,9 +305,9 @@ int main(int argc, char **argv) {
         else if (!strcmp(argv[i], "--batch") && i + 1 < argc) batch = atoi(argv[++i]);
         else if (!strcmp(argv[i], "--block") && i + 1 < argc) block = atoi(argv[++i]);
         else if (!strcmp(argv[i], "--verbose") && i + 1 < argc) verbose = atoi(argv[++i]);
-        else if ((!strcmp(argv[i], "--gcd-threads") || !strcmp(argv[i], "--state")) && i + 1 < argc) {
-            fprintf(stderr, "note: %s ignored (gcds run on the GPU; results file is the resume record)\n",
-                    argv[i]);
+        else if (!strcmp(argv[i], "--state") && i + 1 < argc) state_path = argv[++i];
+        else if (!strcmp(argv[i], "--gcd-threads") && i + 1 < argc) {
+            fprintf(stderr, "note: %s ignored (gcds run on the GPU)\n", argv[i]);
             i++;
         } else {
             fprintf(stderr, "unknown option %s\n", argv[i]);
@@ -241,7 +349,7 @@ int main(int argc, char **argv) {
     u64 nf = 0, nu = 0, nb = 0;
     int rc = todo.empty() ? 0
                           : run(r, todo, k0, maxd, L0, Lmax, batch, block, sched, fres, verbose,
-                                &nf, &nu, &nb);
+                                state_path, &nf, &nu, &nb);
     fclose(fres);
     fprintf(stderr, "done: %" PRIu64 " found, %" PRIu64 " u, %.1fs total%s\n", nf, nu,
             now_s() - t0, nb ? " (WARNING: some factors failed verification)" : "");

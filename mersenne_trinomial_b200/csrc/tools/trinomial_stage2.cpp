@@ -141,7 +141,16 @@ int main(int argc, char **argv) {
         }
         double t0 = now_s();
         for (u64 k = k_start + 1; k <= k1; k++) {
-            S.square_A();
+            // before k0, squarings k and k + 1 share one pass when nothing
+            // (product, checkpoint, progress line) happens at k
+            const bool quiet = k < k0 && k + 1 <= k1 && k % 4096 != 0 &&
+                               !(state_path && k % 1024 == 0);
+            if (quiet) {
+                S.square_A_k(2);
+                k++;
+            } else {
+                S.square_A();
+            }
             if (k >= k0) S.accumulate();
             if (state_path && (k % 1024 == 0 || k == k1)) {
                 std::vector<u64> a = read_dev(S.dA, S.nw), c = read_dev(S.dACC, S.nw);

@@ -15,6 +15,8 @@ int mul(const gf2e_fft_plan *plan, const u64 *a, u64 abits, const u64 *b, u64 bb
         u64 *out, u64 *fa, u64 *fb, cudaStream_t st);
 int mul_fft_m(u64 abits, u64 bbits);
 gf2e_fft_plan *cached_plan(int m);
+int frobenius_states(u64 *a, u64 *b, size_t stride, int nstates, u64 r, const u64 *s_dev,
+                     u64 k, cudaStream_t st, u64 s_uniform);
 }  // namespace gf2e
 
 namespace {
@@ -26,7 +28,8 @@ __global__ void k_xor_word0(u64 *p, u64 v) {
 struct gf2e_trin {
     u64 r = 0, s = 0;
     size_t nw = 0;
-    int m = 0;
+    int m = 0;                            // transform size the products run at
+    int m_full = 0;                       // 2^m_full >= 2 ceil(r/32) - 1 (TrinGPU::m)
     gf2e_fft_plan *plan = nullptr;
     u64 *dA = nullptr, *dACC = nullptr, *dT0 = nullptr, *dT1 = nullptr;
     u64 *dFA = nullptr, *dFB = nullptr;
@@ -51,7 +54,7 @@ int gf2e_trin_create(uint64_t r, gf2e_trin **out) {
     gf2e_trin *c = new gf2e_trin;
     c->r = r;
     c->nw = (size_t)((r + 63) >> 6);
-    c->m = gf2e::mul_fft_m(r, r);
+    c->m = c->m_full = gf2e::mul_fft_m(r, r);
     c->wrap = !getenv("GF2E_NO_WRAP") && gf2e::wrap_mul_plan(r, r, c->wm) &&
               gf2e::wrap_mul_plans(c->wm);
     if (c->wrap) c->m = c->wm.mb;
@@ -61,11 +64,15 @@ int gf2e_trin_create(uint64_t r, gf2e_trin **out) {
         delete c;
         return gf2e::invalid("FFT plan for m=%d failed", m);
     }
-    size_t n = (size_t)1 << c->m;
-    cudaError_t e = cudaMalloc(&c->dA, c->nw * 8);
+    // the transform buffers and dT1 have the reference's sizes (2^m_full
+    // points, 2 nw words), so callers may use them as TrinGPU's dFA, dFB and
+    // dT1; wrapped products use the first 2^m points
+    size_t n = (size_t)1 << c->m_full;
+    // dA has an even word count (the two-squaring pass stores word pairs)
+    cudaError_t e = cudaMalloc(&c->dA, (c->nw + (c->nw & 1)) * 8);
     if (e == cudaSuccess) e = cudaMalloc(&c->dACC, c->nw * 8);
     if (e == cudaSuccess) e = cudaMalloc(&c->dT0, (2 * c->nw + 2) * 8);
-    if (e == cudaSuccess) e = cudaMalloc(&c->dT1, c->nw * 8);
+    if (e == cudaSuccess) e = cudaMalloc(&c->dT1, (2 * c->nw + 2) * 8);
     if (e == cudaSuccess) e = cudaMalloc(&c->dFA, n * 8);
     if (e == cudaSuccess) e = cudaMalloc(&c->dFB, n * 8);
     if (e == cudaSuccess && c->wrap) e = cudaMalloc(&c->dWS, c->wm.per * 8);
@@ -103,6 +110,16 @@ int gf2e_trin_buffers(gf2e_trin *c, uint64_t **dA, uint64_t **dACC, uint64_t **d
     return GF2E_OK;
 }
 
+int gf2e_trin_scratch(gf2e_trin *c, uint64_t **dT1, uint64_t **dFA, uint64_t **dFB,
+                      int *m_full) {
+    if (!c) return gf2e::invalid("null context");
+    if (dT1) *dT1 = c->dT1;
+    if (dFA) *dFA = c->dFA;
+    if (dFB) *dFB = c->dFB;
+    if (m_full) *m_full = c->m_full;
+    return GF2E_OK;
+}
+
 int gf2e_trin_reset_A(gf2e_trin *c, void *stream) {
     if (!c) return gf2e::invalid("null context");
     return gf2e::trin_set_const(c->dA, c->nw, 1, c->r, 2, (cudaStream_t)stream);
@@ -119,6 +136,12 @@ int gf2e_trin_square_A(gf2e_trin *c, void *stream) {
     GF2E_TRY(gf2e::trin_square(c->dA, c->dT1, c->r, c->s, st));
     cudaError_t e = cudaMemcpyAsync(c->dA, c->dT1, c->nw * 8, cudaMemcpyDeviceToDevice, st);
     return gf2e::cuda_status(e, "square_A copy");
+}
+
+int gf2e_trin_square_A_k(gf2e_trin *c, uint64_t k, void *stream) {
+    if (!c || !c->s) return gf2e::invalid("context without s");
+    return gf2e::frobenius_states(c->dA, c->dT1, c->nw + (c->nw & 1), 1, c->r, nullptr, k,
+                                  (cudaStream_t)stream, c->s);
 }
 
 int gf2e_trin_mul_dev(gf2e_trin *c, const uint64_t *x, const uint64_t *y, void *stream) {

@@ -333,6 +333,8 @@ int launch_square(const u64 *in, u64 *out, size_t stride, int nstates, u64 r,
 }  // namespace
 
 namespace gf2e {
+int frobenius_states(u64 *a, u64 *b, size_t stride, int nstates, u64 r, const u64 *s_dev,
+                     u64 k, cudaStream_t st, u64 s_uniform = 0);
 int trin_reduce(const u64 *P, size_t pw, u64 L, u64 *out, u64 r, u64 s, cudaStream_t st) {
     const size_t nw = (size_t)((r + 63) >> 6);
     int threads = 256;
@@ -351,6 +353,10 @@ int trin_reduce_batch(const u64 *P, size_t pstride, size_t pw, u64 L, u64 *out, 
 int trin_square_states(const u64 *in, u64 *out, size_t stride, int nstates, u64 r,
                        const u64 *s_dev, cudaStream_t st) {
     return launch_square(in, out, stride, nstates, r, s_dev, 0, st);
+}
+int trin_square_any(const u64 *in, u64 *out, size_t stride, int nstates, u64 r,
+                    const u64 *s_dev, u64 s, cudaStream_t st) {
+    return launch_square(in, out, stride, nstates, r, s_dev, s, st);
 }
 int trin_square(const u64 *in, u64 *out, u64 r, u64 s, cudaStream_t st) {
     return launch_square(in, out, (size_t)((r + 63) >> 6), 1, r, nullptr, s, st);
@@ -384,18 +390,8 @@ int gf2e_trin_square_batch(uint64_t *states_dev, uint64_t *scratch_dev, size_t s
         return gf2e::invalid("gf2e_trin_square_batch: bad buffers or nstates=%d", nstates);
     if (stride_words < nw || (stride_words & 1))
         return gf2e::invalid("stride_words must be even and >= ceil(r/64)");
-    cudaStream_t st = (cudaStream_t)stream;
-    u64 *a = states_dev, *b = scratch_dev;
-    for (uint32_t i = 0; i < k; i++) {
-        GF2E_TRY(launch_square(a, b, stride_words, nstates, r, s_dev, 0, st));
-        u64 *t = a; a = b; b = t;
-    }
-    if (a != states_dev) {
-        cudaError_t e = cudaMemcpyAsync(states_dev, a, (size_t)nstates * stride_words * 8,
-                                        cudaMemcpyDeviceToDevice, st);
-        if (e != cudaSuccess) return gf2e::cuda_status(e, "square_batch copy-back");
-    }
-    return GF2E_OK;
+    return gf2e::frobenius_states(states_dev, scratch_dev, stride_words, nstates, r, s_dev, k,
+                                  (cudaStream_t)stream);
 }
 
 int gf2e_trin_set_x(uint64_t *states_dev, size_t stride_words, int nstates, uint64_t r,

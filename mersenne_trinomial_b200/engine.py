@@ -435,6 +435,12 @@ def trin_square_batch(states, scratch, stride_words: int, nstates: int, r: int, 
          _ptr(s_dev), k, _sp(stream))
 
 
+def squarings_per_pass(r: int, stride_words: int) -> int:
+    """Squarings one pass of trin_square_batch performs (2 where the fused
+    F -> F^4 pass applies, else 1)."""
+    return int(lib().gf2e_trin_squarings_per_pass(r, stride_words))
+
+
 def frobenius_host(r: int, s_values, k: int, out: Optional[np.ndarray] = None,
                    stream=None) -> np.ndarray:
     """F_k = x^(2^k) mod x^r + x^s + 1 for every s, host in / host out

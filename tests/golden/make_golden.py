@@ -26,7 +26,7 @@ ROOT = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, ROOT)
 
 from oracle import oracle as O  # noqa: E402
-from mersenne_trinomial_b200 import workloads as W  # noqa: E402
+from mersenne_trinomial_b200 import multi, workloads as W  # noqa: E402
 
 REF = O.REF_DIR
 
@@ -93,6 +93,14 @@ def gen_square():
     cfg = W.squaring_config(1)
     for s in [int(x) for x in cfg["s"][:4]]:
         add(cfg["r"], s, 4096, False)
+    # the benchmark's workload: F_256 at r = 136279841 for the first two s of
+    # the default bench's seeded s values (state 0 is checked by bench.py),
+    # and short runs at word-boundary s
+    R = 136279841
+    for s in [int(x) for x in multi.rank_s_values(R, 64, 0)[:2]]:
+        add(R, s, 256, False)
+    for s in (1, 63, 64, 65, 474, (R - 1) // 2):
+        add(R, s, 3, False)
     # interval product ACC = prod_{k=5..12} (F_k + x) (trinomial_stage2.cu:123-146)
     _, acc = stage2(4423, 1200, 5, 12)
     prods = [{"r": 4423, "s": 1200, "k0": 5, "k1": 12, "words": [format(int(x), "x") for x in acc]}]
@@ -102,6 +110,43 @@ def gen_square():
     sel = run([os.path.join(REF, "trinomial_stage2_emul"), "selftest"]).stdout
     with open(os.path.join(HERE, "square.json"), "w") as f:
         json.dump({"cases": cases, "products": prods, "ref_selftest": sel.splitlines()}, f, indent=1)
+
+
+def gen_stage2_cli():
+    """The reference's trinomial_stage2 run mode (under its CPU emulation):
+    output files and the state file of a run stopped at k = 1030 and resumed
+    to k = 2100, and of the same run without a state file
+    (trinomial_stage2.cu:195-277)."""
+    exe = os.path.join(REF, "trinomial_stage2_emul")
+    out = {"runs": []}
+
+    def files(pre, state=None):
+        d = {}
+        for ext in (".fk", ".acc", ".meta"):
+            with open(pre + ext, "rb") as f:
+                d[ext] = sha(f.read())
+        if state:
+            with open(state, "rb") as f:
+                d["state"] = sha(f.read())
+        return d
+    with tempfile.TemporaryDirectory() as td:
+        st = os.path.join(td, "state.bin")
+        for name, args, use_state in [("stop", ["4423", "1200", "1000", "1030"], True),
+                                      ("resume", ["4423", "1200", "1000", "2100"], True),
+                                      ("straight", ["4423", "1200", "1000", "2100"], False)]:
+            pre = os.path.join(td, name)
+            run([exe, "run"] + args + [pre] + ([st] if use_state else []))
+            out["runs"].append({"name": name, "args": args, "state": use_state,
+                                "sha256": files(pre, st if use_state else None)})
+        cfg = W.squaring_config(1)
+        args = [str(cfg["r"]), str(int(cfg["s"][0])), "100", "103"]
+        pre = os.path.join(td, "cfg2")
+        run([exe, "run"] + args + [pre])
+        out["runs"].append({"name": "config2", "args": args, "state": False,
+                            "sha256": files(pre)})
+    out["ref_selftest"] = run([exe, "selftest"]).stdout.splitlines()
+    with open(os.path.join(HERE, "stage2_cli.json"), "w") as f:
+        json.dump(out, f, indent=1)
 
 
 def gen_fft():
@@ -191,5 +236,6 @@ if __name__ == "__main__":
     gen_square()
     gen_fft()
     gen_scan()
+    gen_stage2_cli()
     gen_verify()
     print("golden fixtures written to", HERE)

@@ -64,11 +64,12 @@ def test_sieve_rejects_bad_r(oracle):
 # ----------------------------------------------------------------- squaring
 def test_square_fixtures(oracle):
     for c in load_json("square.json")["cases"]:
-        if c["k"] == 4096:
+        if c["k"] >= 256:
             continue
         got = oracle.trin_square_k(oracle.x_state(c["r"]), c["r"], c["s"], c["k"])
         assert sha(got.tobytes()) == c["sha256"], c
-        assert (got == words_of(c["words"])).all()
+        if "words" in c:
+            assert (got == words_of(c["words"])).all()
 
 
 @pytest.mark.slow
@@ -78,6 +79,17 @@ def test_square_config2_fixtures(oracle):
             continue
         got = oracle.trin_square_k(oracle.x_state(c["r"]), c["r"], c["s"], c["k"])
         assert sha(got.tobytes()) == c["sha256"]
+
+
+@pytest.mark.slow
+def test_square_benchmark_workload_fixtures(oracle):
+    """F_256 at r = 136279841 for the benchmark's first two s values, as the
+    reference's kernels computed it (about 30 s of oracle time each)."""
+    cases = [c for c in load_json("square.json")["cases"] if c["k"] == 256]
+    assert len(cases) == 2
+    for c in cases:
+        got = oracle.trin_square_k(oracle.x_state(c["r"]), c["r"], c["s"], c["k"])
+        assert sha(got.tobytes()) == c["sha256"], c["s"]
 
 
 def test_frobenius_kat(oracle):
