@@ -591,17 +591,23 @@ def serving_sample(n_jobs=24, rate=16.0, seed=1):
     batching from the same jobs queued at once, against the plain path (each
     job alone on the GPU, back to back); every job's lines compared."""
     from mersenne_trinomial_b200 import serve
-    jobs = serve.job_stream(seed, n_jobs, rate, deep_max=600, s_lo=16, s_hi=128)
-    lat, wall, lines = serve.run_stream(jobs, slots=64)
-    _, sat_wall, sat_lines = serve.run_stream(jobs, slots=64, realtime=False)
-    plain_wall, plain_lines = serve.run_one_at_a_time(jobs, slots=64)
+    # deep jobs at r = 136279841 (each s at least one 25 s half-gcd, 4 s when
+    # 8-16 run at once) are measured by profile case serve_deep, not here
+    jobs = serve.job_stream(seed, n_jobs, rate, deep_max=600, s_lo=16, s_hi=4096,
+                            deep_s_cap={"1e7": 8}, deep_classes=("1e5", "1e6", "1e7"))
+    lat, wall, lines, _ = serve.run_stream(jobs, slots=64)
+    _, sat_wall, sat_lines, pairs = serve.run_stream(jobs, slots=64, realtime=False)
+    plain_wall, plain_lines, plain_pairs = serve.run_one_at_a_time(jobs, slots=64)
     v = sorted(lat.values())
-    pairs = serve.pairs_of(jobs)
     same = all(lines[k] == plain_lines[k] == sat_lines[k] for k in lines)
     return {"jobs": n_jobs, "rate_per_s": rate, "p50_s": float(np.percentile(v, 50)),
             "p99_s": float(np.percentile(v, 99)), "realtime_wall_s": wall,
-            "sd_pairs_per_s_batched": pairs / sat_wall,
-            "sd_pairs_per_s_plain_one_at_a_time": pairs / plain_wall,
+            "r_classes": sorted({int(j["r"]) for j in jobs}),
+            "deep_jobs": sum(1 for j in jobs if j["dmax"] > 24),
+            "s_per_job_max": max(int(j["s"].size) for j in jobs),
+            "sieved_scanned_pairs": list(pairs),
+            "sd_pairs_per_s_batched": sum(pairs) / sat_wall,
+            "sd_pairs_per_s_plain_one_at_a_time": sum(plain_pairs) / plain_wall,
             "batched_over_plain": plain_wall / sat_wall,
             "results_identical_alone_vs_mixed": same}
 

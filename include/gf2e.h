@@ -361,6 +361,9 @@ int gf2e_scanner_poll(gf2e_scanner *scanner, gf2e_scan_result *results_host,
  * (trinomial_scan.cu:144-170, 262-275). */
 int gf2e_scanner_frontiers(const gf2e_scanner *scanner, uint64_t *s_host, uint64_t *k_host,
                            uint64_t *tags_host, int cap, int *nout);
+/* Interval gcds the scanner has run and the host wall time spent in them
+ * (the gcd calls return when their results are known). */
+int gf2e_scanner_gcd_time(const gf2e_scanner *scanner, uint64_t *gcds, double *seconds);
 
 /* ======================================================================
  * (f) Serving: continuous batching of (r, s-set, d-range) search jobs.  No
@@ -382,6 +385,11 @@ int gf2e_server_submit(gf2e_server *server, uint64_t job_id, uint64_t r, const u
 int gf2e_server_step(gf2e_server *server, int degrees, void *stream);
 int gf2e_server_status(const gf2e_server *server, int *waiting, int *active, int *finished,
                        size_t *used_bytes);
+/* (s, d) pairs the server has worked through so far: sieved (each admitted
+ * s times the degrees 2..min(dmax, 24) its sieve covered) and scanned (each
+ * resident s times the degrees its deep scan actually stepped, so an s that
+ * retired early counts only the degrees it ran). */
+int gf2e_server_pairs(const gf2e_server *server, uint64_t *sieved, uint64_t *scanned);
 int gf2e_server_poll(gf2e_server *server, uint64_t *job_ids_host, double *latency_s_host,
                      int cap, int *nout);
 int gf2e_server_job_lines(gf2e_server *server, uint64_t job_id, char *buf, size_t cap,

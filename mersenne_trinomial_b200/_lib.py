@@ -128,6 +128,7 @@ SIGNATURES = {
     "gf2e_server_step": (_i32, [_vp, _i32, _vp]),
     "gf2e_server_status": (_i32, [_vp, _P(_i32), _P(_i32), _P(_i32), _P(_sz)]),
     "gf2e_server_poll": (_i32, [_vp, _vp, _vp, _i32, _P(_i32)]),
+    "gf2e_server_pairs": (_i32, [_vp, _P(_u64), _P(_u64)]),
     "gf2e_server_job_lines": (_i32, [_vp, _u64, C.c_char_p, _sz, _P(_sz)]),
     "gf2e_server_release": (_i32, [_vp, _u64]),
     "gf2e_scanner_footprint": (_i32, [_u64, _i32, _P(_sz)]),
@@ -146,6 +147,7 @@ SIGNATURES = {
     "gf2e_scanner_status": (_i32, [_vp, _P(_i32), _P(_i32), _P(_i32), _P(_u64)]),
     "gf2e_scanner_poll": (_i32, [_vp, _P(ScanResult), _vp, _vp, _sz, _i32, _P(_i32)]),
     "gf2e_scanner_frontiers": (_i32, [_vp, _vp, _vp, _vp, _i32, _P(_i32)]),
+    "gf2e_scanner_gcd_time": (_i32, [_vp, _P(_u64), _P(C.c_double)]),
     "gf2e_trin_create": (_i32, [_u64, _P(_vp)]),
     "gf2e_trin_destroy": (_i32, [_vp]),
     "gf2e_trin_set_s": (_i32, [_vp, _u64]),

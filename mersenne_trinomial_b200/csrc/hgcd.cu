@@ -506,13 +506,66 @@ struct Pool {
     cudaMemPool_t pool = nullptr;
 };
 
-// device buffer from the stream-ordered pool, freed on the same stream
+// Sub-allocator for one gcd's device buffers.  Every buffer of a gcd is used
+// on that gcd's stream only, so a block given back can go to the next
+// request at once: stream order keeps the kernels that used it ahead of the
+// next user, as cudaFreeAsync would, without an allocator call per buffer
+// (a half-gcd at r = 136279841 makes several hundred thousand buffers, and
+// concurrent gcds would otherwise queue on those calls).  Blocks are powers
+// of two words, carved from chunks taken from the stream-ordered pool and
+// kept on per-size free lists; the chunks go back to the pool at the end.
+class Arena {
+public:
+    Arena(cudaStream_t st, cudaMemPool_t pool) : st_(st), pool_(pool) {}
+    ~Arena() {
+        for (u64 *c : chunks_) cudaFreeAsync(c, st_);
+    }
+    Arena(const Arena &) = delete;
+    Arena &operator=(const Arena &) = delete;
+
+    u64 *get(size_t words, int &cls) {
+        cls = 6;                                   // at least 64 words
+        while (((size_t)1 << cls) < words) cls++;
+        if (!free_[cls].empty()) {
+            u64 *p = free_[cls].back();
+            free_[cls].pop_back();
+            return p;
+        }
+        const size_t need = (size_t)1 << cls;
+        if (left_ < need) {
+            const size_t chunk = std::max(need, (size_t)1 << 22);    // 32 MB or the block
+            void *c = nullptr;
+            ckc_arena(cudaMallocFromPoolAsync(&c, chunk * 8, pool_, st_));
+            chunks_.push_back((u64 *)c);
+            cur_ = (u64 *)c;
+            left_ = chunk;
+        }
+        u64 *p = cur_;
+        cur_ += need;
+        left_ -= need;
+        return p;
+    }
+    void put(u64 *p, int cls) { free_[cls].push_back(p); }
+
+private:
+    static void ckc_arena(cudaError_t e) { ckc(e, "hgcd pool allocation"); }
+    cudaStream_t st_;
+    cudaMemPool_t pool_;
+    std::vector<u64 *> chunks_;
+    std::vector<u64 *> free_[64];
+    u64 *cur_ = nullptr;
+    size_t left_ = 0;
+};
+
+// device buffer from the gcd's arena, given back when the last owner drops it
 struct DBuf {
     u64 *p = nullptr;
     size_t words = 0;
     cudaStream_t st = nullptr;
-    ~DBuf() {
-        if (p) cudaFreeAsync(p, st);
+    Arena *arena = nullptr;
+    int cls = 0;
+    virtual ~DBuf() {
+        if (p && arena) arena->put(p, cls);
     }
 };
 typedef std::shared_ptr<DBuf> Buf;
@@ -567,7 +620,8 @@ struct Timer {
 
 class Hgcd {
 public:
-    Hgcd(cudaStream_t st, cudaMemPool_t pool) : st_(st), pool_(pool), tn_(tunables()) {
+    Hgcd(cudaStream_t st, cudaMemPool_t pool)
+        : arena_(st, pool), st_(st), pool_(pool), tn_(tunables()) {
         ckc(cudaMallocHost(&h_probe_, 16 * sizeof(long long)), "hgcd probe host buffer");
         d_probe_ = alloc(16);
         d_res_ = alloc(8);
@@ -596,9 +650,8 @@ public:
         auto b = std::make_shared<DBuf>();
         b->st = st_;
         b->words = std::max<size_t>(words, 1);
-        void *p = nullptr;
-        ckc(cudaMallocFromPoolAsync(&p, b->words * 8, pool_, st_), "hgcd pool allocation");
-        b->p = (u64 *)p;
+        b->p = arena_.get(b->words, b->cls);
+        b->arena = &arena_;
         return b;
     }
     Poly zeros(size_t words) {
@@ -1024,6 +1077,7 @@ public:
     }
 
 private:
+    Arena arena_;                      // declared first: destroyed after every buffer
     cudaStream_t st_;
     cudaMemPool_t pool_;
     Tunables tn_;

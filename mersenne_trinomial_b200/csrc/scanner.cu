@@ -31,6 +31,7 @@
 #include "wrapmul.cuh"
 
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <deque>
 #include <vector>
@@ -77,6 +78,8 @@ struct gf2e_scanner {
     std::vector<int64_t> degs;
     std::vector<gf2e_gcd_job> jobs;
     u64 degree_steps = 0, sd_pairs = 0;
+    u64 gcds = 0;                 // interval gcds run, and their host wall time
+    double gcd_seconds = 0;
     // the per-degree launches (squaring, transforms, products, folds) are
     // replayed from CUDA graphs, one per (resident count, F buffer)
     cudaStream_t own = nullptr;
@@ -465,6 +468,7 @@ int degree_step(gf2e_scanner &S, cudaStream_t st) {
         S.jobs[q] = gf2e_gcd_job{S.ACC + S.stride * j, S.r, S.T + S.tw * j, S.r + 1,
                                  S.G + S.gcap * q, S.gcap};
     }
+    const auto t_gcd = std::chrono::steady_clock::now();
     if (S.r >= GCD_LARGE_BITS) {
         const int par = std::max(1, std::min((int)due.size(), S.gcd_parallel));
         GF2E_TRY(gf2e_gcd_large(S.jobs.data(), (int)due.size(), S.degs.data(), par, nullptr, st));
@@ -472,6 +476,9 @@ int degree_step(gf2e_scanner &S, cudaStream_t st) {
         GF2E_TRY(gf2e_gcd_batch(S.jobs.data(), (int)due.size(), S.degs.data(), S.gws,
                                 S.gws_bytes, st));
     }
+    S.gcds += due.size();
+    S.gcd_seconds +=
+        std::chrono::duration<double>(std::chrono::steady_clock::now() - t_gcd).count();
     std::vector<int> retire;
     for (size_t q = 0; q < due.size(); q++) {
         int j = due[q];
@@ -694,6 +701,13 @@ int gf2e_scanner_status(const gf2e_scanner *S, int *queued, int *resident, int *
     if (resident) *resident = S->nact;
     if (finished) *finished = (int)S->done.size();
     if (sd_pairs) *sd_pairs = S->sd_pairs;
+    return GF2E_OK;
+}
+
+int gf2e_scanner_gcd_time(const gf2e_scanner *S, uint64_t *gcds, double *seconds) {
+    if (!S) return gf2e::invalid("null scanner");
+    if (gcds) *gcds = S->gcds;
+    if (seconds) *seconds = S->gcd_seconds;
     return GF2E_OK;
 }
 

@@ -83,6 +83,7 @@ struct gf2e_server {
     uint64_t *best = nullptr;
     size_t best_words = 0;
     uint64_t sd_pairs_sieve = 0;
+    uint64_t sd_pairs_scan_retired = 0;              // scanned pairs of destroyed scanners
     std::vector<gf2e_scan_result> res;
     std::vector<uint64_t> tags, masks;
 };
@@ -285,6 +286,9 @@ int gf2e_server_step(gf2e_server *S, int degrees, void *stream) {
                         int q = 0, a = 0;
                         gf2e_scanner_status(rc.sc, &q, &a, nullptr, nullptr);
                         if (q == 0 && a == 0) {
+                            uint64_t pairs = 0;
+                            gf2e_scanner_status(rc.sc, nullptr, nullptr, nullptr, &pairs);
+                            S->sd_pairs_scan_retired += pairs;
                             gf2e_scanner_destroy(rc.sc);
                             rc.sc = nullptr;
                             S->used -= rc.bytes;
@@ -308,6 +312,19 @@ int gf2e_server_status(const gf2e_server *S, int *waiting, int *active, int *fin
     if (active) *active = act;
     if (finished) *finished = (int)S->finished.size();
     if (used_bytes) *used_bytes = S->used;
+    return GF2E_OK;
+}
+
+int gf2e_server_pairs(const gf2e_server *S, uint64_t *sieved, uint64_t *scanned) {
+    if (!S) return gf2e::invalid("null server");
+    uint64_t sc = S->sd_pairs_scan_retired;
+    for (auto &kv : S->rclass) {
+        uint64_t p = 0;
+        if (kv.second.sc) gf2e_scanner_status(kv.second.sc, nullptr, nullptr, nullptr, &p);
+        sc += p;
+    }
+    if (sieved) *sieved = S->sd_pairs_sieve;
+    if (scanned) *scanned = sc;
     return GF2E_OK;
 }
 

@@ -403,6 +403,66 @@ def scan(r: int, survivors, k0: int, maxd: int, L0: int = 64, Lmax: int = 4096,
     return out
 
 
+class Scanner:
+    """The steppable deep-scan engine (gf2e_scanner_*): submit s values, step
+    degrees, poll finished result lines (the reference's line format)."""
+
+    def __init__(self, r: int, slots: int = 64, block: int = 1, mask_cap_words: int = 1024):
+        h = C.c_void_p()
+        call("gf2e_scanner_create_blocked", r, slots, block, C.byref(h))
+        self.h, self.cap = h.value, mask_cap_words
+
+    def submit(self, s_values, k0: int, maxd: int, L0: int = 64, Lmax: int = 4096, tag0: int = 0):
+        s = np.ascontiguousarray(np.asarray(s_values, dtype=np.uint64))
+        call("gf2e_scanner_submit", self.h, s.ctypes.data, s.size, k0, maxd, L0, Lmax, tag0)
+
+    def step(self, degrees: int = 256, stream=None):
+        call("gf2e_scanner_step", self.h, degrees, _sp(stream))
+
+    def poll(self, n: int = 64) -> list:
+        """[(s, line)] of the s values finished since the last poll."""
+        from ._lib import ScanResult
+        res = (ScanResult * n)()
+        tags = np.zeros(n, dtype=np.uint64)
+        masks = np.zeros((n, self.cap), dtype=np.uint64)
+        out, got = [], C.c_int()
+        while True:
+            call("gf2e_scanner_poll", self.h, res, tags.ctypes.data, masks.ctypes.data, self.cap,
+                 n, C.byref(got))
+            for i in range(got.value):
+                R = res[i]
+                if R.status == 1:
+                    line = f"{R.s} {R.d} p{_hex(masks[i, :R.mask_words])}"
+                elif R.status == 2:
+                    line = f"{R.s} u"
+                else:
+                    line = f"{R.s} r{R.rlo}-{R.rhi}"
+                out.append((int(R.s), line))
+            if got.value < n:
+                return out
+
+    def gcd_time(self):
+        g, t = C.c_uint64(), C.c_double()
+        call("gf2e_scanner_gcd_time", self.h, C.byref(g), C.byref(t))
+        return g.value, t.value
+
+    def pairs(self) -> int:
+        p = C.c_uint64()
+        call("gf2e_scanner_status", self.h, None, None, None, C.byref(p))
+        return p.value
+
+    def close(self):
+        if self.h:
+            lib().gf2e_scanner_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 def resolve_factor(g_words, kmin: int, kmax: int, cap: int = 1024):
     """(d, mask words) of the least-degree, then least, factor of g with
     degree in [kmin, kmax] (host computation on a small gcd)."""

@@ -10,6 +10,8 @@ capture (inputs larger than L2, a few GB at most, a handful of launches).
     python -m mersenne_trinomial_b200.profile_cases hgcd_many [--r R] [--n N]
     python -m mersenne_trinomial_b200.profile_cases scan [--r R --n N --k K]
     python -m mersenne_trinomial_b200.profile_cases scan_step [--r R --n N --block B]
+    python -m mersenne_trinomial_b200.profile_cases config4 [--n 128 --maxd 20000 --block B
+                                                             --l0 L0 --lmax LMAX --out PREFIX]
 """
 from __future__ import annotations
 
@@ -166,10 +168,48 @@ def case_sieve_wide(a):
     M.run_sieve(a.r, a.depth, smax, dmin=a.dmin)
 
 
+def case_config4(a):
+    """The batched deep scan at its stated shape: n seeded survivors of the
+    d <= 24 sieve at r (every s <= (r-1)/2), each scanned to its least
+    factor or maxd with the blocked DDF under the doubling interval schedule
+    (L0, Lmax); writes <out>.results.txt ("s d p<hex>" / "s u" lines) and
+    prints wall time, gcd count and gcd wall share (JSON)."""
+    import json
+    r, n = a.r, a.n
+    smax = (r - 1) // 2
+    t0 = time.perf_counter()
+    best = M.run_sieve(r, 24, smax)
+    t_sieve = time.perf_counter() - t0
+    surv = np.nonzero(best == np.uint64(0xFFFFFFFFFFFFFFFF))[0]
+    surv = surv[surv >= 3]
+    rng = np.random.default_rng(a.seed)
+    pick = np.sort(rng.choice(surv, size=min(n, surv.size), replace=False)).astype(np.uint64)
+    S = M.engine.Scanner(r, slots=min(64, pick.size), block=a.block)
+    S.submit(pick, k0=24, maxd=a.maxd, L0=a.l0, Lmax=a.lmax)
+    lines = {}
+    t1 = time.perf_counter()
+    while len(lines) < pick.size:
+        S.step(256)
+        for s_, line in S.poll():
+            lines[s_] = line
+    t_scan = time.perf_counter() - t1
+    gcds, t_gcd = S.gcd_time()
+    pairs = S.pairs()
+    S.close()
+    with open(a.out + ".results.txt", "w") as f:
+        f.write("".join(lines[s_] + "\n" for s_ in sorted(lines)))
+    found = sum(1 for l in lines.values() if " p" in l)
+    print(json.dumps({"r": r, "survivors": int(pick.size), "maxd": a.maxd, "block": a.block,
+                      "L0": a.l0, "Lmax": a.lmax, "sieve_s": t_sieve, "scan_wall_s": t_scan,
+                      "gcds": gcds, "gcd_wall_s": t_gcd, "gcd_share": t_gcd / t_scan,
+                      "sd_pairs": pairs, "found": found, "u": int(pick.size) - found,
+                      "results": a.out + ".results.txt"}))
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("case", choices=["square", "fft", "mul", "sieve", "sieve_wide", "gcd", "hgcd",
-                                     "hgcd_many", "scan", "scan_step"])
+                                     "hgcd_many", "scan", "scan_step", "config4"])
     ap.add_argument("--r", type=int, default=136279841)
     ap.add_argument("--n", type=int, default=8)
     ap.add_argument("--k", type=int, default=3)
@@ -178,11 +218,17 @@ def main(argv=None):
     ap.add_argument("--dmin", type=int, default=2)
     ap.add_argument("--wide-from", type=int, default=32)
     ap.add_argument("--block", type=int, default=28)
+    ap.add_argument("--maxd", type=int, default=20000)
+    ap.add_argument("--l0", type=int, default=1024)
+    ap.add_argument("--lmax", type=int, default=8192)
+    ap.add_argument("--seed", type=int, default=4)
+    ap.add_argument("--out", default="config4")
     a = ap.parse_args(argv)
     t0 = time.perf_counter()
     {"square": case_square, "fft": case_fft, "mul": case_mul, "sieve": case_sieve,
      "sieve_wide": case_sieve_wide, "gcd": case_gcd, "hgcd": case_hgcd,
-     "hgcd_many": case_hgcd_many, "scan": case_scan, "scan_step": case_scan_step}[a.case](a)
+     "hgcd_many": case_hgcd_many, "scan": case_scan, "scan_step": case_scan_step,
+     "config4": case_config4}[a.case](a)
     print(f"{a.case}: done in {time.perf_counter() - t0:.3f} s")
     return 0
 

@@ -43,6 +43,12 @@ class Server:
         call("gf2e_server_status", self.h, C.byref(w), C.byref(a), C.byref(f), C.byref(used))
         return {"waiting": w.value, "active": a.value, "finished": f.value, "used": used.value}
 
+    def pairs(self):
+        """(sieved, scanned) (s, d) pairs actually worked through so far."""
+        a, b = C.c_uint64(), C.c_uint64()
+        call("gf2e_server_pairs", self.h, C.byref(a), C.byref(b))
+        return a.value, b.value
+
     def poll(self, cap: int = 1024):
         ids = np.zeros(cap, dtype=np.uint64)
         lat = np.zeros(cap, dtype=np.float64)
@@ -76,13 +82,23 @@ R_CLASSES = {"1e5": 100_000, "1e6": 1_000_000, "1e7": 10_000_000}
 BAD_R = {127, 151, 241, 257, 337, 8191, 131071, 178481, 524287}
 
 
+# largest s-set of a deep (squaring + gcd) job per r class: every deep s costs
+# at least one interval gcd of r-bit operands (about 0.1 s at r ~ 1e6, 1 s at
+# r ~ 1e7 and 4 s at r = 136279841 with 8-16 of them running at once)
+DEEP_S_CAP = {"1e5": 256, "1e6": 256, "1e7": 32, "deep": 4}
+
+
 def job_stream(seed: int, n_jobs: int, rate: float, deep_max: int = 2000,
-               s_lo: int = 16, s_hi: int = 256):
+               s_lo: int = 16, s_hi: int = 4096, deep_frac: float = 0.6,
+               deep_s_cap=None, deep_classes=("1e5", "1e6", "1e7", "deep")):
     """Seeded Poisson arrivals.  r from the set {~1e5, ~1e6, ~1e7, 136279841}
     (one seeded prime = +-1 mod 8 that the sieve supports near each of the
-    first three); s-sets of s_lo..s_hi values; d-range 2..24 (sieve only) or,
-    for r ~1e5 / ~1e6, up to 2..deep_max (squaring + gcd).  Jobs with the same
-    r share that r's resident scanner."""
+    first three); s-sets of s_lo..s_hi values (log-uniform); d-range 2..24
+    (sieve only) or, for a fraction deep_frac of the jobs of every r, up to
+    2..deep_max (squaring + gcd), their s-sets capped per r class
+    (DEEP_S_CAP); deep_classes limits which r classes get deep jobs.  Jobs
+    with the same r share that r's resident scanner."""
+    caps = dict(DEEP_S_CAP, **(deep_s_cap or {}))
     rng = np.random.default_rng(seed)
     rset = {}
     for name, near in R_CLASSES.items():
@@ -93,20 +109,22 @@ def job_stream(seed: int, n_jobs: int, rate: float, deep_max: int = 2000,
     jobs = []
     for i in range(n_jobs):
         t += rng.exponential(1.0 / rate)
-        cls = rng.choice(["1e5", "1e6", "1e7", "deep"])
+        cls = str(rng.choice(["1e5", "1e6", "1e7", "deep"]))
         r = W.R_DEEP if cls == "deep" else rset[cls]
-        ns = int(rng.integers(s_lo, s_hi + 1))
+        deep = rng.random() < deep_frac and cls in deep_classes
+        hi = min(s_hi, caps[cls]) if deep else s_hi
+        lo = min(s_lo, hi)
+        ns = int(round(np.exp(rng.uniform(np.log(lo), np.log(hi)))))
         s = np.unique(rng.integers(3, r // 2, size=ns)).astype(np.uint64)
-        deep_ok = r < 2_000_000
-        dmax = int(rng.integers(25, deep_max + 1)) if (deep_ok and rng.random() < 0.6) else \
-            int(rng.integers(2, 25))
+        dmax = int(rng.integers(25, deep_max + 1)) if deep else int(rng.integers(2, 25))
         jobs.append({"id": i + 1, "t": t, "r": r, "s": s, "dmax": dmax})
     return jobs
 
 
 def run_stream(jobs, slots: int = 64, budget: int = 64 << 30, degrees: int = 16,
                realtime: bool = True, block: int = 1):
-    """Serve `jobs` (arrival times in seconds); returns (latencies, wall, lines)."""
+    """Serve `jobs` (arrival times in seconds); returns (latencies, wall,
+    lines, pairs) with pairs the (sieved, scanned) (s, d) pairs worked."""
     srv = Server(budget, slots, block)
     t0 = time.perf_counter()
     pending = sorted(jobs, key=lambda j: j["t"])
@@ -129,28 +147,31 @@ def run_stream(jobs, slots: int = 64, budget: int = 64 << 30, degrees: int = 16,
                 not srv.status()["waiting"]:
             time.sleep(max(0.0, min(0.01, pending[i]["t"] - (time.perf_counter() - t0))))
     wall = time.perf_counter() - t0
+    pairs = srv.pairs()
     srv.close()
-    return lat, wall, lines
+    return lat, wall, lines, pairs
 
 
-def run_one_at_a_time(jobs, slots: int = 64, degrees: int = 256, block: int = 1):
-    """The plain path: each job alone on a fresh server, back to back."""
+def run_one_at_a_time(jobs, slots: int = 64, degrees: int = 16, block: int = 1,
+                      budget: int = 64 << 30):
+    """The plain path: the jobs one after another on one server (each alone
+    on the GPU, nothing overlapping), same step size as the stream; returns
+    (wall, lines, pairs)."""
+    srv = Server(budget, slots, block)
     t0 = time.perf_counter()
     lines = {}
     for j in jobs:
-        srv = Server(64 << 30, slots, block)
         srv.submit(j["id"], j["r"], j["s"], j["dmax"])
         done = []
         while not done:
             srv.step(degrees)
             done = srv.poll()
         lines[j["id"]] = srv.lines(j["id"])
-        srv.close()
-    return time.perf_counter() - t0, lines
-
-
-def pairs_of(jobs):
-    return sum(int(j["s"].size) * (int(j["dmax"]) - 1) for j in jobs)
+        srv.release(j["id"])
+    wall = time.perf_counter() - t0
+    pairs = srv.pairs()
+    srv.close()
+    return wall, lines, pairs
 
 
 def main(argv=None):
@@ -162,14 +183,15 @@ def main(argv=None):
     ap.add_argument("--block", type=int, default=1, help="blocked-DDF degrees per step")
     a = ap.parse_args(argv)
     jobs = job_stream(a.seed, a.jobs, a.rate, a.deep_max)
-    lat, wall, lines = run_stream(jobs, block=a.block)
-    plain_wall, plain_lines = run_one_at_a_time(jobs, block=a.block)
+    lat, wall, lines, pairs = run_stream(jobs, block=a.block)
+    plain_wall, plain_lines, plain_pairs = run_one_at_a_time(jobs, block=a.block)
     v = sorted(lat.values())
     same = all(lines[k] == plain_lines[k] for k in lines)
     out = {"jobs": len(jobs), "p50_s": float(np.percentile(v, 50)),
            "p99_s": float(np.percentile(v, 99)), "wall_s": wall,
-           "sd_pairs_per_s": pairs_of(jobs) / wall, "plain_wall_s": plain_wall,
-           "plain_sd_pairs_per_s": pairs_of(jobs) / plain_wall, "results_identical": same}
+           "sd_pairs_per_s": sum(pairs) / wall, "sieved_scanned_pairs": pairs,
+           "plain_wall_s": plain_wall, "plain_sd_pairs_per_s": sum(plain_pairs) / plain_wall,
+           "results_identical": same}
     print(json.dumps(out))
     return 0 if same else 1
 

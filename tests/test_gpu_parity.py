@@ -89,7 +89,7 @@ def _square_k(engine, st, r, s, k):
 
 def test_square_fixtures_single(engine, oracle):
     for c in load_json("square.json")["cases"]:
-        if c["k"] == 4096:
+        if "words" not in c:          # hash-only cases: test_gpu_frobenius.py
             continue
         got = _square_k(engine, oracle.x_state(c["r"]), c["r"], c["s"], c["k"])
         assert (got == words_of(c["words"])).all(), c

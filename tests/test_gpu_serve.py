@@ -21,10 +21,15 @@ def test_scanner_scan_matches_reference(engine):
 
 def test_job_alone_equals_job_in_mix(engine, oracle):
     from mersenne_trinomial_b200 import serve
-    jobs = serve.job_stream(seed=5, n_jobs=8, rate=1000.0, deep_max=300, s_lo=8, s_hi=24)
+    jobs = serve.job_stream(seed=5, n_jobs=8, rate=1000.0, deep_max=300, s_lo=8, s_hi=24,
+                            deep_classes=("1e5", "1e6"))
     # the mix: everything submitted at once, stepped together
-    lat, wall, mixed = serve.run_stream(jobs, slots=16, realtime=False)
-    alone_wall, alone = serve.run_one_at_a_time(jobs, slots=16)
+    lat, wall, mixed, pairs = serve.run_stream(jobs, slots=16, realtime=False)
+    alone_wall, alone, alone_pairs = serve.run_one_at_a_time(jobs, slots=16)
+    # pairs actually worked: the same sieve either way, and scanned pairs no
+    # more than every deep s over its whole range
+    assert pairs[0] == alone_pairs[0] > 0
+    assert 0 < pairs[1] <= sum(int(j["s"].size) * int(j["dmax"]) for j in jobs if j["dmax"] > 24)
     assert set(mixed) == {j["id"] for j in jobs}
     for j in jobs:
         assert mixed[j["id"]] == alone[j["id"]], j["id"]
@@ -63,7 +68,27 @@ def test_blocked_server_matches_per_degree_server(engine):
     """Scanners in blocked-DDF mode give every job the same lines as the
     per-degree scanners."""
     from mersenne_trinomial_b200 import serve
-    jobs = serve.job_stream(seed=7, n_jobs=6, rate=1000.0, deep_max=300, s_lo=8, s_hi=24)
-    _, _, plain = serve.run_stream(jobs, slots=16, realtime=False)
-    _, _, blocked = serve.run_stream(jobs, slots=16, realtime=False, block=8)
+    jobs = serve.job_stream(seed=7, n_jobs=6, rate=1000.0, deep_max=300, s_lo=8, s_hi=24,
+                            deep_classes=("1e5", "1e6"))
+    _, _, plain, _ = serve.run_stream(jobs, slots=16, realtime=False)
+    _, _, blocked, _ = serve.run_stream(jobs, slots=16, realtime=False, block=8)
     assert plain == blocked
+
+
+def test_deep_jobs_at_large_r_in_the_mix(engine, oracle):
+    """Deep (squaring + gcd) jobs at r ~ 1e7 and r = 136279841 beside small
+    ones, s-sets up to a few thousand for sieve-only jobs: each job's lines
+    equal the job alone, and every factor divides its trinomial."""
+    from mersenne_trinomial_b200 import serve
+    jobs = serve.job_stream(seed=11, n_jobs=8, rate=1000.0, deep_max=60, s_lo=16, s_hi=4096,
+                            deep_s_cap={"1e7": 4, "deep": 2})
+    assert any(j["r"] == 136279841 and j["dmax"] > 24 for j in jobs)
+    assert any(j["r"] > 5_000_000 and j["r"] != 136279841 and j["dmax"] > 24 for j in jobs)
+    _, _, mixed, pairs = serve.run_stream(jobs, slots=16, realtime=False)
+    _, alone, _ = serve.run_one_at_a_time(jobs, slots=16)
+    for j in jobs:
+        assert mixed[j["id"]] == alone[j["id"]], j["id"]
+        for ln in mixed[j["id"]]:
+            p = ln.split()
+            if len(p) == 3 and p[2].startswith("p"):
+                assert oracle.factor_divides(j["r"], int(p[0]), int(p[1]), p[2][1:]) == 1, ln
