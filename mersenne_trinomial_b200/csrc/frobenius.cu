@@ -30,32 +30,34 @@
 // window, XORed into the class accumulator C[c].  The unit's output is the
 // 4-way bit interleave of C[0..3] (bit 4 t + c = bit t of C[c]): cross-
 // register delta swaps, a byte transpose by byte permutes, then two delta
-// swaps inside each 32 bits.
-// Lanes own consecutive units (coalesced 16-byte stores).
+// swaps inside each 32 bits.  Lanes own units u0 + lane + 32 q, q < 8, so
+// loads and 16-byte stores are coalesced.
 //
-// Memory: a warp tile of 128 units needs, per window overlapping it, one
-// contiguous run of 129 input words.  The warp first issues asynchronous
-// 16-byte copies (cp.async, zero-filled past the state's ends) of every
-// such run into its shared-memory slots, so all of the tile's windows are
-// in flight together, then waits once and computes from shared memory.
-// (Reading each window straight from global memory serialises one memory
-// latency per window: measured 3x slower.)  Windows that cover the whole
-// tile are applied unmasked; the few that start or end inside it apply a
-// per-lane mask of their output bits.
+// Per warp tile of 256 units, one ballot lists the windows overlapping it and
+// those covering all of it.  The covering windows whose reads stay inside the
+// state are applied two at a time (both windows' 32 loads issued before
+// either is used) with no masks or bounds tests; the rest (windows that start
+// or end inside the tile, a few tiles per state) with per-lane bit masks and
+// bounds-tested loads.  The kernel is bound by memory latency and integer
+// issue together: measured at r = 136279841, windows one at a time with the
+// high words by shuffle ran 1.06 ms a pass (64 states), the per-tile list
+// with two loads a unit 0.72 ms, two windows at a time 0.68 ms; staging each
+// window's run in shared memory by cp.async first ran 1.5 ms (more issued
+// instructions, fewer resident warps).  Each CTA composes its state's
+// windows in warp 0 with shifts and masks (the moduli are powers of two).
 #include "gf2e_internal.cuh"
 
 #include <algorithm>
 #include <atomic>
 #include <cstdlib>
+#include <cstring>
 
 namespace {
 
 constexpr int KL = 2;                 // squarings per pass
 constexpr int M = 1 << KL;            // residue classes of output bits
 constexpr int NCAND = 25;             // 5^KL composed candidates
-constexpr int UPT = 4;                // units (2 words each) per lane per tile
-constexpr u32 UBITS = 32 * M;         // output bits per unit
-constexpr u32 TWU = 32 * UPT;         // units per warp tile
+constexpr u32 UBITS = 32 * M;         // output bits per unit (two words)
 
 struct FWin {
     int lo, hi;       // output bits j in [lo, hi), lo = hi - 1 = c (mod M)
@@ -67,10 +69,9 @@ struct Win64 {
     int64_t m, c, lo, hi, K;
 };
 
-GF2E_DEV int64_t mod_pos(int64_t a, int64_t m) {
-    int64_t v = a % m;
-    return v < 0 ? v + m : v;
-}
+// a mod m in [0, m) for m a power of two (two's complement: the low bits)
+GF2E_DEV int64_t mod_pos(int64_t a, int64_t m) { return a & (m - 1); }
+GF2E_DEV int log2i(int64_t m) { return 63 - __clzll((unsigned long long)m); }
 
 // window i (0..4) of one squaring; lo >= hi when empty
 GF2E_DEV Win64 square_win(int i, int64_t r, int64_t s) {
@@ -79,27 +80,29 @@ GF2E_DEV Win64 square_win(int i, int64_t r, int64_t s) {
     switch (i) {
         case 0: w.c = 0; w.lo = 0; w.hi = r; w.K = 0; break;
         case 1: w.c = 1; w.lo = 1; w.hi = r - 1; w.K = h; break;
-        case 2: w.c = (s + 1) & 1; w.lo = s + 1; w.hi = r; w.K = h - (s + 1 - w.c) / 2; break;
-        case 3: w.c = s & 1; w.lo = 0; w.hi = s - 1; w.K = h + (r - s - 1 + w.c) / 2; break;
-        default: w.c = 0; w.lo = s; w.hi = 2 * s - 1; w.K = h + (r - 2 * s - 1) / 2; break;
+        case 2: w.c = (s + 1) & 1; w.lo = s + 1; w.hi = r; w.K = h - ((s + 1 - w.c) >> 1); break;
+        case 3: w.c = s & 1; w.lo = 0; w.hi = s - 1; w.K = h + ((r - s - 1 + w.c) >> 1); break;
+        default: w.c = 0; w.lo = s; w.hi = 2 * s - 1; w.K = h + ((r - 2 * s - 1) >> 1); break;
     }
     return w;
 }
 
-// trim [lo, hi) to its first and last member of class c (mod m)
+// trim [lo, hi) to its first and last member of class c (mod m); the moduli
+// are powers of two, so the divisions below are exact shifts
 GF2E_DEV void trim(Win64 &w) {
     if (w.lo >= w.hi) return;
     w.lo += mod_pos(w.c - w.lo, w.m);
-    if (w.lo < w.hi) w.hi = w.lo + w.m * ((w.hi - 1 - w.lo) / w.m) + 1;
+    if (w.lo < w.hi) w.hi = w.lo + ((w.hi - 1 - w.lo) & ~(w.m - 1)) + 1;
 }
 
 // outer window a (modulus 2) applied after inner window b
 GF2E_DEV Win64 compose(const Win64 &a, const Win64 &b) {
     Win64 w;
+    const int la = log2i(a.m), lb = log2i(b.m);
     w.m = a.m * b.m;
     w.c = a.c + a.m * mod_pos(b.c - a.K, b.m);
-    const int64_t t = (w.c - a.c) / a.m + a.K - b.c;      // divisible by b.m
-    w.K = t / b.m + b.K;
+    const int64_t t = ((w.c - a.c) >> la) + a.K - b.c;    // a multiple of b.m
+    w.K = (t >> lb) + b.K;                                 // exact: arithmetic shift
     w.lo = max(a.lo, a.c + a.m * (b.lo - a.K));
     w.hi = min(a.hi, a.c + a.m * (b.hi - a.K));
     trim(w);
@@ -156,79 +159,79 @@ GF2E_DEV ulonglong2 interleave4(u32 c0, u32 c1, u32 c2, u32 c3) {
     return v;
 }
 
-constexpr int WARPS = 8;                           // 256 threads per CTA
-constexpr int SLOT_WORDS = TWU + 8;                // a window's run, 16-byte aligned start
-constexpr size_t SMEM_BYTES = (size_t)WARPS * NCAND * SLOT_WORDS * sizeof(u32);
+// ---- the pass: per warp tile, the overlapping windows, two at a time
+constexpr int UL = 8;                     // units per lane per warp tile
+constexpr u32 TWL = 32 * UL;              // units per warp tile (512 output words)
 
-// 16-byte asynchronous global -> shared copy of `bytes` (0..16) source
-// bytes, the rest of the 16 zero-filled
-GF2E_DEV void cp_async16(u32 *dst, const u32 *src, u32 bytes) {
-    const unsigned sa = (unsigned)__cvta_generic_to_shared(dst);
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(sa), "l"(src), "r"(bytes)
-                 : "memory");
-}
 
-// Stage window w's input run for the tile at unit u0 into `slot`: words
-// [base, base + 4 nch) with base = (u0 + floor(K/32)) rounded down to a
-// multiple of 4; words outside [0, n32) read as zero.  Word u0 + floor(K/32)
-// lands at slot offset (u0 + floor(K/32)) mod 4.
-GF2E_DEV void stage_window(const u32 *__restrict__ in32, u32 n32, u32 u0, int K, u32 lane,
-                          u32 *slot) {
-    const int64_t first = (int64_t)u0 + (K >> 5);
-    const int64_t base = first & ~(int64_t)3;
-    const int delta = (int)(first - base);
-    const int nch = (delta + (int)TWU + 1 + 3) >> 2;
-    for (int ch = (int)lane; ch < nch; ch += 32) {
-        const int64_t g = base + 4 * ch;
-        u32 bytes = 0;
-        if (g >= 0 && g < (int64_t)n32) {
-            const int64_t left = (int64_t)n32 - g;
-            bytes = left >= 4 ? 16u : (u32)(4 * left);
-        }
-        cp_async16(slot + 4 * ch, bytes ? in32 + g : in32, bytes);
-    }
-}
-
-// Apply one staged window to the lane's units: input bits 32 u + K + t,
-// t = 0..31, are the slot's words i and i + 1 funnel-shifted by K mod 32.
-// Windows that start or end inside the tile keep only the bits t whose
-// output position 128 u + c + 4 t lies in [lo, hi).
-GF2E_DEV void apply_window(const u32 *slot, int delta, u32 u0, u32 lane, FWin w, bool full,
-                           u32 (&acc)[UPT]) {
-    const u32 sh = (u32)w.K & 31u;
-    const u32 *p = slot + delta + lane;
+// A full window over all of the tile's units, every index inside the state:
+// lane l's units u0 + l + 32 q read input words first + l + 32 q and the
+// word after it (the high word of the funnel shift) with two plain loads.
+GF2E_DEV void full_window(const u32 *__restrict__ in32, u32 first, u32 lane, u32 sh,
+                          u32 (&acc)[UL]) {
+    const u32 *__restrict__ p = in32 + (first + lane);
+    u32 lo[UL], hi[UL];
 #pragma unroll
-    for (int q = 0; q < UPT; q++) {
-        u32 v = __funnelshift_r(p[32 * q], p[32 * q + 1], sh);
-        if (!full) {
-            const int64_t u = (int64_t)u0 + lane + 32 * q;
-            const int64_t j0 = u * UBITS + w.c;                  // class bit t = 0
-            const int64_t tlo = w.lo > j0 ? (w.lo - j0) / M : 0;
-            int64_t thi = w.hi > j0 ? (w.hi - 1 - j0) / M + 1 : 0;
-            if (thi > 32) thi = 32;
-            u32 mask = 0;
-            if (tlo < thi)
-                mask = (thi == 32 ? 0xffffffffu : ((1u << thi) - 1u)) & ~((1u << tlo) - 1u);
-            v &= mask;
-        }
-        acc[q] ^= v;
+    for (int q = 0; q < UL; q++) {
+        lo[q] = __ldg(p + 32 * q);
+        hi[q] = __ldg(p + 32 * q + 1);
+    }
+#pragma unroll
+    for (int q = 0; q < UL; q++) acc[q] ^= __funnelshift_r(lo[q], hi[q], sh);
+}
+
+// Two full windows of one class, every load of both issued before use, so
+// their memory latencies overlap.
+GF2E_DEV void full_windows2(const u32 *__restrict__ in32, u32 first1, u32 sh1, u32 first2, u32 sh2,
+                         u32 lane, u32 (&acc)[UL]) {
+    const u32 *__restrict__ p1 = in32 + (first1 + lane);
+    const u32 *__restrict__ p2 = in32 + (first2 + lane);
+    u32 l1[UL], h1[UL], l2[UL], h2[UL];
+#pragma unroll
+    for (int q = 0; q < UL; q++) {
+        l1[q] = __ldg(p1 + 32 * q);
+        h1[q] = __ldg(p1 + 32 * q + 1);
+        l2[q] = __ldg(p2 + 32 * q);
+        h2[q] = __ldg(p2 + 32 * q + 1);
+    }
+#pragma unroll
+    for (int q = 0; q < UL; q++)
+        acc[q] ^= __funnelshift_r(l1[q], h1[q], sh1) ^ __funnelshift_r(l2[q], h2[q], sh2);
+}
+
+// Any other overlapping window: per unit the bits t whose output position
+// 128 u + c + 4 t lies in [lo, hi), loads bounds-tested.
+GF2E_DEV void part_window(const u32 *__restrict__ in32, u32 n32, u32 u0, u32 lane, FWin w,
+                        u32 (&acc)[UL]) {
+#pragma unroll
+    for (int q = 0; q < UL; q++) {
+        const int64_t u = (int64_t)u0 + lane + 32 * q;
+        const int64_t j0 = u * UBITS + w.c;
+        const int64_t tlo = w.lo > j0 ? (w.lo - j0) / M : 0;
+        int64_t thi = w.hi > j0 ? (w.hi - 1 - j0) / M + 1 : 0;
+        if (thi > 32) thi = 32;
+        if (tlo >= thi) continue;
+        const u32 mask = (thi == 32 ? 0xffffffffu : ((1u << thi) - 1u)) & ~((1u << tlo) - 1u);
+        const int64_t P = 32 * u + w.K;
+        const int64_t i = P >> 5;
+        const u32 lo = (i >= 0 && i < (int64_t)n32) ? __ldg(in32 + i) : 0u;
+        const u32 hi = (i + 1 >= 0 && i + 1 < (int64_t)n32) ? __ldg(in32 + i + 1) : 0u;
+        acc[q] ^= __funnelshift_r(lo, hi, (u32)P & 31u) & mask;
     }
 }
 
-// Batched F -> F^4 mod T: blockIdx.y = state, warps stride over its tiles.
-// Requires r < 2^31 and an even stride (each unit stores two words; the
-// word after an odd nw is padding and receives zero).
-__global__ void __launch_bounds__(WARPS * 32, 2)
+// Batched F -> F^4 mod T (r < 2^31 - 2^16, even stride): blockIdx.y = state.
+// Per warp tile of 256 units, one ballot lists the overlapping windows and
+// the ones covering the whole tile; those are applied with no masks or
+// bounds tests when the tile's highest index is inside the state.
+__global__ void __launch_bounds__(256, 3)
 k_frob4_batch(const u64 *__restrict__ in, u64 *__restrict__ out, size_t stride, u64 r,
-              const u64 *__restrict__ s_arr, u64 s_uniform) {
-    extern __shared__ u32 stage[];
+             const u64 *__restrict__ s_arr, u64 s_uniform) {
     __shared__ FWin tab[NCAND];
     __shared__ int s_nwin;
     const int st = blockIdx.y;
     const u64 s = s_arr ? s_arr[st] : s_uniform;
     if (threadIdx.x < 32) {
-        // warp 0 composes the candidates and lists the non-empty windows by
-        // class (tab[] in class order)
         const int lane = threadIdx.x;
         Win64 w{};
         bool ok = false;
@@ -255,48 +258,67 @@ k_frob4_batch(const u64 *__restrict__ in, u64 *__restrict__ out, size_t stride, 
     const u32 *in32 = reinterpret_cast<const u32 *>(in + (size_t)st * stride);
     ulonglong2 *o = reinterpret_cast<ulonglong2 *>(out + (size_t)st * stride);
     const u32 lane = threadIdx.x & 31;
-    u32 *slots = stage + (size_t)(threadIdx.x >> 5) * NCAND * SLOT_WORDS;
-    // the lane's own window (lane < nwin) for the per-tile overlap test
     const FWin mine = lane < (u32)nwin ? tab[lane] : FWin{0, 0, 0, 0};
-    const u32 ntiles = (nu + TWU - 1) / TWU;
+    const u32 ntiles = (nu + TWL - 1) / TWL;
     const u32 warps_total = (gridDim.x * blockDim.x) >> 5;
     for (u32 t = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; t < ntiles; t += warps_total) {
-        const u32 u0 = TWU * t;
-        const int64_t B0 = (int64_t)u0 * UBITS, B1 = B0 + (int64_t)TWU * UBITS;
+        const u32 u0 = TWL * t;
+        const int B0 = (int)(u0 * UBITS), B1 = B0 + (int)(TWL * UBITS);
         const bool over = lane < (u32)nwin && mine.hi > B0 && mine.lo < B1;
-        const bool cover = over && mine.lo <= B0 && mine.hi >= B1;
         const u32 act = __ballot_sync(0xffffffffu, over);
-        const u32 full = __ballot_sync(0xffffffffu, cover);
-        // stage every overlapping window's run, then wait once
-        int a = 0;
-        for (u32 m = act; m; m &= m - 1, a++)
-            stage_window(in32, n32, u0, tab[__ffs(m) - 1].K, lane, slots + a * SLOT_WORDS);
-        asm volatile("cp.async.commit_group;\n" ::: "memory");
-        asm volatile("cp.async.wait_group 0;\n" ::: "memory");
-        __syncwarp();
-        u32 C[M][UPT];
+        const u32 full = __ballot_sync(0xffffffffu, over && mine.lo <= B0 && mine.hi >= B1);
+        u32 C[M][UL];
 #pragma unroll
         for (int c = 0; c < M; c++)
 #pragma unroll
-            for (int q = 0; q < UPT; q++) C[c][q] = 0;
-        a = 0;
-        for (u32 m = act; m; m &= m - 1, a++) {
+            for (int q = 0; q < UL; q++) C[c][q] = 0;
+        for (u32 m = act; m; m &= m - 1) {
             const int k = __ffs(m) - 1;
             const FWin w = tab[k];
-            const bool fl = (full >> k) & 1;
-            const u32 *sl = slots + a * SLOT_WORDS;
-            const int delta = (int)(((int64_t)u0 + (w.K >> 5)) & 3);   // as stage_window
-            // the class is warp-uniform (one window at a time)
-            switch (w.c) {
-                case 0: apply_window(sl, delta, u0, lane, w, fl, C[0]); break;
-                case 1: apply_window(sl, delta, u0, lane, w, fl, C[1]); break;
-                case 2: apply_window(sl, delta, u0, lane, w, fl, C[2]); break;
-                default: apply_window(sl, delta, u0, lane, w, fl, C[3]); break;
+            // a full window reads without bounds tests when its highest index,
+            // u0 + floor(K/32) + 32 UL (lane 0's extra word, or one past the
+            // last lane's last word), is inside the state
+            const bool fast = ((full >> k) & 1) && (int)u0 + (w.K >> 5) + (int)TWL + 1 < (int)n32;
+            if (fast && (m & (m - 1))) {
+                const int k2 = __ffs(m & (m - 1)) - 1;
+                const FWin w2 = tab[k2];
+                const bool fast2 =
+                    ((full >> k2) & 1) && (int)u0 + (w2.K >> 5) + (int)TWL + 1 < (int)n32;
+                if (fast2 && w2.c == w.c) {
+                    const u32 f1 = (u32)((int)u0 + (w.K >> 5)), f2 = (u32)((int)u0 + (w2.K >> 5));
+                    const u32 s1 = (u32)w.K & 31u, s2 = (u32)w2.K & 31u;
+                    switch (w.c) {
+                        case 0: full_windows2(in32, f1, s1, f2, s2, lane, C[0]); break;
+                        case 1: full_windows2(in32, f1, s1, f2, s2, lane, C[1]); break;
+                        case 2: full_windows2(in32, f1, s1, f2, s2, lane, C[2]); break;
+                        default: full_windows2(in32, f1, s1, f2, s2, lane, C[3]); break;
+                    }
+                    m &= m - 1;                   // the second window is done too
+                    continue;
+                }
+            }
+            const u32 first = (u32)((int)u0 + (w.K >> 5)), sh = (u32)w.K & 31u;
+            switch (w.c) {            // the class is warp-uniform (one window at a time)
+                case 0:
+                    if (fast) full_window(in32, first, lane, sh, C[0]);
+                    else part_window(in32, n32, u0, lane, w, C[0]);
+                    break;
+                case 1:
+                    if (fast) full_window(in32, first, lane, sh, C[1]);
+                    else part_window(in32, n32, u0, lane, w, C[1]);
+                    break;
+                case 2:
+                    if (fast) full_window(in32, first, lane, sh, C[2]);
+                    else part_window(in32, n32, u0, lane, w, C[2]);
+                    break;
+                default:
+                    if (fast) full_window(in32, first, lane, sh, C[3]);
+                    else part_window(in32, n32, u0, lane, w, C[3]);
+                    break;
             }
         }
-        __syncwarp();                     // slots are rewritten by the next tile
 #pragma unroll
-        for (int q = 0; q < UPT; q++) {
+        for (int q = 0; q < UL; q++) {
             const u32 u = u0 + lane + 32 * q;
             if (u < nu) o[u] = interleave4(C[0][q], C[1][q], C[2][q], C[3][q]);
         }
@@ -317,34 +339,24 @@ int squarings_per_pass() {
     return v;
 }
 
-bool frob4_supported(u64 r, size_t stride) { return r < (1ull << 31) && !(stride & 1); }
+bool frob4_supported(u64 r, size_t stride) {
+    return r < (1ull << 31) - (1ull << 16) && !(stride & 1);
+}
 
 int launch_frob4(const u64 *in, u64 *out, size_t stride, int nstates, u64 r, const u64 *s_dev,
                  u64 s, cudaStream_t st) {
     if (!frob4_supported(r, stride)) return invalid("launch_frob4: needs r < 2^31, even stride");
     const size_t nw = (size_t)((r + 63) >> 6);
     const size_t nu = (nw + 1) / 2;
-    const int threads = 256;
-    // two warp tiles per warp when the grid still fills every SM at least
-    // four times over (2 resident blocks each), else one
-    const size_t tile_units = (size_t)TWU * (threads / 32);
-    const size_t wide = (nu + 2 * tile_units - 1) / (2 * tile_units);
-    const bool two = wide * (size_t)nstates >= (size_t)8 * sm_count();
-    const size_t per_block = two ? 2 * tile_units : tile_units;
-    size_t bx = (nu + per_block - 1) / per_block;
+    // each warp takes four warp tiles (the window set each CTA composes then
+    // serves 32 tiles) when that still gives every SM two rounds of its 3
+    // resident CTAs, else one (small states, r ~ 10^6)
+    const size_t ntile = (nu + TWL - 1) / TWL;
+    const bool four = (ntile + 31) / 32 * (size_t)nstates >= (size_t)6 * sm_count();
+    size_t bx = four ? (ntile + 31) / 32 : (ntile + 7) / 8;
     if (bx > 65535) bx = 65535;
-    static std::atomic<bool> attr_done[64];
-    int dev = 0;
-    cudaGetDevice(&dev);
-    if (dev >= 0 && dev < 64 && !attr_done[dev].load(std::memory_order_acquire)) {
-        cudaError_t e = cudaFuncSetAttribute(k_frob4_batch,
-                                             cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             (int)SMEM_BYTES);
-        if (e != cudaSuccess) return cuda_status(e, "k_frob4_batch smem attribute");
-        attr_done[dev].store(true, std::memory_order_release);
-    }
-    k_frob4_batch<<<dim3((unsigned)bx, (unsigned)nstates), threads, SMEM_BYTES, st>>>(
-        in, out, stride, r, s_dev, s);
+    k_frob4_batch<<<dim3((unsigned)bx, (unsigned)nstates), 256, 0, st>>>(in, out, stride, r,
+                                                                      s_dev, s);
     GF2E_CHECK_LAUNCH("k_frob4_batch");
     return GF2E_OK;
 }

@@ -248,26 +248,42 @@ GF2E_DEV Lehmer lehmer_round(u64 wa, u64 wb, long long da, long long db, long lo
     int dga = (int)(da - lo), dgb = deg64(wb), dma = 0, dmb = 0, steps = 0;
     const bool exact = (lo == 0);
     const int dstop = (int)max(-1LL, m - lo);          // window degree of x^m
+    // the windows left-aligned (leading coefficient at bit 63): the division
+    // below then tests one bit and shifts, with no degree search per step
+    u64 A = wa << (63 - dga);
+    u64 B = dgb >= 0 ? wb << (63 - dgb) : 0;
     for (int it = 0; it < 64; it++) {
         if (dgb < 0 || dgb < dstop) break;              // b = 0 / half-gcd stop
         const int dq = dga - dgb;
         const int ndm = max(dma, dmb + dq);
         if (ndm > 31) break;                            // matrix degree bound
         if (!exact && dgb < ndm) break;                 // quotient not exact
+        // a <- a mod b, row a += q row b: at each of the dq + 1 degrees from
+        // the top, XOR in b (and x^(dq-j) row b) when a's leading bit is set,
+        // then move one degree down.  Afterwards bit 63 of A is degree dgb.
+        u32 s0 = mb0 << dq, s1 = mb1 << dq;
 #pragma unroll 1
-        do {                                            // a <- a mod b
-            const int k = dga - dgb;
-            wa ^= wb << k;
-            ma0 ^= mb0 << k;
-            ma1 ^= mb1 << k;
-            dga = deg64(wa);
-        } while (dga >= dgb);
-        dma = ndm;
-        u64 t = wa; wa = wb; wb = t;                    // (a, b) <- (b, a mod b)
+        for (int j = 0;; j++) {
+            const u64 msk = (u64)((long long)A >> 63);
+            A ^= B & msk;
+            ma0 ^= s0 & (u32)msk;
+            ma1 ^= s1 & (u32)msk;
+            if (j == dq) break;
+            A <<= 1;
+            s0 >>= 1;
+            s1 >>= 1;
+        }
+        const int c = A ? __clzll(A) : 64;
+        const u64 Bn = A ? A << c : 0;
+        const int dr = A ? dgb - c : -1;
+        A = B;                                          // (a, b) <- (b, a mod b)
+        B = Bn;
+        dga = dgb;
+        dgb = dr;
         u32 y = ma0; ma0 = mb0; mb0 = y;
         y = ma1; ma1 = mb1; mb1 = y;
-        int z = dga; dga = dgb; dgb = z;
-        z = dma; dma = dmb; dmb = z;
+        dma = dmb;
+        dmb = ndm;
         steps++;
     }
     if (steps == 0) {
