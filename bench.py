@@ -246,7 +246,7 @@ def main():
     states = torch.empty(stride * n, dtype=torch.int64, device="cuda")
     scratch = torch.empty_like(states)
     s_dev = torch.from_numpy(s_host.view(np.int64)).cuda()
-    per_pass = M.engine.squarings_per_pass(r, stride)
+    per_pass = M.engine.squarings_per_pass(r, stride, n)
     # passes of the squaring kernel per step (an odd pass count gets one
     # fused pass split in two, as gf2e_trin_square_batch does)
     n4 = k // 2 if per_pass == 2 else 0

@@ -119,10 +119,13 @@ int gf2e_trin_square_batch(uint64_t *states_dev, uint64_t *scratch_dev,
                            size_t stride_words, int nstates, uint64_t r,
                            const uint64_t *s_dev, uint32_t k, void *stream);
 
-/* Squarings per pass that gf2e_trin_square_batch uses for this r and
- * stride: 2, or 1 where the fused pass does not apply (r >= 2^31, an odd
- * stride, or GF2E_SQUARINGS_PER_PASS=1 in the environment).  Host only. */
-int gf2e_trin_squarings_per_pass(uint64_t r, size_t stride_words);
+/* Squarings per pass that gf2e_trin_square_batch uses for this r, stride
+ * and state count: 2, or 1 where the fused pass does not apply or does not
+ * pay (r >= 2^31 - 2^16, an odd stride, states and scratch small enough to
+ * stay in L2 (at most 96 MB), or GF2E_SQUARINGS_PER_PASS=1 in the
+ * environment; GF2E_SQUARINGS_PER_PASS=2 uses the fused pass wherever it
+ * applies).  Host only. */
+int gf2e_trin_squarings_per_pass(uint64_t r, size_t stride_words, int nstates);
 
 /* Host-buffer form of the above, the whole of trinomial_stage2.cu `run`
  * (195-277) for many s with k0 > k1: F_k = x^(2^k) mod x^r + x^(s_i) + 1 for

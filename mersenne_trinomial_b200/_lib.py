@@ -96,7 +96,7 @@ SIGNATURES = {
     "gf2e_trin_square": (_i32, [_vp, _vp, _u64, _u64, _vp]),
     "gf2e_trin_square_batch": (_i32, [_vp, _vp, _sz, _i32, _u64, _vp, C.c_uint32, _vp]),
     "gf2e_trin_frobenius_host": (_i32, [_u64, _vp, _i32, C.c_uint32, _vp, _sz, _vp]),
-    "gf2e_trin_squarings_per_pass": (_i32, [_u64, _sz]),
+    "gf2e_trin_squarings_per_pass": (_i32, [_u64, _sz, _i32]),
     "gf2e_trin_set_x": (_i32, [_vp, _sz, _i32, _u64, _vp]),
     "gf2e_trin_set_one": (_i32, [_vp, _sz, _i32, _u64, _vp]),
     "gf2e_trin_reduce": (_i32, [_vp, _u64, _vp, _u64, _u64, _vp]),

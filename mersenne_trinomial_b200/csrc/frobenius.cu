@@ -329,19 +329,33 @@ k_frob4_batch(const u64 *__restrict__ in, u64 *__restrict__ out, size_t stride, 
 
 namespace gf2e {
 
-// squarings fused per pass for the batched entry points: 2 (default) or 1
-// (GF2E_SQUARINGS_PER_PASS=1 keeps the one-squaring kernel throughout)
-int squarings_per_pass() {
-    static const int v = [] {
-        const char *e = getenv("GF2E_SQUARINGS_PER_PASS");
-        return (e && atoi(e) == 1) ? 1 : 2;
-    }();
-    return v;
-}
-
 bool frob4_supported(u64 r, size_t stride) {
     return r < (1ull << 31) - (1ull << 16) && !(stride & 1);
 }
+
+// squarings fused per pass for the batched entry points, from
+// GF2E_SQUARINGS_PER_PASS (read at each call): 1 keeps the one-squaring
+// kernel throughout, 2 uses the fused pass wherever it applies; unset, the
+// fused pass is used where it applies and the states do not fit in L2.
+int squarings_per_pass() {
+    const char *e = getenv("GF2E_SQUARINGS_PER_PASS");
+    if (!e) return 0;
+    const int v = atoi(e);
+    return v == 1 || v == 2 ? v : 0;
+}
+
+// fused pass for this batch: applies (r, stride) and pays (not in L2), or forced
+bool use_frob4(u64 r, size_t stride, int nstates) {
+    const int mode = squarings_per_pass();
+    if (mode == 1 || !frob4_supported(r, stride)) return false;
+    if (mode == 2) return true;
+    // the fused pass halves the HBM traffic per squaring but issues more
+    // instructions per byte: when the states and their scratch fit in L2
+    // (measured: 256 states at r ~ 10^6, 64 MB, 7 % slower fused) the
+    // one-squaring pass is kept
+    return (size_t)nstates * stride * 16 > ((size_t)96 << 20);
+}
+
 
 int launch_frob4(const u64 *in, u64 *out, size_t stride, int nstates, u64 r, const u64 *s_dev,
                  u64 s, cudaStream_t st) {
@@ -372,7 +386,7 @@ int trin_square_any(const u64 *in, u64 *out, size_t stride, int nstates, u64 r,
 // only single passes apply and k is odd.
 int frobenius_states(u64 *a, u64 *b, size_t stride, int nstates, u64 r, const u64 *s_dev,
                      u64 k, cudaStream_t st, u64 s_uniform) {
-    const bool fused = squarings_per_pass() == 2 && frob4_supported(r, stride);
+    const bool fused = use_frob4(r, stride, nstates);
     u64 n4 = fused ? k / 2 : 0, n1 = k - 2 * n4;
     if (((n4 + n1) & 1) && n4 > 0) {
         n4--;
@@ -397,6 +411,6 @@ int frobenius_states(u64 *a, u64 *b, size_t stride, int nstates, u64 r, const u6
 
 }  // namespace gf2e
 
-extern "C" int gf2e_trin_squarings_per_pass(uint64_t r, size_t stride_words) {
-    return (gf2e::squarings_per_pass() == 2 && gf2e::frob4_supported(r, stride_words)) ? 2 : 1;
+extern "C" int gf2e_trin_squarings_per_pass(uint64_t r, size_t stride_words, int nstates) {
+    return gf2e::use_frob4(r, stride_words, nstates < 1 ? 1 : nstates) ? 2 : 1;
 }

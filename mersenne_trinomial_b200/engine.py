@@ -495,10 +495,10 @@ def trin_square_batch(states, scratch, stride_words: int, nstates: int, r: int, 
          _ptr(s_dev), k, _sp(stream))
 
 
-def squarings_per_pass(r: int, stride_words: int) -> int:
+def squarings_per_pass(r: int, stride_words: int, nstates: int) -> int:
     """Squarings one pass of trin_square_batch performs (2 where the fused
-    F -> F^4 pass applies, else 1)."""
-    return int(lib().gf2e_trin_squarings_per_pass(r, stride_words))
+    F -> F^4 pass applies and pays, else 1)."""
+    return int(lib().gf2e_trin_squarings_per_pass(r, stride_words, nstates))
 
 
 def frobenius_host(r: int, s_values, k: int, out: Optional[np.ndarray] = None,

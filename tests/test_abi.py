@@ -90,3 +90,26 @@ def test_workloads_are_seeded_and_valid():
     assert all(2**16 <= a <= 2**27 and 2**16 <= b <= 2**27 for a, b in c3["sizes"])
     x = W.random_bits(1000, 5)
     assert x.size == 16 and int(x[-1]) >> 40 == 0
+
+
+def test_squarings_per_pass_rule(monkeypatch):
+    """Host-only: the fused two-squaring pass is chosen for batches that do
+    not fit in L2 (states and scratch above 96 MB), the one-squaring pass for
+    smaller ones, r near 2^31 or an odd stride; GF2E_SQUARINGS_PER_PASS
+    forces either."""
+    import mersenne_trinomial_b200 as M
+    L = M.lib()
+    monkeypatch.delenv("GF2E_SQUARINGS_PER_PASS", raising=False)
+    r = 136279841
+    nw = (r + 63) // 64
+    stride = nw + (nw & 1)
+    assert L.gf2e_trin_squarings_per_pass(r, stride, 64) == 2
+    assert L.gf2e_trin_squarings_per_pass(r, stride, 2) == 1          # 68 MB: in L2
+    assert L.gf2e_trin_squarings_per_pass(r, stride + 1, 64) == 1     # odd stride
+    assert L.gf2e_trin_squarings_per_pass(999961, 15626, 256) == 1    # config 2: 64 MB
+    assert L.gf2e_trin_squarings_per_pass((1 << 31) - 1, 1 << 25, 8) == 1
+    monkeypatch.setenv("GF2E_SQUARINGS_PER_PASS", "2")
+    assert L.gf2e_trin_squarings_per_pass(999961, 15626, 256) == 2
+    assert L.gf2e_trin_squarings_per_pass(r, stride + 1, 64) == 1
+    monkeypatch.setenv("GF2E_SQUARINGS_PER_PASS", "1")
+    assert L.gf2e_trin_squarings_per_pass(r, stride, 64) == 1

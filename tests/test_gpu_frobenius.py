@@ -16,6 +16,13 @@ from conftest import load_json
 pytestmark = pytest.mark.gpu
 
 
+@pytest.fixture(autouse=True)
+def fused_everywhere(monkeypatch):
+    """Small batches would take the one-squaring pass (they fit in L2): force
+    the fused pass so that every case here exercises it."""
+    monkeypatch.setenv("GF2E_SQUARINGS_PER_PASS", "2")
+
+
 def rand_states(rng, r, n):
     nw = (r + 63) // 64
     st = rng.integers(0, 2**63, size=(n, nw), dtype=np.uint64) * np.uint64(2) + \
