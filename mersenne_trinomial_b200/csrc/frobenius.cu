@@ -29,8 +29,8 @@
 // consecutive input bits 32 u + K + t: one funnel-shifted 32-bit read per
 // window, XORed into the class accumulator C[c].  The unit's output is the
 // 4-way bit interleave of C[0..3] (bit 4 t + c = bit t of C[c]): cross-
-// register delta swaps, a byte transpose by byte permutes, then two delta
-// swaps inside each 32 bits.  Lanes own units u0 + lane + 32 q, q < 8, so
+// register and in-register delta swaps, then a byte transpose by byte
+// permutes.  Lanes own units u0 + lane + 32 q, q < 8, so
 // loads and 16-byte stores are coalesced.
 //
 // Per warp tile of 256 units, one ballot lists the windows overlapping it and
@@ -121,15 +121,15 @@ GF2E_DEV Win64 candidate(int i, int64_t r, int64_t s) {
 }
 
 // 4-way bit interleave of one unit: bit 4 t + c of the 128-bit output is
-// bit t of C[c].  Index bookkeeping (register index, then bit position): the
-// input holds bit t of class c = (c1 c0) at register (c1 c0), position
-// (t4 t3 t2 t1 t0).  Two cross-register delta swaps exchange register bit 0
-// with position bit 0 and register bit 1 with position bit 1, giving
-// register (t1 t0), position (t4 t3 t2 c1 c0); a 4x4 byte transpose (8 byte
-// permutes) exchanges the register index with the byte index, giving
-// register (t4 t3), position (t1 t0 t2 c1 c0); two delta swaps inside each
-// register rotate its position bits to (t2 t1 t0 c1 c0), so register b
-// holds output bits [32 b, 32 b + 32).
+// bit t of C[c].  Index bookkeeping (register index r1 r0, then bit position
+// p4..p0): the input holds bit t of class c = (c1 c0) at register (c1 c0),
+// position (t4 t3 t2 t1 t0).  Relabelling the registers (free) swaps r1 and
+// r0; a cross-register delta swap exchanges r0 with p1, another r1 with p2,
+// and one delta swap inside each register exchanges p0 with p2, which gives
+// register (t2 t1), position (t4 t3 t0 c1 c0); a 4x4 byte transpose (8 byte
+// permutes) then exchanges the register index with the byte index (p4 p3):
+// register (t4 t3), position (t2 t1 t0 c1 c0), so register b holds output
+// bits [32 b, 32 b + 32).  44 operations for 128 output bits.
 GF2E_DEV void xswap(u32 &x, u32 &y, int sh, u32 m) {    // x[p + sh] <-> y[p], p in m
     const u32 t = ((x >> sh) ^ y) & m;
     y ^= t;
@@ -139,34 +139,32 @@ GF2E_DEV u32 dswap(u32 x, int d, u32 m) {                // x[p] <-> x[p + d], p
     const u32 t = (x ^ (x >> d)) & m;
     return x ^ (t * (1u + (1u << d)));       // t and t << d are disjoint
 }
-GF2E_DEV u32 rot_pos(u32 x) {                            // (t1 t0 t2 c1 c0) -> (t2 t1 t0 c1 c0)
-    return dswap(dswap(x, 4, 0x00F000F0u), 8, 0x0000FF00u);
-}
 GF2E_DEV ulonglong2 interleave4(u32 c0, u32 c1, u32 c2, u32 c3) {
-    xswap(c0, c1, 1, 0x55555555u);
-    xswap(c2, c3, 1, 0x55555555u);
-    xswap(c0, c2, 2, 0x33333333u);
-    xswap(c1, c3, 2, 0x33333333u);
-    const u32 lo01 = __byte_perm(c0, c1, 0x5140), hi01 = __byte_perm(c0, c1, 0x7362);
-    const u32 lo23 = __byte_perm(c2, c3, 0x5140), hi23 = __byte_perm(c2, c3, 0x7362);
-    const u32 o0 = rot_pos(__byte_perm(lo01, lo23, 0x5410));
-    const u32 o1 = rot_pos(__byte_perm(lo01, lo23, 0x7632));
-    const u32 o2 = rot_pos(__byte_perm(hi01, hi23, 0x5410));
-    const u32 o3 = rot_pos(__byte_perm(hi01, hi23, 0x7632));
+    u32 r0 = c0, r1 = c2, r2 = c1, r3 = c3;              // r1 <-> r0 of the index
+    xswap(r0, r1, 2, 0x33333333u);                       // r0 <-> p1
+    xswap(r2, r3, 2, 0x33333333u);
+    xswap(r0, r2, 4, 0x0F0F0F0Fu);                       // r1 <-> p2
+    xswap(r1, r3, 4, 0x0F0F0F0Fu);
+    r0 = dswap(r0, 3, 0x0A0A0A0Au);                      // p0 <-> p2
+    r1 = dswap(r1, 3, 0x0A0A0A0Au);
+    r2 = dswap(r2, 3, 0x0A0A0A0Au);
+    r3 = dswap(r3, 3, 0x0A0A0A0Au);
+    const u32 lo01 = __byte_perm(r0, r1, 0x5140), hi01 = __byte_perm(r0, r1, 0x7362);
+    const u32 lo23 = __byte_perm(r2, r3, 0x5140), hi23 = __byte_perm(r2, r3, 0x7362);
     ulonglong2 v;
-    v.x = ((u64)o1 << 32) | o0;
-    v.y = ((u64)o3 << 32) | o2;
+    v.x = ((u64)__byte_perm(lo01, lo23, 0x7632) << 32) | __byte_perm(lo01, lo23, 0x5410);
+    v.y = ((u64)__byte_perm(hi01, hi23, 0x7632) << 32) | __byte_perm(hi01, hi23, 0x5410);
     return v;
 }
 
 // ---- the pass: per warp tile, the overlapping windows, two at a time
-constexpr int UL = 8;                     // units per lane per warp tile
-constexpr u32 TWL = 32 * UL;              // units per warp tile (512 output words)
+constexpr int UL_DEFAULT = 8;             // units per lane per warp tile (512 words a tile)
 
 
 // A full window over all of the tile's units, every index inside the state:
 // lane l's units u0 + l + 32 q read input words first + l + 32 q and the
 // word after it (the high word of the funnel shift) with two plain loads.
+template <int UL>
 GF2E_DEV void full_window(const u32 *__restrict__ in32, u32 first, u32 lane, u32 sh,
                           u32 (&acc)[UL]) {
     const u32 *__restrict__ p = in32 + (first + lane);
@@ -182,6 +180,7 @@ GF2E_DEV void full_window(const u32 *__restrict__ in32, u32 first, u32 lane, u32
 
 // Two full windows of one class, every load of both issued before use, so
 // their memory latencies overlap.
+template <int UL>
 GF2E_DEV void full_windows2(const u32 *__restrict__ in32, u32 first1, u32 sh1, u32 first2, u32 sh2,
                          u32 lane, u32 (&acc)[UL]) {
     const u32 *__restrict__ p1 = in32 + (first1 + lane);
@@ -201,6 +200,7 @@ GF2E_DEV void full_windows2(const u32 *__restrict__ in32, u32 first1, u32 sh1, u
 
 // Any other overlapping window: per unit the bits t whose output position
 // 128 u + c + 4 t lies in [lo, hi), loads bounds-tested.
+template <int UL>
 GF2E_DEV void part_window(const u32 *__restrict__ in32, u32 n32, u32 u0, u32 lane, FWin w,
                         u32 (&acc)[UL]) {
 #pragma unroll
@@ -220,108 +220,161 @@ GF2E_DEV void part_window(const u32 *__restrict__ in32, u32 n32, u32 u0, u32 lan
     }
 }
 
-// Batched F -> F^4 mod T (r < 2^31 - 2^16, even stride): blockIdx.y = state.
-// Per warp tile of 256 units, one ballot lists the overlapping windows and
-// the ones covering the whole tile; those are applied with no masks or
-// bounds tests when the tile's highest index is inside the state.
-__global__ void __launch_bounds__(256, 3)
+// Warp-wide: compose the windows of F -> F^4 mod x^r + x^s + 1 into tab[]
+// in class order; returns their number (lane 0's count, on every lane).
+GF2E_DEV int compose_windows(u64 r, u64 s, FWin *tab, u32 lane) {
+    Win64 w{};
+    bool ok = false;
+    if (lane < (u32)NCAND) {
+        w = candidate((int)lane, (int64_t)r, (int64_t)s);
+        ok = w.lo < w.hi;
+    }
+    int base = 0;
+    for (int c = 0; c < M; c++) {
+        const u32 b = __ballot_sync(0xffffffffu, ok && w.c == c);
+        if (ok && w.c == c) {
+            const int pos = base + __popc(b & ((1u << lane) - 1u));
+            tab[pos] = FWin{(int)w.lo, (int)w.hi, (int)w.K, c};
+        }
+        base += __popc(b);
+    }
+    __syncwarp();
+    return base;
+}
+
+// One warp tile: the 32 UL units from u0 of one state.  tab[] holds the
+// state's nwin windows, `mine` is tab[lane] (lane < nwin).  One ballot lists
+// the windows overlapping the tile and another those covering all of it;
+// the covering ones whose reads stay inside the state are applied with no
+// masks or bounds tests, two of a class at a time.
+template <int UL>
+GF2E_DEV void frob4_tile(const u32 *__restrict__ in32, ulonglong2 *__restrict__ o, u32 n32,
+                         u32 nu, const FWin *tab, int nwin, const FWin &mine, u32 u0, u32 lane) {
+    constexpr u32 TWL = 32 * UL;
+    const int B0 = (int)(u0 * UBITS), B1 = B0 + (int)(TWL * UBITS);
+    const bool over = lane < (u32)nwin && mine.hi > B0 && mine.lo < B1;
+    const u32 act = __ballot_sync(0xffffffffu, over);
+    const u32 full = __ballot_sync(0xffffffffu, over && mine.lo <= B0 && mine.hi >= B1);
+    u32 C[M][UL];
+#pragma unroll
+    for (int c = 0; c < M; c++)
+#pragma unroll
+        for (int q = 0; q < UL; q++) C[c][q] = 0;
+    for (u32 m = act; m; m &= m - 1) {
+        const int k = __ffs(m) - 1;
+        const FWin w = tab[k];
+        // a full window reads without bounds tests when its highest index,
+        // u0 + floor(K/32) + 32 UL (one past the last lane's last word), is
+        // inside the state
+        const bool fast = ((full >> k) & 1) && (int)u0 + (w.K >> 5) + (int)TWL + 1 < (int)n32;
+        if (fast && (m & (m - 1))) {
+            const int k2 = __ffs(m & (m - 1)) - 1;
+            const FWin w2 = tab[k2];
+            const bool fast2 =
+                ((full >> k2) & 1) && (int)u0 + (w2.K >> 5) + (int)TWL + 1 < (int)n32;
+            if (fast2 && w2.c == w.c) {
+                const u32 f1 = (u32)((int)u0 + (w.K >> 5)), f2 = (u32)((int)u0 + (w2.K >> 5));
+                const u32 s1 = (u32)w.K & 31u, s2 = (u32)w2.K & 31u;
+                switch (w.c) {
+                    case 0: full_windows2<UL>(in32, f1, s1, f2, s2, lane, C[0]); break;
+                    case 1: full_windows2<UL>(in32, f1, s1, f2, s2, lane, C[1]); break;
+                    case 2: full_windows2<UL>(in32, f1, s1, f2, s2, lane, C[2]); break;
+                    default: full_windows2<UL>(in32, f1, s1, f2, s2, lane, C[3]); break;
+                }
+                m &= m - 1;                   // the second window is done too
+                continue;
+            }
+        }
+        const u32 first = (u32)((int)u0 + (w.K >> 5)), sh = (u32)w.K & 31u;
+        switch (w.c) {            // the class is warp-uniform (one window at a time)
+            case 0:
+                if (fast) full_window<UL>(in32, first, lane, sh, C[0]);
+                else part_window<UL>(in32, n32, u0, lane, w, C[0]);
+                break;
+            case 1:
+                if (fast) full_window<UL>(in32, first, lane, sh, C[1]);
+                else part_window<UL>(in32, n32, u0, lane, w, C[1]);
+                break;
+            case 2:
+                if (fast) full_window<UL>(in32, first, lane, sh, C[2]);
+                else part_window<UL>(in32, n32, u0, lane, w, C[2]);
+                break;
+            default:
+                if (fast) full_window<UL>(in32, first, lane, sh, C[3]);
+                else part_window<UL>(in32, n32, u0, lane, w, C[3]);
+                break;
+        }
+    }
+#pragma unroll
+    for (int q = 0; q < UL; q++) {
+        const u32 u = u0 + lane + 32 * q;
+        if (u < nu) o[u] = interleave4(C[0][q], C[1][q], C[2][q], C[3][q]);
+    }
+}
+
+// Batched F -> F^4 mod T (r < 2^31 - 2^16, even stride): blockIdx.y = state;
+// warp 0 composes the state's windows for the CTA, the warps stride over
+// its tiles.
+template <int UL, int MINB>
+__global__ void __launch_bounds__(256, MINB)
 k_frob4_batch(const u64 *__restrict__ in, u64 *__restrict__ out, size_t stride, u64 r,
-             const u64 *__restrict__ s_arr, u64 s_uniform) {
+              const u64 *__restrict__ s_arr, u64 s_uniform) {
     __shared__ FWin tab[NCAND];
     __shared__ int s_nwin;
     const int st = blockIdx.y;
-    const u64 s = s_arr ? s_arr[st] : s_uniform;
+    const u32 lane = threadIdx.x & 31;
     if (threadIdx.x < 32) {
-        const int lane = threadIdx.x;
-        Win64 w{};
-        bool ok = false;
-        if (lane < NCAND) {
-            w = candidate(lane, (int64_t)r, (int64_t)s);
-            ok = w.lo < w.hi;
-        }
-        int base = 0;
-        for (int c = 0; c < M; c++) {
-            const u32 b = __ballot_sync(0xffffffffu, ok && w.c == c);
-            if (ok && w.c == c) {
-                const int pos = base + __popc(b & ((1u << lane) - 1u));
-                tab[pos] = FWin{(int)w.lo, (int)w.hi, (int)w.K, c};
-            }
-            base += __popc(b);
-        }
-        if (lane == 0) s_nwin = base;
+        const int n = compose_windows(r, s_arr ? s_arr[st] : s_uniform, tab, lane);
+        if (lane == 0) s_nwin = n;
     }
     __syncthreads();
     const int nwin = s_nwin;
     const u32 nw = (u32)((r + 63) >> 6);
-    const u32 n32 = 2 * nw;
-    const u32 nu = (nw + 1) >> 1;
+    const u32 n32 = 2 * nw, nu = (nw + 1) >> 1;
     const u32 *in32 = reinterpret_cast<const u32 *>(in + (size_t)st * stride);
     ulonglong2 *o = reinterpret_cast<ulonglong2 *>(out + (size_t)st * stride);
-    const u32 lane = threadIdx.x & 31;
     const FWin mine = lane < (u32)nwin ? tab[lane] : FWin{0, 0, 0, 0};
+    constexpr u32 TWL = 32 * UL;
     const u32 ntiles = (nu + TWL - 1) / TWL;
     const u32 warps_total = (gridDim.x * blockDim.x) >> 5;
-    for (u32 t = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; t < ntiles; t += warps_total) {
-        const u32 u0 = TWL * t;
-        const int B0 = (int)(u0 * UBITS), B1 = B0 + (int)(TWL * UBITS);
-        const bool over = lane < (u32)nwin && mine.hi > B0 && mine.lo < B1;
-        const u32 act = __ballot_sync(0xffffffffu, over);
-        const u32 full = __ballot_sync(0xffffffffu, over && mine.lo <= B0 && mine.hi >= B1);
-        u32 C[M][UL];
-#pragma unroll
-        for (int c = 0; c < M; c++)
-#pragma unroll
-            for (int q = 0; q < UL; q++) C[c][q] = 0;
-        for (u32 m = act; m; m &= m - 1) {
-            const int k = __ffs(m) - 1;
-            const FWin w = tab[k];
-            // a full window reads without bounds tests when its highest index,
-            // u0 + floor(K/32) + 32 UL (lane 0's extra word, or one past the
-            // last lane's last word), is inside the state
-            const bool fast = ((full >> k) & 1) && (int)u0 + (w.K >> 5) + (int)TWL + 1 < (int)n32;
-            if (fast && (m & (m - 1))) {
-                const int k2 = __ffs(m & (m - 1)) - 1;
-                const FWin w2 = tab[k2];
-                const bool fast2 =
-                    ((full >> k2) & 1) && (int)u0 + (w2.K >> 5) + (int)TWL + 1 < (int)n32;
-                if (fast2 && w2.c == w.c) {
-                    const u32 f1 = (u32)((int)u0 + (w.K >> 5)), f2 = (u32)((int)u0 + (w2.K >> 5));
-                    const u32 s1 = (u32)w.K & 31u, s2 = (u32)w2.K & 31u;
-                    switch (w.c) {
-                        case 0: full_windows2(in32, f1, s1, f2, s2, lane, C[0]); break;
-                        case 1: full_windows2(in32, f1, s1, f2, s2, lane, C[1]); break;
-                        case 2: full_windows2(in32, f1, s1, f2, s2, lane, C[2]); break;
-                        default: full_windows2(in32, f1, s1, f2, s2, lane, C[3]); break;
-                    }
-                    m &= m - 1;                   // the second window is done too
-                    continue;
-                }
-            }
-            const u32 first = (u32)((int)u0 + (w.K >> 5)), sh = (u32)w.K & 31u;
-            switch (w.c) {            // the class is warp-uniform (one window at a time)
-                case 0:
-                    if (fast) full_window(in32, first, lane, sh, C[0]);
-                    else part_window(in32, n32, u0, lane, w, C[0]);
-                    break;
-                case 1:
-                    if (fast) full_window(in32, first, lane, sh, C[1]);
-                    else part_window(in32, n32, u0, lane, w, C[1]);
-                    break;
-                case 2:
-                    if (fast) full_window(in32, first, lane, sh, C[2]);
-                    else part_window(in32, n32, u0, lane, w, C[2]);
-                    break;
-                default:
-                    if (fast) full_window(in32, first, lane, sh, C[3]);
-                    else part_window(in32, n32, u0, lane, w, C[3]);
-                    break;
-            }
+    for (u32 t = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; t < ntiles; t += warps_total)
+        frob4_tile<UL>(in32, o, n32, nu, tab, nwin, mine, TWL * t, lane);
+}
+
+// The same pass as a persistent grid (a fixed number of CTAs): warp w takes
+// the w-th contiguous share of all (state, tile) pairs and composes its own
+// window table whenever its share moves to the next state.
+template <int UL, int MINB>
+__global__ void __launch_bounds__(256, MINB)
+k_frob4_persist(const u64 *__restrict__ in, u64 *__restrict__ out, size_t stride, u64 r,
+                const u64 *__restrict__ s_arr, u64 s_uniform, int nstates) {
+    __shared__ FWin tabs[8][NCAND];
+    const u32 lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    FWin *tab = tabs[wid];
+    const u32 nw = (u32)((r + 63) >> 6);
+    const u32 n32 = 2 * nw, nu = (nw + 1) >> 1;
+    constexpr u32 TWL = 32 * UL;
+    const u32 ntiles = (nu + TWL - 1) / TWL;
+    const u64 total = (u64)ntiles * (u64)nstates;
+    const u64 warps = (u64)((gridDim.x * blockDim.x) >> 5);
+    const u64 share = (total + warps - 1) / warps;
+    const u64 w = (u64)blockIdx.x * (blockDim.x >> 5) + wid;
+    const u64 g0 = w * share, g1 = g0 + share < total ? g0 + share : total;
+    int cur = -1, nwin = 0;
+    FWin mine{0, 0, 0, 0};
+    const u32 *in32 = nullptr;
+    ulonglong2 *o = nullptr;
+    for (u64 g = g0; g < g1; g++) {
+        const int st = (int)(g / ntiles);
+        const u32 t = (u32)(g - (u64)st * ntiles);
+        if (st != cur) {
+            cur = st;
+            nwin = compose_windows(r, s_arr ? s_arr[st] : s_uniform, tab, lane);
+            mine = lane < (u32)nwin ? tab[lane] : FWin{0, 0, 0, 0};
+            in32 = reinterpret_cast<const u32 *>(in + (size_t)st * stride);
+            o = reinterpret_cast<ulonglong2 *>(out + (size_t)st * stride);
         }
-#pragma unroll
-        for (int q = 0; q < UL; q++) {
-            const u32 u = u0 + lane + 32 * q;
-            if (u < nu) o[u] = interleave4(C[0][q], C[1][q], C[2][q], C[3][q]);
-        }
+        frob4_tile<UL>(in32, o, n32, nu, tab, nwin, mine, TWL * t, lane);
     }
 }
 
@@ -365,12 +418,29 @@ int launch_frob4(const u64 *in, u64 *out, size_t stride, int nstates, u64 r, con
     // each warp takes four warp tiles (the window set each CTA composes then
     // serves 32 tiles) when that still gives every SM two rounds of its 3
     // resident CTAs, else one (small states, r ~ 10^6)
-    const size_t ntile = (nu + TWL - 1) / TWL;
+    static const int variant = [] {
+        const char *e = getenv("GF2E_FROB4_VARIANT");
+        return e ? atoi(e) : 0;
+    }();
+    const int ul = variant == 1 ? 6 : variant == 2 ? 4 : UL_DEFAULT;
+    const size_t twl = 32 * (size_t)ul;
+    const size_t ntile = (nu + twl - 1) / twl;
     const bool four = (ntile + 31) / 32 * (size_t)nstates >= (size_t)6 * sm_count();
     size_t bx = four ? (ntile + 31) / 32 : (ntile + 7) / 8;
     if (bx > 65535) bx = 65535;
-    k_frob4_batch<<<dim3((unsigned)bx, (unsigned)nstates), 256, 0, st>>>(in, out, stride, r,
-                                                                      s_dev, s);
+    const dim3 grid((unsigned)bx, (unsigned)nstates);
+    if (variant == 3) {
+        k_frob4_persist<UL_DEFAULT, 3><<<3 * sm_count(), 256, 0, st>>>(in, out, stride, r, s_dev,
+                                                                      s, nstates);
+        GF2E_CHECK_LAUNCH("k_frob4_persist");
+        return GF2E_OK;
+    }
+    if (variant == 1)
+        k_frob4_batch<6, 4><<<grid, 256, 0, st>>>(in, out, stride, r, s_dev, s);
+    else if (variant == 2)
+        k_frob4_batch<4, 4><<<grid, 256, 0, st>>>(in, out, stride, r, s_dev, s);
+    else
+        k_frob4_batch<UL_DEFAULT, 3><<<grid, 256, 0, st>>>(in, out, stride, r, s_dev, s);
     GF2E_CHECK_LAUNCH("k_frob4_batch");
     return GF2E_OK;
 }
