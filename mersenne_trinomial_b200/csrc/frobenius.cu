@@ -30,10 +30,10 @@
 // window, XORed into the class accumulator C[c].  The unit's output is the
 // 4-way bit interleave of C[0..3] (bit 4 t + c = bit t of C[c]): cross-
 // register and in-register delta swaps, then a byte transpose by byte
-// permutes.  Lanes own units u0 + lane + 32 q, q < 8, so
+// permutes.  Lanes own units u0 + lane + 32 q, q < 6, so
 // loads and 16-byte stores are coalesced.
 //
-// Per warp tile of 256 units, one ballot lists the windows overlapping it and
+// Per warp tile of 192 units, one ballot lists the windows overlapping it and
 // those covering all of it.  The covering windows whose reads stay inside the
 // state are applied two at a time (both windows' 32 loads issued before
 // either is used) with no masks or bounds tests; the rest (windows that start
@@ -158,8 +158,12 @@ GF2E_DEV ulonglong2 interleave4(u32 c0, u32 c1, u32 c2, u32 c3) {
 }
 
 // ---- the pass: per warp tile, the overlapping windows, two at a time
-constexpr int UL_DEFAULT = 8;             // units per lane per warp tile (512 words a tile)
-
+// units per lane per warp tile (384 words a tile) and resident CTAs per SM:
+// measured at r = 136279841 x 64 states, 6 units at 4 CTAs beats 8 at 3 by
+// 1.2 % and 4 at 4 by 8 % (a persistent grid of contiguous tile shares was
+// 36 % slower than any of them)
+constexpr int LANE_UNITS = 6;
+constexpr int MIN_CTAS = 4;
 
 // A full window over all of the tile's units, every index inside the state:
 // lane l's units u0 + l + 32 q read input words first + l + 32 q and the
@@ -315,8 +319,7 @@ GF2E_DEV void frob4_tile(const u32 *__restrict__ in32, ulonglong2 *__restrict__ 
 // Batched F -> F^4 mod T (r < 2^31 - 2^16, even stride): blockIdx.y = state;
 // warp 0 composes the state's windows for the CTA, the warps stride over
 // its tiles.
-template <int UL, int MINB>
-__global__ void __launch_bounds__(256, MINB)
+__global__ void __launch_bounds__(256, MIN_CTAS)
 k_frob4_batch(const u64 *__restrict__ in, u64 *__restrict__ out, size_t stride, u64 r,
               const u64 *__restrict__ s_arr, u64 s_uniform) {
     __shared__ FWin tab[NCAND];
@@ -334,48 +337,11 @@ k_frob4_batch(const u64 *__restrict__ in, u64 *__restrict__ out, size_t stride, 
     const u32 *in32 = reinterpret_cast<const u32 *>(in + (size_t)st * stride);
     ulonglong2 *o = reinterpret_cast<ulonglong2 *>(out + (size_t)st * stride);
     const FWin mine = lane < (u32)nwin ? tab[lane] : FWin{0, 0, 0, 0};
-    constexpr u32 TWL = 32 * UL;
+    constexpr u32 TWL = 32 * LANE_UNITS;
     const u32 ntiles = (nu + TWL - 1) / TWL;
     const u32 warps_total = (gridDim.x * blockDim.x) >> 5;
     for (u32 t = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; t < ntiles; t += warps_total)
-        frob4_tile<UL>(in32, o, n32, nu, tab, nwin, mine, TWL * t, lane);
-}
-
-// The same pass as a persistent grid (a fixed number of CTAs): warp w takes
-// the w-th contiguous share of all (state, tile) pairs and composes its own
-// window table whenever its share moves to the next state.
-template <int UL, int MINB>
-__global__ void __launch_bounds__(256, MINB)
-k_frob4_persist(const u64 *__restrict__ in, u64 *__restrict__ out, size_t stride, u64 r,
-                const u64 *__restrict__ s_arr, u64 s_uniform, int nstates) {
-    __shared__ FWin tabs[8][NCAND];
-    const u32 lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    FWin *tab = tabs[wid];
-    const u32 nw = (u32)((r + 63) >> 6);
-    const u32 n32 = 2 * nw, nu = (nw + 1) >> 1;
-    constexpr u32 TWL = 32 * UL;
-    const u32 ntiles = (nu + TWL - 1) / TWL;
-    const u64 total = (u64)ntiles * (u64)nstates;
-    const u64 warps = (u64)((gridDim.x * blockDim.x) >> 5);
-    const u64 share = (total + warps - 1) / warps;
-    const u64 w = (u64)blockIdx.x * (blockDim.x >> 5) + wid;
-    const u64 g0 = w * share, g1 = g0 + share < total ? g0 + share : total;
-    int cur = -1, nwin = 0;
-    FWin mine{0, 0, 0, 0};
-    const u32 *in32 = nullptr;
-    ulonglong2 *o = nullptr;
-    for (u64 g = g0; g < g1; g++) {
-        const int st = (int)(g / ntiles);
-        const u32 t = (u32)(g - (u64)st * ntiles);
-        if (st != cur) {
-            cur = st;
-            nwin = compose_windows(r, s_arr ? s_arr[st] : s_uniform, tab, lane);
-            mine = lane < (u32)nwin ? tab[lane] : FWin{0, 0, 0, 0};
-            in32 = reinterpret_cast<const u32 *>(in + (size_t)st * stride);
-            o = reinterpret_cast<ulonglong2 *>(out + (size_t)st * stride);
-        }
-        frob4_tile<UL>(in32, o, n32, nu, tab, nwin, mine, TWL * t, lane);
-    }
+        frob4_tile<LANE_UNITS>(in32, o, n32, nu, tab, nwin, mine, TWL * t, lane);
 }
 
 }  // namespace
@@ -416,31 +382,15 @@ int launch_frob4(const u64 *in, u64 *out, size_t stride, int nstates, u64 r, con
     const size_t nw = (size_t)((r + 63) >> 6);
     const size_t nu = (nw + 1) / 2;
     // each warp takes four warp tiles (the window set each CTA composes then
-    // serves 32 tiles) when that still gives every SM two rounds of its 3
+    // serves 32 tiles) when that still gives every SM 1.5 rounds of its 4
     // resident CTAs, else one (small states, r ~ 10^6)
-    static const int variant = [] {
-        const char *e = getenv("GF2E_FROB4_VARIANT");
-        return e ? atoi(e) : 0;
-    }();
-    const int ul = variant == 1 ? 6 : variant == 2 ? 4 : UL_DEFAULT;
-    const size_t twl = 32 * (size_t)ul;
+    const size_t twl = 32 * (size_t)LANE_UNITS;
     const size_t ntile = (nu + twl - 1) / twl;
     const bool four = (ntile + 31) / 32 * (size_t)nstates >= (size_t)6 * sm_count();
     size_t bx = four ? (ntile + 31) / 32 : (ntile + 7) / 8;
     if (bx > 65535) bx = 65535;
     const dim3 grid((unsigned)bx, (unsigned)nstates);
-    if (variant == 3) {
-        k_frob4_persist<UL_DEFAULT, 3><<<3 * sm_count(), 256, 0, st>>>(in, out, stride, r, s_dev,
-                                                                      s, nstates);
-        GF2E_CHECK_LAUNCH("k_frob4_persist");
-        return GF2E_OK;
-    }
-    if (variant == 1)
-        k_frob4_batch<6, 4><<<grid, 256, 0, st>>>(in, out, stride, r, s_dev, s);
-    else if (variant == 2)
-        k_frob4_batch<4, 4><<<grid, 256, 0, st>>>(in, out, stride, r, s_dev, s);
-    else
-        k_frob4_batch<UL_DEFAULT, 3><<<grid, 256, 0, st>>>(in, out, stride, r, s_dev, s);
+    k_frob4_batch<<<grid, 256, 0, st>>>(in, out, stride, r, s_dev, s);
     GF2E_CHECK_LAUNCH("k_frob4_batch");
     return GF2E_OK;
 }

@@ -148,10 +148,15 @@ def case_hgcd_many(a):
         keep += [da, db]
         pairs.append((da, r, db, r + 1))
     M.stream_sync()
+    import resource
+    ru0 = resource.getrusage(resource.RUSAGE_SELF)
     t0 = time.perf_counter()
     degs, _, _ = M.gcd_large(pairs, max_parallel=n)
     dt = time.perf_counter() - t0
+    ru1 = resource.getrusage(resource.RUSAGE_SELF)
+    cpu = (ru1.ru_utime - ru0.ru_utime) + (ru1.ru_stime - ru0.ru_stime)
     print(f"hgcd_many: {n} x {r} bits in {dt:.1f} s, {dt / n:.2f} s per gcd, "
+          f"host cpu {cpu:.1f} s ({cpu / dt:.1f} cores of {os.cpu_count()}), "
           f"degrees {sorted(set(degs.tolist()))[:4]}")
 
 
