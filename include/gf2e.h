@@ -449,12 +449,16 @@ int gf2e_trin_accumulate(gf2e_trin *ctx, void *stream);
  * gf2_gcd_ntl.cpp:32-42; hybrid HGCD gf2_gcd_ntl.cpp:360-452) with the same
  * contract as gf2e_gcd_batch: deg_host[i] = deg gcd (0 means gcd = 1), and
  * the gcd itself in g_dev when it fits g_cap_words.  Operands are read, not
- * modified.  Each job runs the half-gcd recursion on its own stream and host
- * thread, up to max_parallel jobs at once (a single gcd is latency-bound;
- * independent ones overlap on the GPU).  Device memory comes from a private
- * stream-ordered pool (about 40 words per operand word per job in flight).
- * Synchronous: returns when every job is done.  stats (may be NULL) sums the
- * work counters of all jobs.
+ * modified.  max_parallel <= 1: one job after another.  max_parallel >= 2:
+ * lockstep batches of up to max_parallel jobs (at most 64, and as many as
+ * device memory holds): one host thread steps every member of a batch
+ * through the half-gcd recursion together, each launch (base cases, shifts,
+ * products, degree reads, division steps) serving all members with their
+ * own sizes, so launches and host round trips per gcd fall by the batch
+ * size.  Device memory comes from a private stream-ordered pool (about 40
+ * words per operand word per member, plus the transforms of the largest
+ * matrix product).  Synchronous: returns when every job is done.  stats (may
+ * be NULL) sums the work counters (in a batch, its steps count once).
  * ====================================================================== */
 typedef struct gf2e_hgcd_stats {
     int64_t nodes;            /* half-gcd calls */

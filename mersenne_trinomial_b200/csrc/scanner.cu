@@ -87,7 +87,7 @@ struct gf2e_scanner {
     struct GraphKey { int nact; const u64 *F; };
     std::vector<std::pair<GraphKey, cudaGraphExec_t>> graphs;
     bool use_graphs = true;
-    int gcd_parallel = 16;        // concurrent half-gcds at interval ends (large r)
+    int gcd_parallel = 64;        // half-gcds per lockstep batch at interval ends (large r)
     // blocked mode: m residues h per slot (slot j's at H + (j*m + t)*stride),
     // their squaring scratch, the block product C per slot, s per h state
     int m = 1;

@@ -326,7 +326,10 @@ def gcd_large(pairs, g_cap_words: int = 0, max_parallel: int = 1, stream=None):
     """Subquadratic (half-gcd) gcd of every (a_dev, abits, b_dev, bbits) pair,
     same contract as gcd_batch; for operands of millions of bits up to
     r = 136279841 (the reference delegates these to NTL, gf2_gcd_ntl.cpp:32-42).
-    Returns (degrees, gcds or None, work counters)."""
+    max_parallel >= 2 runs the pairs as lockstep batches of up to that many
+    (at most 64, and as many as device memory holds): one recursion, one
+    launch per step, for the whole batch.  Returns (degrees, gcds or None,
+    work counters; in a batch the step counters count batch steps)."""
     from ._lib import GcdJob, HgcdStats
     n = len(pairs)
     jobs = (GcdJob * n)()

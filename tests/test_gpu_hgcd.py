@@ -1,8 +1,11 @@
 """Subquadratic GPU gcd (half-gcd recursion) against the oracle's Euclid
 (gf2_gcd.h:48-75) and the quadratic GPU gcd: planted common factors, edge
 cases, scan accumulators against the trinomial, small thresholds that force
-deep recursion and FFT products, concurrent jobs, and the reference's
-known answer at r = 136279841 (s = 474: least factor 3991ef16129, degree 41)."""
+deep recursion and FFT products, lockstep batches (max_parallel >= 2: all
+jobs stepped through the recursion together, members of very different
+sizes and members that finish early) against one-at-a-time runs, and the
+reference's known answer at r = 136279841 (s = 474: least factor
+3991ef16129, degree 41)."""
 import os
 
 import numpy as np
@@ -65,9 +68,10 @@ def planted(oracle, rng, t, gd, ud, vd):
     return a, b
 
 
+@pytest.mark.parametrize("par", [1, 5])
 @pytest.mark.parametrize("base,small,fft", [(None, None, None), (256, 512, 2048),
                                             (512, 1024, 1 << 30), (4096, 8192, 4096)])
-def test_hgcd_planted_factors(engine, oracle, thresholds, base, small, fft):
+def test_hgcd_planted_factors(engine, oracle, thresholds, base, small, fft, par):
     thresholds(base, small, fft)
     rng = np.random.default_rng(11)
     arrays, want = [], []
@@ -76,7 +80,7 @@ def test_hgcd_planted_factors(engine, oracle, thresholds, base, small, fft):
         a, b = planted(oracle, rng, t, gd, ud, vd)
         arrays.append((a, 64 * a.size, b, 64 * b.size))
         want.append(oracle.poly_gcd(a, b))
-    degs, gs, st = run_pairs(engine, arrays, cap=1200)
+    degs, gs, st = run_pairs(engine, arrays, cap=1200, par=par)
     for (wd, wg), d, g in zip(want, degs.tolist(), gs):
         assert d == wd
         n = min(len(wg), len(g))
@@ -85,7 +89,10 @@ def test_hgcd_planted_factors(engine, oracle, thresholds, base, small, fft):
         assert st["nodes"] > st["base_cases"] > 0          # the recursion really ran
 
 
-def test_hgcd_edge_cases(engine, oracle, thresholds):
+@pytest.mark.parametrize("par", [1, 8])
+def test_hgcd_edge_cases(engine, oracle, thresholds, par):
+    """Units, zeros, x, equal operands, swapped orders, b | a; in a lockstep
+    batch these members finish at different steps."""
     thresholds(256, 512, 2048)
     one = np.array([1], dtype=np.uint64)
     zero = np.zeros(2, dtype=np.uint64)
@@ -102,11 +109,12 @@ def test_hgcd_edge_cases(engine, oracle, thresholds):
     for a, ab, b, bb in cases:
         arrays.append((a, ab, b, bb))
         want.append(oracle.poly_gcd(a, b)[0])
-    degs, _, _ = run_pairs(engine, arrays)
+    degs, _, _ = run_pairs(engine, arrays, par=par)
     assert degs.tolist() == want
 
 
-def test_hgcd_matches_quadratic_gpu_gcd_on_trinomials(engine, thresholds):
+@pytest.mark.parametrize("par", [1, 3])
+def test_hgcd_matches_quadratic_gpu_gcd_on_trinomials(engine, thresholds, par):
     """gcd(ACC, T) at r ~ 2*10^5 for running products like the scan's, half-gcd
     vs the quadratic Lehmer gcd (both GPU; the latter is pinned to the oracle)."""
     thresholds(2048, 4096, 1 << 17)
@@ -125,7 +133,7 @@ def test_hgcd_matches_quadratic_gpu_gcd_on_trinomials(engine, thresholds):
         acc = T.read("ACC")
         T.fini()
         arrays.append((acc, r, trinomial(r, s), r + 1))
-    degs, gs, _ = run_pairs(engine, arrays, cap=64)
+    degs, gs, _ = run_pairs(engine, arrays, cap=64, par=par)
     keep, pairs = [], []
     for a, ab, b, bb in arrays:
         da, db = engine.DeviceBuffer.from_array(a), engine.DeviceBuffer.from_array(b)
@@ -150,6 +158,41 @@ def test_hgcd_concurrent_jobs_match_serial(engine, oracle):
     assert d1.tolist() == d4.tolist()
     for x, y in zip(g1, g4):
         assert (x == y).all()
+
+
+def scan_accumulators(engine, r, ss, k1, k0):
+    arrays = []
+    for s in ss:
+        T = engine.TrinGPU()
+        T.init(r)
+        T.set_s(s)
+        T.set_x()
+        T.reset_acc()
+        for k in range(1, k1 + 1):
+            T.square_A()
+            if k >= k0:
+                T.accumulate()
+        arrays.append((T.read("ACC"), r, trinomial(r, s), r + 1))
+        T.fini()
+    return arrays
+
+
+def test_lockstep_matches_single_at_default_thresholds(engine):
+    """Eight interval gcds at r = 1000003 (default thresholds: base cases,
+    schoolbook and FFT products, all batched) in one lockstep batch and in
+    two batches of four, against one gcd at a time."""
+    r = 1000003
+    ss = [3, 12, 101, 4567, 33333, 77777, 250001, 499999]
+    arrays = scan_accumulators(engine, r, ss, 48, 20)
+    d1, g1, _ = run_pairs(engine, arrays, cap=64, par=1)
+    for par in (8, 4):
+        dp, gp, st = run_pairs(engine, arrays, cap=64, par=par)
+        assert dp.tolist() == d1.tolist(), par
+        for x, y in zip(g1, gp):
+            assert (x is None) == (y is None)
+            if x is not None:
+                assert (x == y).all()
+        assert st["base_cases"] > 0 and st["fft_products"] > 0
 
 
 @pytest.mark.timeout(900)
