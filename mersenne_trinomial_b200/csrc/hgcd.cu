@@ -23,14 +23,20 @@
 //   gcd(a, b): while deg b >= G0: M = hgcd(a, b); (a, b) = M (a, b); one
 //   division step.  Then the quadratic Lehmer gcd (gcd.cu) finishes.
 //
-// B200 mapping.  The recursion is host-driven on one stream per gcd; degrees
-// are read back with one small probe per node.  Products are sums of two
+// B200 mapping.  The recursion is host-driven on one stream; degrees are
+// read back with one small probe per node.  Products are sums of two
 // products (matrix x vector and matrix x matrix): a schoolbook carry-less
 // kernel split over output words and input chunks (atomicXor partials) below
 // a size threshold, the Cantor FFT above it (transforms of a and b shared by
-// both rows).  Temporaries come from a private stream-ordered memory pool.
-// A single gcd is latency-bound (the quotient sequence is sequential), so
-// independent gcds run concurrently, one host thread and stream each.
+// both rows).  Temporaries come from a per-gcd arena over a private
+// stream-ordered memory pool.  A single gcd is latency-bound (the quotient
+// sequence is sequential, and its base cases run on one SM each), so
+// independent gcds run as a lockstep batch (class HgcdBatch): one host
+// thread steps up to 64 of them through the recursion together, every
+// launch serving all members with their own sizes (the base cases as one
+// grid of a CTA per member, the transforms as batched FFTs).  Run one host
+// thread per gcd instead, 16 gcds of 136 Mbit kept 16 host cores busy on
+// stream waits and launches while the GPU idled between kernels.
 #include "gf2e_internal.cuh"
 
 #include <algorithm>
@@ -427,17 +433,20 @@ GF2E_DEV Lehmer lehmer_round(u64 wa, u64 wb, long long da, long long db, long lo
         // a <- a mod b, row a += q row b: at each of the dq + 1 degrees from
         // the top, XOR in b (and x^(dq-j) row b) when a's leading bit is set,
         // then move one degree down.  Afterwards bit 63 of A is degree dgb.
+        // At the top degree the bit is a's leading coefficient, always set.
         u32 s0 = mb0 << dq, s1 = mb1 << dq;
+        A ^= B;
+        ma0 ^= s0;
+        ma1 ^= s1;
 #pragma unroll 1
-        for (int j = 0;; j++) {
+        for (int j = 1; j <= dq; j++) {
+            A <<= 1;
+            s0 >>= 1;
+            s1 >>= 1;
             const u64 msk = (u64)((long long)A >> 63);
             A ^= B & msk;
             ma0 ^= s0 & (u32)msk;
             ma1 ^= s1 & (u32)msk;
-            if (j == dq) break;
-            A <<= 1;
-            s0 >>= 1;
-            s1 >>= 1;
         }
         const int c = A ? __clzll(A) : 64;
         const u64 Bn = A ? A << c : 0;
@@ -531,7 +540,6 @@ k_hgcd_base(const BaseBatch BB, u64 W, u64 mw, BaseAcc *acc) {
     __shared__ int s_va[2], s_vb[2], s_ra[2], s_mode[2], s_done[2], s_slow;
     __shared__ long long s_k[2], s_top[2], s_md[2];
     __shared__ u32 s_m[2][4];
-    __shared__ u64 s_tw[6];
     const int tid = threadIdx.x;
     for (u64 i = tid; i < 4 * W; i += BASE_THREADS) {
         u64 v = 0;
@@ -658,39 +666,38 @@ k_hgcd_base(const BaseBatch BB, u64 W, u64 mw, BaseAcc *acc) {
             }
         } else if (warp == 0) {
             // warp 0: the three top words of the new A (lanes 0-2) and B (3-5)
+            // in one pass (each lane with its own matrix row), then their
+            // degrees and the next windows by ballot and shuffle
             const int lane = tid;
-            if (lane < 6) {
-                const bool v = lane >= 3;
-                const long long w = top - (lane % 3);
-                u64 val = 0;
-                if (w >= 0)
-                    val = v ? new_word(mode, A, B, w, m2, m3, k, false)
-                            : new_word(mode, A, B, w, m0, m1, k, true);
-                s_tw[lane] = val;
+            const bool vb = lane >= 3;
+            const long long w = top - (lane % 3);
+            u64 val = 0;
+            if (lane < 6 && w >= 0)
+                val = new_word(mode, A, B, w, vb ? m2 : m0, vb ? m3 : m1, k, !vb);
+            const unsigned nz = __ballot_sync(0xffffffffu, lane < 6 && val != 0);
+            const int fa = __ffs(nz & 7u) - 1, fb = __ffs((nz >> 3) & 7u) - 1;
+            const u64 ta = __shfl_sync(0xffffffffu, val, fa < 0 ? 0 : fa);
+            const u64 tb = __shfl_sync(0xffffffffu, val, fb < 0 ? 3 : 3 + fb);
+            const long long dn0 = fa < 0 ? -1 : (top - fa) * 64 + 63 - __clzll(ta);
+            const long long dn1 = fb < 0 ? -1 : (top - fb) * 64 + 63 - __clzll(tb);
+            bool slow = dn0 < 0 || dn1 < 0;
+            long long lo = 0;
+            if (!slow) {
+                const long long dhi = max(dn0, dn1);
+                lo = dhi >= 63 ? dhi - 63 : 0;
+                slow = (lo >> 6) < top - 2;
             }
-            __syncwarp();
+            // the windows' low words are words lo/64 (lane top - lo/64) and
+            // lo/64 + 1 (one lane lower) of the new vectors
+            const int ia = slow ? 0 : (int)(top - (lo >> 6));
+            const int ib = ia >= 1 ? ia - 1 : 0;
+            const u64 x0a = __shfl_sync(0xffffffffu, val, ia), x1a = __shfl_sync(0xffffffffu, val, ib);
+            const u64 x0b = __shfl_sync(0xffffffffu, val, 3 + ia), x1b = __shfl_sync(0xffffffffu, val, 3 + ib);
             if (lane == 0) {
-                long long dn[2] = {-1, -1};
-                for (int v = 0; v < 2; v++)
-                    for (int i = 0; i < 3 && dn[v] < 0; i++)
-                        if (s_tw[3 * v + i]) dn[v] = (top - i) * 64 + 63 - __clzll(s_tw[3 * v + i]);
-                bool slow = dn[0] < 0 || dn[1] < 0;
                 if (!slow) {
-                    const long long dhi = max(dn[0], dn[1]);
-                    const long long lo = dhi >= 63 ? dhi - 63 : 0;
-                    const long long i0 = lo >> 6;
-                    slow = i0 < top - 2;
-                    if (!slow) {
-                        u64 wn[2];
-                        const unsigned sb = (unsigned)(lo & 63);
-                        for (int v = 0; v < 2; v++) {
-                            const u64 x0 = s_tw[3 * v + (int)(top - i0)];
-                            const u64 x1 = (i0 + 1 <= top) ? s_tw[3 * v + (int)(top - i0 - 1)] : 0;
-                            wn[v] = funnel64(x0, x1, sb);
-                        }
-                        publish(q, spare[0], spare[1], 0, dn[0], dn[1], wn[0], wn[1], md_next,
-                                round + 1);
-                    }
+                    const unsigned sb = (unsigned)(lo & 63);
+                    publish(q, spare[0], spare[1], 0, dn0, dn1, funnel64(x0a, ia >= 1 ? x1a : 0, sb),
+                            funnel64(x0b, ia >= 1 ? x1b : 0, sb), md_next, round + 1);
                 }
                 s_slow = slow;
             }
@@ -752,15 +759,27 @@ public:
     Arena(const Arena &) = delete;
     Arena &operator=(const Arena &) = delete;
 
+    // size classes 2^e (1 + j/4), j = 0..3, e >= 6: a block wastes under a
+    // fifth of its size (lockstep batches make single buffers of GBs)
+    static size_t class_words(int cls) {
+        const int e = cls >> 2, j = cls & 3;
+        return ((size_t)1 << e) + (size_t)j * ((size_t)1 << (e - 2));
+    }
+    static int class_of(size_t words) {
+        int e = 6;
+        while (((size_t)1 << (e + 1)) < words) e++;
+        int cls = 4 * e;
+        while (class_words(cls) < words) cls++;
+        return cls;
+    }
     u64 *get(size_t words, int &cls) {
-        cls = 6;                                   // at least 64 words
-        while (((size_t)1 << cls) < words) cls++;
+        cls = class_of(words);
         if (!free_[cls].empty()) {
             u64 *p = free_[cls].back();
             free_[cls].pop_back();
             return p;
         }
-        const size_t need = (size_t)1 << cls;
+        const size_t need = class_words(cls);
         if (left_ < need) {
             const size_t chunk = std::max(need, (size_t)1 << 22);    // 32 MB or the block
             void *c = nullptr;
@@ -781,7 +800,7 @@ private:
     cudaStream_t st_;
     cudaMemPool_t pool_;
     std::vector<u64 *> chunks_;
-    std::vector<u64 *> free_[64];
+    std::vector<u64 *> free_[4 * 64];
     u64 *cur_ = nullptr;
     size_t left_ = 0;
 };
@@ -849,8 +868,14 @@ struct Tunables {
     long long small_gcd_bits = 1 << 15;  // finish with the quadratic gcd below this
 };
 
-Tunables tunables() {
+// A lockstep batch fills the GPU with every product, so the FFT's lower
+// work pays from smaller sizes than for one gcd, whose small products leave
+// most SMs idle either way (measured, 64 gcds of 16 Mbit at once: 6.3 s
+// with the FFT from 2^15 bits, 6.5 s from 2^16, 7.5 s from 2^17, 8.3 s from
+// 2^18, 11.7 s from 2^19, 17.2 s from 2^20).
+Tunables tunables(bool lockstep = false) {
     Tunables t;
+    if (lockstep) t.fft_bits = 1 << 16;
     if (const char *e = getenv("GF2E_HGCD_BASE_BITS")) t.base_bits = atoll(e);
     if (const char *e = getenv("GF2E_HGCD_FFT_BITS")) t.fft_bits = atoll(e);
     if (const char *e = getenv("GF2E_HGCD_SMALL_BITS")) t.small_gcd_bits = atoll(e);
@@ -1379,7 +1404,7 @@ struct BMat {
 class HgcdBatch {
 public:
     HgcdBatch(int G, cudaStream_t st, cudaMemPool_t pool)
-        : arena_(st, pool), G_(G), st_(st), tn_(tunables()) {
+        : arena_(st, pool), G_(G), st_(st), tn_(tunables(true)) {
         ckc(cudaMallocHost(&h_probe_, (size_t)GMAX * 8 * sizeof(long long)), "hgcd probe host buffer");
         d_probe_ = alloc(GMAX * 8);
         d_res_ = alloc(8);
@@ -2137,8 +2162,9 @@ int run_one(const gf2e_gcd_job &j, int64_t *deg_out, gf2e_hgcd_stats *stats, cud
 
 // members per lockstep batch: the caller's cap, GMAX, and what device
 // memory holds (per member about 40 operand-sized buffers and the 12
-// transforms of the largest matrix product)
-int batch_size(const gf2e_gcd_job *jobs, int njobs, int max_parallel) {
+// transforms of the largest matrix product), counting as free what the
+// gcd pool holds from earlier gcds but does not use
+int batch_size(cudaMemPool_t pool, const gf2e_gcd_job *jobs, int njobs, int max_parallel) {
     u64 bits = 1;
     for (int i = 0; i < njobs; i++) bits = std::max(bits, std::max(jobs[i].abits, jobs[i].bbits));
     const u64 words = (bits + 63) / 64;
@@ -2147,8 +2173,14 @@ int batch_size(const gf2e_gcd_job *jobs, int njobs, int max_parallel) {
     const double per = 8.0 * (40.0 * (double)words + 12.0 * (double)n);
     size_t fr = 0, tot = 0;
     int cap = GMAX;
-    if (cudaMemGetInfo(&fr, &tot) == cudaSuccess)
-        cap = (int)std::max(1.0, std::min((double)GMAX, 0.6 * (double)fr / per));
+    if (cudaMemGetInfo(&fr, &tot) == cudaSuccess) {
+        unsigned long long reserved = 0, used = 0;
+        if (cudaMemPoolGetAttribute(pool, cudaMemPoolAttrReservedMemCurrent, &reserved) == cudaSuccess &&
+            cudaMemPoolGetAttribute(pool, cudaMemPoolAttrUsedMemCurrent, &used) == cudaSuccess &&
+            reserved > used)
+            fr += (size_t)(reserved - used);
+        cap = (int)std::max(1.0, std::min((double)GMAX, 0.8 * (double)fr / per));
+    }
     return std::max(1, std::min(std::min(njobs, max_parallel), cap));
 }
 
@@ -2178,7 +2210,7 @@ int run_lockstep(const gf2e_gcd_job *jobs, int njobs, int64_t *deg_host, int max
     if (e != cudaSuccess) return gf2e::cuda_status(e, "hgcd stream");
     int rc = GF2E_OK;
     if (stats) memset(stats, 0, sizeof *stats);
-    const int B = batch_size(jobs, njobs, max_parallel);
+    const int B = batch_size(pool, jobs, njobs, max_parallel);
     for (int i0 = 0; i0 < njobs && rc == GF2E_OK; i0 += B) {
         const int nb = std::min(B, njobs - i0);
         try {
