@@ -34,9 +34,11 @@
 // independent gcds run as a lockstep batch (class HgcdBatch): one host
 // thread steps up to 64 of them through the recursion together, every
 // launch serving all members with their own sizes (the base cases as one
-// grid of a CTA per member, the transforms as batched FFTs).  Run one host
-// thread per gcd instead, 16 gcds of 136 Mbit kept 16 host cores busy on
-// stream waits and launches while the GPU idled between kernels.
+// grid of a CTA per member, the transforms as batched FFTs); two such
+// batches run at once on two streams, one's base cases overlapping the
+// other's products.  Run one host thread per gcd instead, 16 gcds of 136
+// Mbit kept 16 host cores busy on stream waits and launches while the GPU
+// idled between kernels.
 #include "gf2e_internal.cuh"
 
 #include <algorithm>
@@ -45,6 +47,7 @@
 #include <cstring>
 #include <memory>
 #include <mutex>
+#include <thread>
 #include <vector>
 
 namespace gf2e {
@@ -783,7 +786,13 @@ public:
         if (left_ < need) {
             const size_t chunk = std::max(need, (size_t)1 << 22);    // 32 MB or the block
             void *c = nullptr;
-            ckc_arena(cudaMallocFromPoolAsync(&c, chunk * 8, pool_, st_));
+            const cudaError_t e = cudaMallocFromPoolAsync(&c, chunk * 8, pool_, st_);
+            if (e == cudaErrorMemoryAllocation) {      // not sticky: the caller may retry smaller
+                cudaGetLastError();
+                gf2e::set_error("hgcd pool allocation: out of device memory");
+                throw Fail{GF2E_ERR_NOMEM};
+            }
+            ckc_arena(e);
             chunks_.push_back((u64 *)c);
             cur_ = (u64 *)c;
             left_ = chunk;
@@ -866,6 +875,7 @@ struct Tunables {
     long long base_bits = 1 << 14;       // n <= base_bits: one-CTA base kernel
     long long fft_bits = 1 << 19;        // products above this many bits use the FFT
     long long small_gcd_bits = 1 << 15;  // finish with the quadratic gcd below this
+    int streams = 2;                     // lockstep batches run at once
 };
 
 // A lockstep batch fills the GPU with every product, so the FFT's lower
@@ -879,6 +889,7 @@ Tunables tunables(bool lockstep = false) {
     if (const char *e = getenv("GF2E_HGCD_BASE_BITS")) t.base_bits = atoll(e);
     if (const char *e = getenv("GF2E_HGCD_FFT_BITS")) t.fft_bits = atoll(e);
     if (const char *e = getenv("GF2E_HGCD_SMALL_BITS")) t.small_gcd_bits = atoll(e);
+    if (const char *e = getenv("GF2E_HGCD_STREAMS")) t.streams = std::max(1, atoi(e));
     t.base_bits = std::max(256LL, std::min(t.base_bits, 1LL << 16));
     t.small_gcd_bits = std::max(t.small_gcd_bits, 2 * t.base_bits);
     return t;
@@ -1779,17 +1790,16 @@ private:
         gf2e_fft_plan *plan = gf2e::cached_plan(fft_m(need));
         if (!plan) throw Fail{GF2E_ERR_CUDA};
         const u64 n = gf2e::fft_plan_n(plan);
-        Buf Fa = alloc(G_ * n), Fb = alloc(G_ * n), Fm[4];
+        Buf Fa = alloc(G_ * n), Fb = alloc(G_ * n);
         fwd(plan, a, Fa->p, n);
         fwd(plan, b, Fb->p, n);
-        for (int i = 0; i < 4; i++) {
-            Fm[i] = alloc(G_ * n);
-            fwd(plan, M.e[i], Fm[i]->p, n);
+        for (int row = 0; row < 2; row++) {     // one row's transforms live at a time
+            Buf F0 = alloc(G_ * n), F1 = alloc(G_ * n);
+            fwd(plan, M.e[2 * row], F0->p, n);
+            fwd(plan, M.e[2 * row + 1], F1->p, n);
+            (row ? d : c) = product_out(plan, F0->p, F0->p, Fa->p, F1->p, Fb->p, n, need,
+                                        sum_bound(M.e[2 * row], a, M.e[2 * row + 1], b));
         }
-        c = product_out(plan, Fm[0]->p, Fm[0]->p, Fa->p, Fm[1]->p, Fb->p, n, need,
-                        sum_bound(M.e[0], a, M.e[1], b));
-        d = product_out(plan, Fm[2]->p, Fm[2]->p, Fa->p, Fm[3]->p, Fb->p, n, need,
-                        sum_bound(M.e[2], a, M.e[3], b));
         stats.fft_mul2 += 2;
     }
 
@@ -2160,10 +2170,10 @@ int run_one(const gf2e_gcd_job &j, int64_t *deg_out, gf2e_hgcd_stats *stats, cud
     }
 }
 
-// members per lockstep batch: the caller's cap, GMAX, and what device
-// memory holds (per member about 40 operand-sized buffers and the 12
-// transforms of the largest matrix product), counting as free what the
-// gcd pool holds from earlier gcds but does not use
+// members in flight: the caller's cap, GMAX, and what device memory holds
+// (per member about 40 operand-sized buffers and 12 transforms of the
+// largest matrix product: 1.52 GB measured at r = 136279841), counting as
+// free what the gcd pool holds from earlier gcds but does not use
 int batch_size(cudaMemPool_t pool, const gf2e_gcd_job *jobs, int njobs, int max_parallel) {
     u64 bits = 1;
     for (int i = 0; i < njobs; i++) bits = std::max(bits, std::max(jobs[i].abits, jobs[i].bbits));
@@ -2179,7 +2189,7 @@ int batch_size(cudaMemPool_t pool, const gf2e_gcd_job *jobs, int njobs, int max_
             cudaMemPoolGetAttribute(pool, cudaMemPoolAttrUsedMemCurrent, &used) == cudaSuccess &&
             reserved > used)
             fr += (size_t)(reserved - used);
-        cap = (int)std::max(1.0, std::min((double)GMAX, 0.8 * (double)fr / per));
+        cap = (int)std::max(1.0, std::min((double)GMAX, 0.9 * (double)fr / per));
     }
     return std::max(1, std::min(std::min(njobs, max_parallel), cap));
 }
@@ -2200,29 +2210,67 @@ void add_stats(gf2e_hgcd_stats &t, const Stats &s) {
     t.base_cycles_total += s.cyc_total;
 }
 
-// lockstep batches, one after another on one stream
+// lockstep batches: the members in flight (the memory cap) split over
+// `streams` batches that run at once, each on its own host thread and
+// stream, so that one batch's base cases (a CTA per member, most SMs idle)
+// overlap another's products; further batches follow as these finish
 int run_lockstep(const gf2e_gcd_job *jobs, int njobs, int64_t *deg_host, int max_parallel,
                  gf2e_hgcd_stats *stats) {
     cudaMemPool_t pool = hgcd_pool();
     if (!pool) return gf2e::cuda_status(cudaErrorMemoryAllocation, "hgcd memory pool");
-    cudaStream_t st;
-    cudaError_t e = cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
-    if (e != cudaSuccess) return gf2e::cuda_status(e, "hgcd stream");
-    int rc = GF2E_OK;
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return gf2e::cuda_status(e, "hgcd device");
     if (stats) memset(stats, 0, sizeof *stats);
     const int B = batch_size(pool, jobs, njobs, max_parallel);
-    for (int i0 = 0; i0 < njobs && rc == GF2E_OK; i0 += B) {
-        const int nb = std::min(B, njobs - i0);
-        try {
-            HgcdBatch H(nb, st, pool);
-            H.run(jobs + i0, deg_host + i0);
-            if (stats) add_stats(*stats, H.stats);
-        } catch (const Fail &f) {
-            cudaStreamSynchronize(st);
-            rc = f.st;
+    const int lanes = std::max(1, std::min(tunables(true).streams, B / 8));
+    const int per = (B + lanes - 1) / lanes;
+    std::atomic<int> next(0);
+    std::mutex mu;
+    int rc = GF2E_OK;
+    auto worker = [&]() {
+        cudaSetDevice(dev);
+        cudaStream_t st;
+        cudaError_t ce = cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
+        if (ce != cudaSuccess) {
+            std::lock_guard<std::mutex> lk(mu);
+            rc = gf2e::cuda_status(ce, "hgcd stream");
+            return;
         }
+        // a batch that runs out of device memory (the other batch in flight,
+        // or the estimate) is retried as two halves
+        auto run_members = [&](auto &&self, int i0, int nb) -> int {
+            try {
+                HgcdBatch H(nb, st, pool);
+                H.run(jobs + i0, deg_host + i0);
+                std::lock_guard<std::mutex> lk(mu);
+                if (stats) add_stats(*stats, H.stats);
+                return GF2E_OK;
+            } catch (const Fail &f) {
+                cudaStreamSynchronize(st);
+                if (f.st != GF2E_ERR_NOMEM || nb == 1) return f.st;
+            }
+            const int h = nb / 2;
+            const int r1 = self(self, i0, h);
+            return r1 != GF2E_OK ? r1 : self(self, i0 + h, nb - h);
+        };
+        for (int b; (b = next.fetch_add(1)) * per < njobs;) {
+            const int i0 = b * per;
+            const int r1 = run_members(run_members, i0, std::min(per, njobs - i0));
+            if (r1 != GF2E_OK) {
+                std::lock_guard<std::mutex> lk(mu);
+                if (rc == GF2E_OK) rc = r1;
+            }
+        }
+        cudaStreamDestroy(st);
+    };
+    if (lanes == 1) {
+        worker();
+    } else {
+        std::vector<std::thread> th;
+        for (int t = 0; t < lanes; t++) th.emplace_back(worker);
+        for (auto &t : th) t.join();
     }
-    cudaStreamDestroy(st);
     return rc;
 }
 

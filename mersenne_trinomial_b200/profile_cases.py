@@ -149,14 +149,19 @@ def case_hgcd_many(a):
         pairs.append((da, r, db, r + 1))
     M.stream_sync()
     import resource
+    import torch
+    free0 = torch.cuda.mem_get_info()[0]
     ru0 = resource.getrusage(resource.RUSAGE_SELF)
     t0 = time.perf_counter()
     degs, _, _ = M.gcd_large(pairs, max_parallel=n)
     dt = time.perf_counter() - t0
     ru1 = resource.getrusage(resource.RUSAGE_SELF)
     cpu = (ru1.ru_utime - ru0.ru_utime) + (ru1.ru_stime - ru0.ru_stime)
+    # the gcd memory pool keeps what it reserved: its high-water mark
+    pool = free0 - torch.cuda.mem_get_info()[0]
     print(f"hgcd_many: {n} x {r} bits in {dt:.1f} s, {dt / n:.2f} s per gcd, "
           f"host cpu {cpu:.1f} s ({cpu / dt:.1f} cores of {os.cpu_count()}), "
+          f"pool {pool / 2**30:.1f} GiB ({pool / n / 2**20:.0f} MiB a gcd), "
           f"degrees {sorted(set(degs.tolist()))[:4]}")
 
 

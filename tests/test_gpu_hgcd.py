@@ -178,14 +178,16 @@ def scan_accumulators(engine, r, ss, k1, k0):
 
 
 def test_lockstep_matches_single_at_default_thresholds(engine):
-    """Eight interval gcds at r = 1000003 (default thresholds: base cases,
-    schoolbook and FFT products, all batched) in one lockstep batch and in
-    two batches of four, against one gcd at a time."""
+    """Sixteen interval gcds at r = 1000003 (default thresholds: base cases,
+    schoolbook and FFT products, all batched) as two lockstep batches of
+    eight running at once on two streams, as one batch of eight after
+    another, and as batches of four, against one gcd at a time."""
     r = 1000003
-    ss = [3, 12, 101, 4567, 33333, 77777, 250001, 499999]
+    ss = [3, 12, 101, 4567, 33333, 77777, 250001, 499999,
+          5, 77, 1234, 9999, 123457, 300007, 444443, 499001]
     arrays = scan_accumulators(engine, r, ss, 48, 20)
     d1, g1, _ = run_pairs(engine, arrays, cap=64, par=1)
-    for par in (8, 4):
+    for par in (16, 8, 4):
         dp, gp, st = run_pairs(engine, arrays, cap=64, par=par)
         assert dp.tolist() == d1.tolist(), par
         for x, y in zip(g1, gp):
