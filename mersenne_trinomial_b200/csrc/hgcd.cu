@@ -82,111 +82,6 @@ GF2E_DEV void clmul64(u64 a, u64 b, u64 &lo, u64 &hi) {
 
 GF2E_DEV int deg64(u64 v) { return v ? 63 - __clzll(v) : -1; }
 
-// degree and the 64-bit top window (bit 63 = leading coefficient) of up to
-// four polynomials; warp w scans polynomial w downwards from word nw-1
-struct ProbeArgs {
-    const u64 *p[4];
-    u64 nw[4];
-};
-__global__ void k_probe(ProbeArgs a, int np, long long *out) {
-    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    if (w >= np) return;
-    const u64 *X = a.p[w];
-    long long top = -1;
-    for (long long base = (long long)a.nw[w] - 1; base >= 0 && top < 0; base -= 32) {
-        long long i = base - lane;
-        u64 v = (i >= 0) ? X[i] : 0;
-        unsigned ball = __ballot_sync(0xffffffffu, v != 0);
-        if (ball) top = base - (__ffs(ball) - 1);
-    }
-    if (lane == 0) {
-        long long deg = -1;
-        u64 win = 0;
-        if (top >= 0) {
-            const u64 hiw = X[top];
-            const int t = 63 - __clzll(hiw);
-            deg = top * 64 + t;
-            win = hiw << (63 - t);
-            if (t < 63 && top > 0) win |= X[top - 1] >> (t + 1);
-        }
-        out[2 * w] = deg;
-        out[2 * w + 1] = (long long)win;
-    }
-}
-
-// dst = src quo x^k (dst has nd words)
-__global__ void k_shr(const u64 *__restrict__ src, u64 ns, u64 k, u64 *__restrict__ dst, u64 nd) {
-    const u64 ks = k >> 6;
-    const unsigned kb = (unsigned)(k & 63);
-    for (u64 w = (u64)blockIdx.x * blockDim.x + threadIdx.x; w < nd;
-         w += (u64)gridDim.x * blockDim.x) {
-        u64 lo = (w + ks < ns) ? src[w + ks] : 0, hi = (w + ks + 1 < ns) ? src[w + ks + 1] : 0;
-        dst[w] = funnel64(lo, hi, kb);
-    }
-}
-
-// out = x1*y1 + x2*y2 (schoolbook).  Thread = two adjacent output words,
-// blockIdx.y = a chunk of the x index; partial sums are XORed into out,
-// which must be zero on entry.
-struct Mul2Jobs {                       // up to four sums of two products, blockIdx.z = job
-    const u64 *x1[4], *y1[4], *x2[4], *y2[4];
-    u64 nx1[4], ny1[4], nx2[4], ny2[4];
-    unsigned long long *out[4];
-    u64 nout[4];
-};
-__global__ void k_mul2(const Mul2Jobs J, u64 chunk) {
-    const int z = blockIdx.z;
-    const u64 *__restrict__ x1 = J.x1[z], *__restrict__ y1 = J.y1[z];
-    const u64 *__restrict__ x2 = J.x2[z], *__restrict__ y2 = J.y2[z];
-    const u64 nx1 = J.nx1[z], ny1 = J.ny1[z], nx2 = J.nx2[z], ny2 = J.ny2[z];
-    unsigned long long *__restrict__ out = J.out[z];
-    const u64 nout = J.nout[z];
-    const u64 w = 2 * ((u64)blockIdx.x * blockDim.x + threadIdx.x);
-    if (w >= nout) return;
-    const u64 i0 = (u64)blockIdx.y * chunk;
-    u64 r0 = 0, r1 = 0;
-    for (int pr = 0; pr < 2; pr++) {
-        const u64 *x = pr ? x2 : x1, *y = pr ? y2 : y1;
-        const u64 nx = pr ? nx2 : nx1, ny = pr ? ny2 : ny1;
-        if (!x || !nx || !ny) continue;
-        const u64 i1 = min(nx, i0 + chunk);
-        for (u64 i = i0; i < i1; i++) {
-            const u64 xi = x[i];
-            if (!xi) continue;
-            u64 lo, hi;
-            // j = w-1-i: hi -> word w
-            if (w >= i + 1 && w - 1 - i < ny) { clmul64(xi, y[w - 1 - i], lo, hi); r0 ^= hi; }
-            // j = w-i: lo -> w, hi -> w+1
-            if (w >= i && w - i < ny) { clmul64(xi, y[w - i], lo, hi); r0 ^= lo; r1 ^= hi; }
-            // j = w+1-i: lo -> w+1
-            if (w + 1 >= i && w + 1 - i < ny) { clmul64(xi, y[w + 1 - i], lo, hi); r1 ^= lo; }
-        }
-    }
-    if (r0) atomicXor(out + w, (unsigned long long)r0);
-    if (r1 && w + 1 < nout) atomicXor(out + w + 1, (unsigned long long)r1);
-}
-
-// out = x ^ ((q * y) << s) for out words [0, nout); x read below nx (x may be out)
-__global__ void k_axpy_q(u64 *out, u64 nout, const u64 *x, u64 nx, const u64 *__restrict__ y,
-                         u64 ny, u64 q, u64 s) {
-    const u64 sw = s >> 6;
-    const unsigned sb = (unsigned)(s & 63);
-    for (u64 w = (u64)blockIdx.x * blockDim.x + threadIdx.x; w < nout;
-         w += (u64)gridDim.x * blockDim.x) {
-        // word j of P = q*y: lo(q*y[j]) ^ hi(q*y[j-1])
-        auto Pw = [&](long long j) -> u64 {
-            if (j < 0 || j > (long long)ny) return 0;
-            u64 v = 0, lo, hi;
-            if (j < (long long)ny) { clmul64(q, y[j], lo, hi); v ^= lo; }
-            if (j >= 1) { clmul64(q, y[j - 1], lo, hi); v ^= hi; }
-            return v;
-        };
-        const long long j = (long long)w - (long long)sw;
-        u64 sh = sb ? ((Pw(j) << sb) | (Pw(j - 1) >> (64 - sb))) : Pw(j);
-        out[w] = (w < nx ? x[w] : 0) ^ sh;
-    }
-}
-
 // out = X1*Y1 ^ X2*Y2 pointwise in GF(2^64)
 __global__ void k_pw_muladd(u64 *out, const u64 *x1,
                             const u64 *__restrict__ y1, const u64 *__restrict__ x2,
@@ -261,8 +156,9 @@ __global__ void k_shr_b(const ShrBatch B) {
     }
 }
 
-// up to four sums x1*y1 + x2*y2 per member (schoolbook, as k_mul2);
-// blockIdx.z = job * G + member; outputs zero on entry
+// up to four sums x1*y1 + x2*y2 per member (schoolbook): thread = two
+// adjacent output words, blockIdx.y = a chunk of the x index (partial sums
+// XORed into the output, zero on entry), blockIdx.z = job * G + member
 struct Mul2Batch {
     const u64 *x1[4], *y1[4], *x2[4], *y2[4];
     u64 sx1[4], sy1[4], sx2[4], sy2[4];
@@ -855,22 +751,6 @@ void base_smem_attr() {
     }
 }
 
-// polynomial on the device: deg exact for remainders, an upper bound for
-// matrix entries (words() covers every nonzero word either way)
-struct Poly {
-    Buf b;
-    long long deg = -1;
-    u64 win = 0;          // top 64 bits aligned at deg, valid when has_win
-    bool has_win = false;
-    u64 *p() const { return b ? b->p : nullptr; }
-    u64 words() const { return deg < 0 ? 0 : (u64)(deg >> 6) + 1; }
-};
-
-struct Mat {
-    Poly e[4];          // M00 M01 M10 M11
-    bool ident = false;
-};
-
 struct Tunables {
     long long base_bits = 1 << 14;       // n <= base_bits: one-CTA base kernel
     long long fft_bits = 1 << 19;        // products above this many bits use the FFT
@@ -909,457 +789,6 @@ struct Timer {
     ~Timer() {
         acc += std::chrono::duration<double, std::micro>(std::chrono::steady_clock::now() - t0).count();
     }
-};
-
-class Hgcd {
-public:
-    Hgcd(cudaStream_t st, cudaMemPool_t pool)
-        : arena_(st, pool), st_(st), pool_(pool), tn_(tunables()) {
-        ckc(cudaMallocHost(&h_probe_, 16 * sizeof(long long)), "hgcd probe host buffer");
-        d_probe_ = alloc(16);
-        d_res_ = alloc(8);
-        ckc(cudaMemsetAsync(d_res_->p, 0, sizeof(BaseAcc), st_), "hgcd base accumulator");
-    }
-
-    // read the base-case totals; a failed base case fails the gcd
-    void finish_bases() {
-        BaseAcc acc;
-        ckc(cudaMemcpyAsync(&acc, d_res_->p, sizeof acc, cudaMemcpyDeviceToHost, st_), "base totals");
-        ckc(cudaStreamSynchronize(st_), "base totals sync");
-        stats.base_rounds = (long long)acc.rounds;
-        stats.cyc_serial = (long long)acc.cyc_serial;
-        stats.cyc_total = (long long)acc.cyc_total;
-        if (acc.worst != GF2E_OK) {
-            gf2e::set_error("hgcd base case status %d", acc.worst);
-            throw Fail{acc.worst};
-        }
-    }
-    ~Hgcd() {
-        if (h_probe_) cudaFreeHost(h_probe_);
-    }
-    Stats stats;
-
-    Buf alloc(size_t words) {
-        auto b = std::make_shared<DBuf>();
-        b->st = st_;
-        b->words = std::max<size_t>(words, 1);
-        b->p = arena_.get(b->words, b->cls);
-        b->arena = &arena_;
-        return b;
-    }
-    Poly zeros(size_t words) {
-        Poly r;
-        r.b = alloc(words);
-        ckc(cudaMemsetAsync(r.b->p, 0, r.b->words * 8, st_), "hgcd memset");
-        return r;
-    }
-    Poly from_device(const u64 *src, u64 bits) {
-        const size_t nw = (size_t)((bits + 63) >> 6);
-        Poly r = zeros(nw + 1);
-        if (nw) ckc(cudaMemcpyAsync(r.p(), src, nw * 8, cudaMemcpyDeviceToDevice, st_), "hgcd copy");
-        r.deg = (long long)nw * 64 - 1;    // bound until probed
-        probe({&r});
-        return r;
-    }
-    Poly constant1() {
-        Poly r = zeros(1);
-        u64 one = 1;
-        ckc(cudaMemcpyAsync(r.p(), &one, 8, cudaMemcpyHostToDevice, st_), "hgcd const");
-        ckc(cudaStreamSynchronize(st_), "hgcd const sync");
-        r.deg = 0;
-        return r;
-    }
-
-    // exact degrees (and top windows) of up to four polynomials whose
-    // current deg is an upper bound
-    void probe(std::initializer_list<Poly *> ps, u64 *wins = nullptr) {
-        ProbeArgs a;
-        memset(&a, 0, sizeof a);
-        int n = 0;
-        for (Poly *p : ps) {
-            a.p[n] = p->p();
-            a.nw[n] = p->p() ? p->words() : 0;
-            n++;
-        }
-        k_probe<<<1, 32 * n, 0, st_>>>(a, n, (long long *)d_probe_->p);
-        ckc(cudaGetLastError(), "k_probe");
-        ckc(cudaMemcpyAsync(h_probe_, d_probe_->p, 2 * n * sizeof(long long),
-                            cudaMemcpyDeviceToHost, st_), "probe read");
-        ckc(cudaStreamSynchronize(st_), "probe sync");
-        stats.probes++;
-        int i = 0;
-        for (Poly *p : ps) {
-            p->deg = h_probe_[2 * i];
-            p->win = (u64)h_probe_[2 * i + 1];
-            p->has_win = true;
-            if (wins) wins[i] = p->win;
-            i++;
-        }
-    }
-
-    Poly shr(const Poly &x, long long k) {
-        Poly r;
-        if (x.deg < k) { r.deg = -1; r.b = alloc(1); return r; }
-        r.deg = x.deg - k;
-        const u64 nd = r.words();
-        r.b = alloc(nd);
-        k_shr<<<gf2e::grid_for(nd, 256), 256, 0, st_>>>(x.p(), x.words(), (u64)k, r.p(), nd);
-        ckc(cudaGetLastError(), "k_shr");
-        return r;
-    }
-
-    // up to four sums x1*y1 + x2*y2 in one schoolbook launch (one zeroed
-    // buffer for all outputs); degrees of the results are bounds
-    struct Pair { const Poly *x1, *y1, *x2, *y2; };
-    void mul2_school(const Pair *jobs, int nj, Poly *outs) {
-        Mul2Jobs J;
-        memset(&J, 0, sizeof J);
-        u64 off[4], total = 0, nmax = 0, xmax = 0;
-        long long dm[4];
-        for (int z = 0; z < nj; z++) {
-            const Pair &P = jobs[z];
-            const bool t1 = P.x1->deg >= 0 && P.y1->deg >= 0;
-            const bool t2 = P.x2 && P.x2->deg >= 0 && P.y2->deg >= 0;
-            dm[z] = -1;
-            if (t1) dm[z] = std::max(dm[z], P.x1->deg + P.y1->deg);
-            if (t2) dm[z] = std::max(dm[z], P.x2->deg + P.y2->deg);
-            J.nout[z] = dm[z] < 0 ? 1 : (u64)(dm[z] >> 6) + 2;
-            off[z] = total;
-            total += J.nout[z];
-            if (t1) { J.x1[z] = P.x1->p(); J.nx1[z] = P.x1->words(); J.y1[z] = P.y1->p(); J.ny1[z] = P.y1->words(); }
-            if (t2) { J.x2[z] = P.x2->p(); J.nx2[z] = P.x2->words(); J.y2[z] = P.y2->p(); J.ny2[z] = P.y2->words(); }
-            nmax = std::max(nmax, J.nout[z]);
-            xmax = std::max(xmax, std::max(J.nx1[z], J.nx2[z]));
-        }
-        Poly all = zeros(total);
-        for (int z = 0; z < nj; z++) {
-            J.out[z] = (unsigned long long *)(all.p() + off[z]);
-            outs[z] = Poly();
-            outs[z].b = alias(all.b, off[z], J.nout[z]);
-            outs[z].deg = dm[z];
-        }
-        const u64 chunk = 32;
-        dim3 grid((unsigned)((nmax / 2 + 1 + 127) / 128), (unsigned)std::max<u64>(1, (xmax + chunk - 1) / chunk),
-                  (unsigned)nj);
-        k_mul2<<<grid, 128, 0, st_>>>(J, chunk);
-        ckc(cudaGetLastError(), "k_mul2");
-        stats.school_mul2 += nj;
-    }
-
-    // (c, d) = M (a, b); exact degrees
-    void mat_vec(const Mat &M, const Poly &a, const Poly &b, Poly &c, Poly &d) {
-        Timer tm(stats.us_products);
-        if (M.ident) {
-            c = a;
-            d = b;
-            return;
-        }
-        if (std::max(M.e[0].deg + a.deg, M.e[1].deg + b.deg) + 1 > tn_.fft_bits) {
-            fft_mat_vec(M, a, b, c, d);
-        } else {
-            Pair P[2] = {{&M.e[0], &a, &M.e[1], &b}, {&M.e[2], &a, &M.e[3], &b}};
-            Poly o[2];
-            mul2_school(P, 2, o);
-            c = o[0];
-            d = o[1];
-        }
-        probe({&c, &d});
-    }
-
-    // FFT matrix x vector: the transforms of a and b serve both rows
-    void fft_mat_vec(const Mat &M, const Poly &a, const Poly &b, Poly &c, Poly &d) {
-        auto chunks = [](const Poly &p) { return p.deg < 0 ? 0 : ((u64)p.deg + 1 + 31) / 32; };
-        u64 need = 1;
-        for (int i = 0; i < 4; i++) {
-            const Poly &v = (i & 1) ? b : a;
-            if (M.e[i].deg >= 0 && v.deg >= 0) need = std::max(need, chunks(M.e[i]) + chunks(v) - 1);
-        }
-        int m = 1;
-        while (((u64)1 << m) < need) m++;
-        gf2e_fft_plan *plan = gf2e::cached_plan(m);
-        if (!plan) throw Fail{GF2E_ERR_CUDA};
-        const u64 n = (u64)1 << m;
-        Buf Fa = alloc(n), Fb = alloc(n), Fm[4];
-        auto fwd = [&](const Poly &p, u64 *f) {
-            if (p.deg < 0) ckc(cudaMemsetAsync(f, 0, n * 8, st_), "fft zero operand");
-            else ck(gf2e::fft_fwd_packed(plan, f, reinterpret_cast<const u32 *>(p.p()), chunks(p), st_));
-        };
-        fwd(a, Fa->p);
-        fwd(b, Fb->p);
-        for (int i = 0; i < 4; i++) {
-            Fm[i] = alloc(n);
-            fwd(M.e[i], Fm[i]->p);
-        }
-        for (int row = 0; row < 2; row++) {
-            u64 *o = Fm[2 * row]->p;
-            k_pw_muladd<<<gf2e::grid_for(n, 256), 256, 0, st_>>>(o, Fm[2 * row]->p, Fa->p,
-                                                                 Fm[2 * row + 1]->p, Fb->p, n);
-            ckc(cudaGetLastError(), "k_pw_muladd");
-            ck(gf2e::fft_run(plan, false, o, st_));
-            long long dmax = std::max(M.e[2 * row].deg + a.deg, M.e[2 * row + 1].deg + b.deg);
-            Poly &out = row ? d : c;
-            out = Poly();
-            if (dmax < 0) { out.b = alloc(1); out.deg = -1; continue; }
-            const u64 nout = (u64)(dmax >> 6) + 2;
-            out.b = alloc(nout);
-            ck(gf2e::overlap_add(o, need, out.p(), nout, st_));
-            out.deg = (long long)nout * 64 - 1;
-        }
-        stats.fft_mul2 += 2;
-    }
-
-    // M2 * M1 (degree bounds)
-    Mat mat_mul(const Mat &M2, const Mat &M1) {
-        Timer tm(stats.us_products);
-        if (M2.ident) return M1;
-        if (M1.ident) return M2;
-        Mat r;
-        long long dmax = 0;
-        for (int i = 0; i < 2; i++)
-            for (int j = 0; j < 2; j++)
-                dmax = std::max(dmax, std::max(M2.e[2 * i].deg + M1.e[j].deg,
-                                               M2.e[2 * i + 1].deg + M1.e[2 + j].deg));
-        if (dmax + 1 > tn_.fft_bits) return fft_mat_mul(M2, M1);
-        Pair P[4];
-        for (int i = 0; i < 2; i++)
-            for (int j = 0; j < 2; j++)
-                P[2 * i + j] = Pair{&M2.e[2 * i], &M1.e[j], &M2.e[2 * i + 1], &M1.e[2 + j]};
-        mul2_school(P, 4, r.e);
-        return r;
-    }
-
-    // FFT matrix x matrix: eight forward transforms, four inverse
-    Mat fft_mat_mul(const Mat &M2, const Mat &M1) {
-        auto chunks = [](const Poly &p) { return p.deg < 0 ? 0 : ((u64)p.deg + 1 + 31) / 32; };
-        u64 need = 1;
-        for (int i = 0; i < 2; i++)
-            for (int j = 0; j < 2; j++)
-                for (int k = 0; k < 2; k++) {
-                    const Poly &x = M2.e[2 * i + k], &y = M1.e[2 * k + j];
-                    if (x.deg >= 0 && y.deg >= 0) need = std::max(need, chunks(x) + chunks(y) - 1);
-                }
-        int m = 1;
-        while (((u64)1 << m) < need) m++;
-        gf2e_fft_plan *plan = gf2e::cached_plan(m);
-        if (!plan) throw Fail{GF2E_ERR_CUDA};
-        const u64 n = (u64)1 << m;
-        Buf F2[4], F1[4];
-        auto fwd = [&](const Poly &p, Buf &f) {
-            f = alloc(n);
-            if (p.deg < 0) ckc(cudaMemsetAsync(f->p, 0, n * 8, st_), "fft zero operand");
-            else ck(gf2e::fft_fwd_packed(plan, f->p, reinterpret_cast<const u32 *>(p.p()), chunks(p), st_));
-        };
-        for (int i = 0; i < 4; i++) { fwd(M2.e[i], F2[i]); fwd(M1.e[i], F1[i]); }
-        Mat r;
-        Buf O[4];
-        for (int i = 0; i < 2; i++)
-            for (int j = 0; j < 2; j++) {
-                Buf &o = O[2 * i + j];
-                o = alloc(n);
-                k_pw_muladd<<<gf2e::grid_for(n, 256), 256, 0, st_>>>(
-                    o->p, F2[2 * i]->p, F1[j]->p, F2[2 * i + 1]->p, F1[2 + j]->p, n);
-                ckc(cudaGetLastError(), "k_pw_muladd");
-                ck(gf2e::fft_run(plan, false, o->p, st_));
-                long long dm = std::max(M2.e[2 * i].deg + M1.e[j].deg,
-                                        M2.e[2 * i + 1].deg + M1.e[2 + j].deg);
-                Poly &out = r.e[2 * i + j];
-                if (dm < 0) { out.b = alloc(1); out.deg = -1; continue; }
-                const u64 nout = (u64)(dm >> 6) + 2;
-                out.b = alloc(nout);
-                ck(gf2e::overlap_add(o->p, need, out.p(), nout, st_));
-                out.deg = dm;
-            }
-        stats.fft_mul2 += 4;
-        return r;
-    }
-
-    Mat identity() {
-        Mat I;
-        I.ident = true;
-        return I;
-    }
-    Mat materialize(const Mat &M) {
-        if (!M.ident) return M;
-        Mat r;
-        r.e[0] = constant1();
-        r.e[3] = constant1();
-        r.e[1].b = alloc(1); r.e[1].deg = -1;
-        r.e[2].b = alloc(1); r.e[2].deg = -1;
-        ckc(cudaMemsetAsync(r.e[1].p(), 0, 8, st_), "zero");
-        ckc(cudaMemsetAsync(r.e[2].p(), 0, 8, st_), "zero");
-        return r;
-    }
-
-    // out = x ^ ((q y) << s), new buffer sized for the bound
-    Poly axpy(const Poly &x, const Poly &y, u64 q, long long s, long long deg_bound) {
-        Poly r;
-        const long long dq = deg64_host(q);
-        long long d = x.deg;
-        if (y.deg >= 0 && dq >= 0) d = std::max(d, y.deg + dq + s);
-        d = std::min(d, deg_bound < 0 ? d : deg_bound);
-        if (d < 0) { r.b = alloc(1); r.deg = -1; return r; }
-        const u64 nout = (u64)(d >> 6) + 1;
-        r.b = alloc(nout);
-        k_axpy_q<<<gf2e::grid_for(nout, 256), 256, 0, st_>>>(r.p(), nout, x.p(), x.words(),
-                                                              y.p(), y.words(), q, (u64)s);
-        ckc(cudaGetLastError(), "k_axpy_q");
-        r.deg = d;
-        return r;
-    }
-    static long long deg64_host(u64 v) { return v ? 63 - __builtin_clzll(v) : -1; }
-
-    // (c, d), rows (R0, R1) -> (d, c mod d), rows (R1, R0 + q R1); c, d exact
-    void divstep(Poly &c, Poly &d, Mat *M) {
-        Timer tm(stats.us_division);
-        stats.divsteps++;
-        if (d.deg < 0) throw Fail{gf2e::invalid("hgcd: division by zero")};
-        u64 win[2];
-        Poly cc = c;
-        if (!c.has_win || !d.has_win) probe({&cc, &d}, win);
-        u64 wc = cc.win;
-        const u64 wd = d.win;
-        Poly r0a, r0b;
-        if (M) { r0a = M->e[0]; r0b = M->e[1]; }
-        bool first = true;
-        for (int guard = 0; cc.deg >= d.deg; guard++) {
-            if (guard > (1 << 22)) throw Fail{gf2e::invalid("hgcd: division did not converge")};
-            const long long delta = cc.deg - d.deg;
-            const int nb = (int)std::min<long long>(delta, 63);   // quotient bits - 1
-            u64 q = 0, r = wc;
-            for (int t = 0; t <= nb; t++)
-                if ((r >> (63 - t)) & 1) {
-                    q |= 1ull << (nb - t);
-                    r ^= wd >> t;
-                }
-            const long long s = delta - nb;
-            // c ^= (q d) << s, in place (the result has lower degree)
-            Poly nc;
-            nc.b = first ? alloc(cc.words()) : cc.b;
-            nc.deg = cc.deg;
-            k_axpy_q<<<gf2e::grid_for(cc.words(), 256), 256, 0, st_>>>(
-                nc.p(), cc.words(), cc.p(), cc.words(), d.p(), d.words(), q, (u64)s);
-            ckc(cudaGetLastError(), "k_axpy_q");
-            if (M) {
-                r0a = axpy(r0a, M->e[2], q, s, -1);
-                r0b = axpy(r0b, M->e[3], q, s, -1);
-            }
-            first = false;
-            cc = nc;
-            probe({&cc}, win);
-            wc = win[0];
-        }
-        if (M) {
-            Poly n0 = M->e[2], n1 = M->e[3];
-            M->e[0] = n0; M->e[1] = n1;
-            M->e[2] = r0a; M->e[3] = r0b;
-        }
-        c = d;
-        d = cc;
-    }
-
-    Mat base(const Poly &a, const Poly &b, long long m) {
-        Timer tm(stats.us_base);
-        stats.bases++;
-        const u64 W = (u64)(a.deg >> 6) + 2;
-        const u64 mw = (u64)((a.deg - m) >> 6) + 3;
-        Buf out = alloc(4 * mw);
-        const size_t smem = (4 * W + 8 * mw) * 8;
-        base_smem_attr();
-        // no round trip: statuses and counters accumulate on the device and
-        // are read once when the gcd is done (finish_bases)
-        BaseBatch BB;
-        memset(&BB, 0, sizeof BB);
-        BB.a = a.p();
-        BB.b = b.p();
-        BB.M = out->p;
-        BB.da[0] = a.deg;
-        BB.db[0] = b.deg;
-        BB.m[0] = m;
-        k_hgcd_base<<<1, BASE_THREADS, smem, st_>>>(BB, W, mw, (BaseAcc *)d_res_->p);
-        ckc(cudaGetLastError(), "k_hgcd_base");
-        Mat M;
-        const long long dm = a.deg - m;       // entries have degree <= n - m
-        for (int i = 0; i < 4; i++) {         // four views into the output buffer
-            M.e[i].b = alias(out, (size_t)i * mw, mw);
-            M.e[i].deg = std::max(0LL, dm);
-        }
-        return M;
-    }
-
-    Buf alias(const Buf &owner, size_t off, size_t words) { return view_of(owner, off, words); }
-
-    // deg a = n > deg b; exact degrees on entry
-    Mat hgcd(const Poly &a, const Poly &b) {
-        stats.nodes++;
-        const long long n = a.deg, m = (n + 1) / 2;
-        if (b.deg < m) return identity();
-        if (n <= tn_.base_bits) return base(a, b, m);
-        Poly a1 = shr(a, m), b1 = shr(b, m);
-        Mat M1 = hgcd(a1, b1);
-        Poly c, d;
-        mat_vec(M1, a, b, c, d);
-        if (c.deg < d.deg) {                      // not expected; keep the order
-            std::swap(c, d);
-            if (!M1.ident) { std::swap(M1.e[0], M1.e[2]); std::swap(M1.e[1], M1.e[3]); }
-        }
-        if (d.deg < m) return M1;
-        M1 = materialize(M1);
-        divstep(c, d, &M1);
-        if (d.deg < m) return M1;
-        const long long l = c.deg, k = std::max(0LL, 2 * m - l);
-        Poly c1 = shr(c, k), d1 = shr(d, k);
-        Mat M2 = hgcd(c1, d1);
-        return mat_mul(M2, M1);
-    }
-
-    // gcd of two polynomials on the device; returns the gcd (exact degree)
-    Poly gcd(Poly a, Poly b) {
-        for (long long it = 0;; it++) {
-            if (a.deg < b.deg) std::swap(a, b);
-            if (b.deg < 0) return a;
-            if (a.deg < tn_.small_gcd_bits) return small_gcd(a, b);
-            if (a.deg == b.deg) { divstep(a, b, nullptr); continue; }
-            Mat M = hgcd(a, b);
-            if (!M.ident) {
-                Poly c, d;
-                mat_vec(M, a, b, c, d);
-                a = c;
-                b = d;
-                if (a.deg < b.deg) std::swap(a, b);
-            }
-            if (b.deg >= 0) divstep(a, b, nullptr);
-            if (it > 4 * 64) throw Fail{gf2e::invalid("hgcd: no convergence")};
-        }
-    }
-
-    Poly small_gcd(const Poly &a, const Poly &b) {
-        Timer tm(stats.us_small);
-        gf2e_gcd_job job;
-        memset(&job, 0, sizeof job);
-        job.a_dev = a.p();
-        job.abits = (u64)a.deg + 1;
-        job.b_dev = b.p();
-        job.bbits = (u64)b.deg + 1;
-        const u64 gw = (u64)(std::max(a.deg, b.deg) >> 6) + 2;
-        Poly g = zeros(gw);
-        job.g_dev = g.p();
-        job.g_cap_words = gw;
-        size_t need = 0;
-        ck(gf2e_gcd_workspace_size(&job, 1, &need));
-        Buf ws = alloc((need + 7) / 8);
-        int64_t deg = -1;
-        ck(gf2e_gcd_batch(&job, 1, &deg, ws->p, need, st_));
-        g.deg = deg;
-        return g;
-    }
-
-private:
-    Arena arena_;                      // declared first: destroyed after every buffer
-    cudaStream_t st_;
-    cudaMemPool_t pool_;
-    Tunables tn_;
-    long long *h_probe_ = nullptr;
-    Buf d_probe_, d_res_;
 };
 
 // ================================================================ lockstep
@@ -1415,7 +844,7 @@ struct BMat {
 class HgcdBatch {
 public:
     HgcdBatch(int G, cudaStream_t st, cudaMemPool_t pool)
-        : arena_(st, pool), G_(G), st_(st), tn_(tunables(true)) {
+        : arena_(st, pool), G_(G), st_(st), tn_(tunables(G > 1)) {
         ckc(cudaMallocHost(&h_probe_, (size_t)GMAX * 8 * sizeof(long long)), "hgcd probe host buffer");
         d_probe_ = alloc(GMAX * 8);
         d_res_ = alloc(8);
@@ -2130,46 +1559,6 @@ cudaMemPool_t hgcd_pool() {
     return pools[dev];
 }
 
-int run_one(const gf2e_gcd_job &j, int64_t *deg_out, gf2e_hgcd_stats *stats, cudaStream_t st) {
-    cudaMemPool_t pool = hgcd_pool();
-    if (!pool) return gf2e::cuda_status(cudaErrorMemoryAllocation, "hgcd memory pool");
-    try {
-        Hgcd H(st, pool);
-        Poly a = H.from_device(j.a_dev, j.abits), b = H.from_device(j.b_dev, j.bbits);
-        Poly g = H.gcd(a, b);
-        H.finish_bases();
-        *deg_out = g.deg < 0 ? 0 : g.deg;
-        if (j.g_dev && j.g_cap_words) {
-            const u64 gw = g.deg < 0 ? 0 : g.words();
-            if (gw <= j.g_cap_words) {
-                ckc(cudaMemsetAsync(j.g_dev, 0, j.g_cap_words * 8, st), "gcd out clear");
-                if (gw) ckc(cudaMemcpyAsync(j.g_dev, g.p(), gw * 8, cudaMemcpyDeviceToDevice, st),
-                            "gcd out");
-            }
-        }
-        ckc(cudaStreamSynchronize(st), "hgcd done");
-        if (stats) {
-            stats->nodes = H.stats.nodes;
-            stats->base_cases = H.stats.bases;
-            stats->base_rounds = H.stats.base_rounds;
-            stats->fft_products = H.stats.fft_mul2;
-            stats->school_products = H.stats.school_mul2;
-            stats->division_steps = H.stats.divsteps;
-            stats->probes = H.stats.probes;
-            stats->us_base = (int64_t)H.stats.us_base;
-            stats->us_products = (int64_t)H.stats.us_products;
-            stats->us_division = (int64_t)H.stats.us_division;
-            stats->us_small_gcd = (int64_t)H.stats.us_small;
-            stats->base_cycles_serial = H.stats.cyc_serial;
-            stats->base_cycles_total = H.stats.cyc_total;
-        }
-        return GF2E_OK;
-    } catch (const Fail &f) {
-        cudaStreamSynchronize(st);
-        return f.st;
-    }
-}
-
 // members in flight: the caller's cap, GMAX, and what device memory holds
 // (per member about 40 operand-sized buffers and 12 transforms of the
 // largest matrix product: 1.52 GB measured at r = 136279841), counting as
@@ -2294,38 +1683,7 @@ int gf2e_gcd_large(const gf2e_gcd_job *jobs, int njobs, int64_t *deg_host, int m
     if (e == cudaSuccess) e = cudaEventSynchronize(ready);
     cudaEventDestroy(ready);
     if (e != cudaSuccess) return gf2e::cuda_status(e, "gf2e_gcd_large operands");
-    if (njobs >= 2 && max_parallel >= 2) return run_lockstep(jobs, njobs, deg_host, max_parallel, stats);
-    // one job at a time
-    cudaStream_t s;
-    e = cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking);
-    if (e != cudaSuccess) return gf2e::cuda_status(e, "hgcd stream");
-    int worst = GF2E_OK;
-    if (stats) memset(stats, 0, sizeof *stats);
-    for (int i = 0; i < njobs; i++) {
-        gf2e_hgcd_stats one;
-        memset(&one, 0, sizeof one);
-        int64_t d = -1;
-        const int rc = run_one(jobs[i], &d, &one, s);
-        deg_host[i] = d;
-        if (rc != GF2E_OK) worst = rc;
-        if (stats) {
-            stats->nodes += one.nodes;
-            stats->base_cases += one.base_cases;
-            stats->base_rounds += one.base_rounds;
-            stats->fft_products += one.fft_products;
-            stats->school_products += one.school_products;
-            stats->division_steps += one.division_steps;
-            stats->probes += one.probes;
-            stats->us_base += one.us_base;
-            stats->us_products += one.us_products;
-            stats->us_division += one.us_division;
-            stats->us_small_gcd += one.us_small_gcd;
-            stats->base_cycles_serial += one.base_cycles_serial;
-            stats->base_cycles_total += one.base_cycles_total;
-        }
-    }
-    cudaStreamDestroy(s);
-    return worst;
+    return run_lockstep(jobs, njobs, deg_host, std::max(1, max_parallel), stats);
 }
 
 }  // extern "C"
