@@ -570,7 +570,7 @@ def deep_scan_gcd_sample(M, nsurv=8, maxd=88, block=1):
     """Config 4's full cycle at r = 136279841 on a bounded sample: `nsurv`
     d<=24 survivors (s = 474 first, the reference's known answer
     `474 41 p3991ef16129`), ramp to k0 = 24, running products for degrees
-    25..maxd, then the interval-end gcds (concurrent half-gcds) and hit
+    25..maxd, then the interval-end gcds (one lockstep half-gcd batch) and hit
     resolution; wall time of the whole scan call."""
     smax = 200000
     best = M.run_sieve(R, 24, smax)
@@ -582,7 +582,7 @@ def deep_scan_gcd_sample(M, nsurv=8, maxd=88, block=1):
     return {"survivors": surv, "k0": 24, "maxd": maxd, "results": lines, "wall_s": wall,
             "sd_pairs_per_s": nsurv * (maxd - 24) / wall,
             "known_answer_474": "474 41 p3991ef16129" in lines, "block": block,
-            "note": "one interval of 64 degrees then one half-gcd per s (concurrent)"}
+            "note": "one interval of 64 degrees then one half-gcd per s (one lockstep batch)"}
 
 
 def serving_sample(n_jobs=24, rate=16.0, seed=1):

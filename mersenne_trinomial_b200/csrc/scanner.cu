@@ -103,8 +103,9 @@ struct gf2e_scanner {
 // operands of at least this many bits take the half-gcd (hgcd.cu) at
 // interval ends; smaller ones the quadratic batched gcd (gcd.cu)
 constexpr u64 GCD_LARGE_BITS = 1ull << 19;
-// device words a concurrent half-gcd job draws from its pool, per operand word
-constexpr size_t HGCD_WORDS_PER_WORD = 48;
+// device words one member of a lockstep half-gcd batch draws from the gcd
+// pool, per operand word (its high-water mark: 1.52 GB at r = 136279841)
+constexpr size_t HGCD_WORDS_PER_WORD = 90;
 
 namespace gf2e {
 
@@ -550,8 +551,9 @@ int gf2e_scanner_footprint_blocked(uint64_t r, int slots, int block, size_t *byt
         return gf2e::invalid("scanner: block size must be 1 or even in 2..62");
     Geometry g = geometry(r);
     size_t words = device_words(g, slots, block);
-    // gcd workspace: job table + 4 buffers per job (quadratic gcd), or the
-    // pools of the concurrent half-gcds
+    // gcd workspace: job table + 4 buffers per job (quadratic gcd), or room
+    // for 16 members of a half-gcd batch (a batch sizes itself from the
+    // memory free when it starts, so more slots only make it run in parts)
     size_t gw = ((size_t)slots * 96 + 255) + (size_t)slots * 4 * (g.tw + 1) * 8;
     if (r >= GCD_LARGE_BITS) {
         int par = 16;
