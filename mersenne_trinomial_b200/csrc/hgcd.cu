@@ -45,6 +45,7 @@
 #include <atomic>
 #include <chrono>
 #include <cstring>
+#include <exception>
 #include <memory>
 #include <mutex>
 #include <thread>
@@ -1638,6 +1639,10 @@ int run_lockstep(const gf2e_gcd_job *jobs, int njobs, int64_t *deg_host, int max
             } catch (const Fail &f) {
                 cudaStreamSynchronize(st);
                 if (f.st != GF2E_ERR_NOMEM || nb == 1) return f.st;
+            } catch (const std::exception &x) {        // host allocation and the like
+                cudaStreamSynchronize(st);
+                gf2e::set_error("hgcd: %s", x.what());
+                return GF2E_ERR_INTERNAL;
             }
             const int h = nb / 2;
             const int r1 = self(self, i0, h);
