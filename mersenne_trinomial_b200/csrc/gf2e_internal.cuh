@@ -86,18 +86,39 @@ GF2E_DEV u64 spread32(u32 v) {
 // 8 ones, which never carries into the next column of the same residue
 // class mod 4, so masking each partial product to its class recovers the
 // XOR sum.
-GF2E_DEV u64 clmul32(u32 a, u32 b) {
-    const u32 m0 = 0x11111111u, m1 = 0x22222222u, m2 = 0x44444444u,
-              m3 = 0x88888888u;
-    u64 a0 = a & m0, a1 = a & m1, a2 = a & m2, a3 = a & m3;
-    u64 b0 = b & m0, b1 = b & m1, b2 = b & m2, b3 = b & m3;
+// 32 x 32 -> 64 integer product (one widening multiply)
+GF2E_DEV u64 mulw32(u32 a, u32 b) {
+    u64 r;
+    asm("mul.wide.u32 %0, %1, %2;" : "=l"(r) : "r"(a), "r"(b));
+    return r;
+}
+// a 32-bit operand split into its four bit classes mod 4
+struct Masked {
+    u32 p[4];
+};
+GF2E_DEV Masked mask32(u32 a) {
+    Masked m;
+    m.p[0] = a & 0x11111111u;
+    m.p[1] = a & 0x22222222u;
+    m.p[2] = a & 0x44444444u;
+    m.p[3] = a & 0x88888888u;
+    return m;
+}
+// the product from operands already split (a matrix entry or a word used
+// in several products is split once)
+GF2E_DEV u64 clmul_masked(const Masked &a, const Masked &b) {
     const u64 M0 = 0x1111111111111111ull;
-    u64 c0 = (a0 * b0) ^ (a1 * b3) ^ (a2 * b2) ^ (a3 * b1);
-    u64 c1 = (a0 * b1) ^ (a1 * b0) ^ (a2 * b3) ^ (a3 * b2);
-    u64 c2 = (a0 * b2) ^ (a1 * b1) ^ (a2 * b0) ^ (a3 * b3);
-    u64 c3 = (a0 * b3) ^ (a1 * b2) ^ (a2 * b1) ^ (a3 * b0);
+    const u64 c0 = mulw32(a.p[0], b.p[0]) ^ mulw32(a.p[1], b.p[3]) ^ mulw32(a.p[2], b.p[2]) ^
+                   mulw32(a.p[3], b.p[1]);
+    const u64 c1 = mulw32(a.p[0], b.p[1]) ^ mulw32(a.p[1], b.p[0]) ^ mulw32(a.p[2], b.p[3]) ^
+                   mulw32(a.p[3], b.p[2]);
+    const u64 c2 = mulw32(a.p[0], b.p[2]) ^ mulw32(a.p[1], b.p[1]) ^ mulw32(a.p[2], b.p[0]) ^
+                   mulw32(a.p[3], b.p[3]);
+    const u64 c3 = mulw32(a.p[0], b.p[3]) ^ mulw32(a.p[1], b.p[2]) ^ mulw32(a.p[2], b.p[1]) ^
+                   mulw32(a.p[3], b.p[0]);
     return (c0 & M0) ^ (c1 & (M0 << 1)) ^ (c2 & (M0 << 2)) ^ (c3 & (M0 << 3));
 }
+GF2E_DEV u64 clmul32(u32 a, u32 b) { return clmul_masked(mask32(a), mask32(b)); }
 
 // GF(2^64) = GF(2)[x]/(x^64 + x^4 + x^3 + x + 1) multiply (Karatsuba over
 // clmul32 and the two-step reduction by the sparse modulus).

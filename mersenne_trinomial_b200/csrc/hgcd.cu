@@ -257,21 +257,6 @@ __global__ void k_set_one_b(u64 *p, u64 stride, int G) {
 }
 
 // ---- base case: Lehmer half-gcd in one CTA, operands in shared memory ----
-struct Masked { u64 p[4]; };
-GF2E_DEV Masked mask32(u32 a) {
-    Masked m;
-    m.p[0] = a & 0x11111111u; m.p[1] = a & 0x22222222u;
-    m.p[2] = a & 0x44444444u; m.p[3] = a & 0x88888888u;
-    return m;
-}
-GF2E_DEV u64 clmul_masked(const Masked &a, const Masked &b) {
-    const u64 M0 = 0x1111111111111111ull;
-    u64 c0 = (a.p[0] * b.p[0]) ^ (a.p[1] * b.p[3]) ^ (a.p[2] * b.p[2]) ^ (a.p[3] * b.p[1]);
-    u64 c1 = (a.p[0] * b.p[1]) ^ (a.p[1] * b.p[0]) ^ (a.p[2] * b.p[3]) ^ (a.p[3] * b.p[2]);
-    u64 c2 = (a.p[0] * b.p[2]) ^ (a.p[1] * b.p[1]) ^ (a.p[2] * b.p[0]) ^ (a.p[3] * b.p[3]);
-    u64 c3 = (a.p[0] * b.p[3]) ^ (a.p[1] * b.p[2]) ^ (a.p[2] * b.p[1]) ^ (a.p[3] * b.p[0]);
-    return (c0 & M0) ^ (c1 & (M0 << 1)) ^ (c2 & (M0 << 2)) ^ (c3 & (M0 << 3));
-}
 
 GF2E_DEV u64 win_at(const u64 *X, long long nw, long long pos) {   // bits pos..pos+63
     long long i = pos >> 6;
