@@ -365,14 +365,25 @@ GF2E_DEV u64 mul64x32_lo(u64 x, const Masked &m) {
 GF2E_DEV u64 mul64x32_hi(u64 x, const Masked &m) {
     return clmul_masked(mask32((u32)(x >> 32)), m) >> 32;
 }
-// x * m as 96 bits (lo: bits 0..63, hi: bits 64..95) from the masks of
-// x's two halves
-struct WordMasks { Masked l, h; };
-GF2E_DEV WordMasks word_masks(u64 x) { return {mask32((u32)x), mask32((u32)(x >> 32))}; }
-GF2E_DEV void mul96(const WordMasks &x, const Masked &m, u64 &lo, u64 &hi) {
-    const u64 pl = clmul_masked(x.l, m), ph = clmul_masked(x.h, m);
-    lo = pl ^ (ph << 32);
-    hi = ph >> 32;
+// x * m_a and x * m_b as 96 bits each (lo: bits 0..63, hi: bits 64..95) by
+// 16-entry tables T[v] = v * m (v a nibble, entries of up to 35 bits), one
+// pass over x's nibbles for both: lookups, shifts and XORs, no multiplies
+// (the 32 x 32 -> 64 multiplier of the bit-class product is the apply's
+// bottleneck)
+GF2E_DEV void mul96_tab2(u64 x, const u64 *Ta, const u64 *Tb, u64 &la, u64 &ha, u64 &lb,
+                         u64 &hb) {
+    la = ha = lb = hb = 0;
+#pragma unroll
+    for (int i = 0; i < 16; i++) {
+        const unsigned v = (unsigned)(x >> (4 * i)) & 15u;
+        const u64 ta = Ta[v], tb = Tb[v];
+        la ^= ta << (4 * i);
+        lb ^= tb << (4 * i);
+        if (i >= 8) {                                  // entries reach bit 34
+            ha ^= ta >> (64 - 4 * i);
+            hb ^= tb >> (64 - 4 * i);
+        }
+    }
 }
 // word w of (X << k) for a vector X
 GF2E_DEV u64 shl_word(const u64 *X, long long w, long long k) {
@@ -425,6 +436,7 @@ k_hgcd_base(const BaseBatch BB, u64 W, u64 mw, BaseAcc *acc) {
     __shared__ int s_va[2], s_vb[2], s_ra[2], s_mode[2], s_done[2], s_slow;
     __shared__ long long s_k[2], s_top[2], s_md[2];
     __shared__ u32 s_m[2][4];
+    __shared__ u64 s_tab[(BASE_THREADS / 32 / 4) * 3][64];   // per apply warp: v * m_e
     const int tid = threadIdx.x;
     for (u64 i = tid; i < 4 * W; i += BASE_THREADS) {
         u64 v = 0;
@@ -505,10 +517,23 @@ k_hgcd_base(const BaseBatch BB, u64 W, u64 mw, BaseAcc *acc) {
             // new vectors (A', B') from (A, B), or the new row entries
             // (N[col], N[2 + col]) from (RA[col], RB[col]).  Lane l takes
             // word 31 c + l - 1 of the inputs, computes its full products
-            // and passes their high words up one lane: lane 0's word only
-            // feeds lane 1, so every input word is masked and multiplied once.
+            // (by the warp's nibble tables of the four matrix entries) and
+            // passes their high words up one lane: lane 0's word only feeds
+            // lane 1, so every input word is multiplied once.
             constexpr int APPLY_WARPS = (BASE_THREADS / 32 / 4) * 3;
             const int aw = warp - 1 - (warp >> 2), lane = tid & 31;
+            u64 *T = s_tab[aw];                         // T[16 e + v] = v * m_e
+            if (mode != 1) {
+                for (int i = lane; i < 64; i += 32) {
+                    const u64 me = s_m[p][i >> 4];
+                    u64 t = 0;
+#pragma unroll
+                    for (int b = 0; b < 4; b++)
+                        if ((i >> b) & 1) t ^= me << b;
+                    T[i] = t;
+                }
+                __syncwarp();
+            }
             const long long ncv = (nwv + 30) / 31, ncr = (nwm + 31) / 31;
             for (long long c = aw; c < ncv + 2 * ncr; c += APPLY_WARPS) {
                 const bool vec = c < ncv;
@@ -526,14 +551,11 @@ k_hgcd_base(const BaseBatch BB, u64 W, u64 mw, BaseAcc *acc) {
                         o1 = Y[w];
                     }
                 } else {                                // (m0 X + m1 Y, m2 X + m3 Y)
-                    const WordMasks xm = word_masks(in ? X[w] : 0), ym = word_masks(in ? Y[w] : 0);
-                    u64 l0, h0, l1, h1, tl, th;
-                    mul96(xm, m0, l0, h0);
-                    mul96(ym, m1, tl, th);
-                    l0 ^= tl; h0 ^= th;
-                    mul96(xm, m2, l1, h1);
-                    mul96(ym, m3, tl, th);
-                    l1 ^= tl; h1 ^= th;
+                    u64 l0, h0, l1, h1, tl0, th0, tl1, th1;
+                    mul96_tab2(in ? X[w] : 0, T, T + 32, l0, h0, l1, h1);        // x m0, x m2
+                    mul96_tab2(in ? Y[w] : 0, T + 16, T + 48, tl0, th0, tl1, th1);  // y m1, y m3
+                    l0 ^= tl0; h0 ^= th0;
+                    l1 ^= tl1; h1 ^= th1;
                     o0 = l0 ^ __shfl_up_sync(0xffffffffu, h0, 1);
                     o1 = l1 ^ __shfl_up_sync(0xffffffffu, h1, 1);
                 }
