@@ -853,10 +853,11 @@ class HgcdBatch {
 public:
     HgcdBatch(int G, cudaStream_t st, cudaMemPool_t pool)
         : arena_(st, pool), G_(G), st_(st), tn_(tunables(G > 1)) {
-        ckc(cudaMallocHost(&h_probe_, (size_t)GMAX * 8 * sizeof(long long)), "hgcd probe host buffer");
         d_probe_ = alloc(GMAX * 8);
         d_res_ = alloc(8);
         ckc(cudaMemsetAsync(d_res_->p, 0, sizeof(BaseAcc), st_), "hgcd base accumulator");
+        // last: a constructor that throws runs no destructor
+        ckc(cudaMallocHost(&h_probe_, (size_t)GMAX * 8 * sizeof(long long)), "hgcd probe host buffer");
     }
     ~HgcdBatch() {
         if (h_probe_) cudaFreeHost(h_probe_);
